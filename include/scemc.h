@@ -1,0 +1,233 @@
+/*
+ * scemc.h — C ABI of libscemc_cuda.so, the B200 (sm_100a) chain-level spin Monte
+ * Carlo sweep for SCEMonteCarlo.jl tiled SCE Hamiltonians.
+ *
+ * Conventions
+ *   - Every entry point returns an int32 status (SCEMC_OK = 0); on failure the
+ *     message is available from scemc_last_error(). No exception or abort ever
+ *     crosses the boundary; device waits are bounded and report SCEMC_ERR_TIMEOUT.
+ *   - Index arrays are passed exactly as the Julia `TiledHamiltonian` holds them
+ *     (1-based); the library rebases them when it builds its device tables.
+ *   - Spin configurations cross the boundary as 3 x n_sites FP64 column-major
+ *     arrays (the `to_matrix` layout of the reference); the device holds them as
+ *     FP32 float4. Energies are FP64.
+ *   - Calls are synchronous: they return after the device work completed.
+ *   - Objects are not thread-safe; one host thread per chain/batch at a time.
+ *
+ * Reference interfaces replaced (paths relative to the SCEMonteCarlo.jl root):
+ *   scemc_tables_create        GPUTiledHamiltonian(backend, H)   src/gpu/gpu_hamiltonian.jl:438-459
+ *   scemc_chain_create         GPUChainState(gH, st; seed)       src/gpu/gpu_state.jl:335-347
+ *   scemc_metropolis_sweep     gpu_metropolis_sweep!             src/gpu/gpu_sweep.jl:158-190
+ *   scemc_run_sweeps           gpu_run_sweeps!                   src/gpu/gpu_sweep.jl:204-218
+ *   scemc_download             to_host!                          src/gpu/gpu_state.jl:357-362
+ *   scemc_upload               _from_host!                       src/gpu/gpu_state.jl:367-372
+ *   scemc_swap_payload         _swap_payload! (device lanes)     src/gpu/gpu_pt.jl:46-51
+ *   scemc_overrelaxation_sweep overrelaxation_sweep! (CPU-only in the reference)
+ *                                                                src/updates.jl:231-248
+ *   scemc_total_energy         _total_energy                     src/energy.jl:55-75
+ *   scemc_renormalize          _renormalize!                     src/state.jl:168-185
+ *   scemc_batch_*              gpu_run_pt lanes + exchanges      src/gpu/gpu_pt.jl:82-140
+ *   scemc_color_sites          _color_sites (table-build helper) src/hamiltonian.jl:456-499
+ */
+#ifndef SCEMC_H
+#define SCEMC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  SCEMC_OK = 0,
+  SCEMC_ERR_ARG = 1,          /* ArgumentError / DimensionMismatch equivalents */
+  SCEMC_ERR_UNSUPPORTED = 2,  /* e.g. lmax > 6 (gpu_hamiltonian.jl:439-440) */
+  SCEMC_ERR_CUDA = 3,         /* a CUDA runtime call failed */
+  SCEMC_ERR_TIMEOUT = 4,      /* a bounded device wait gave up (grid barrier) */
+  SCEMC_ERR_EXHAUSTED = 5,    /* 32-bit sweep counter exhausted (gpu_sweep.jl:163-164) */
+  SCEMC_ERR_NUMERIC = 6       /* non-finite value detected in the state */
+};
+
+typedef struct scemc_tables scemc_tables;
+/* A chain and a batch are the same device object: a set of replicas over one or
+ * more table sets. A chain is a batch of one replica. */
+typedef struct scemc_ensemble scemc_chain;
+typedef struct scemc_ensemble scemc_batch;
+
+/* The flat arrays of one TiledHamiltonian (src/hamiltonian.jl:234-265,62-91),
+ * 1-based as Julia holds them. Lengths: site_ptr n_sites+1; site_inst/site_slot/
+ * site_prog/site_col/site_col2 n_adj; inst_term n_inst; inst_ptr n_inst+1;
+ * inst_sites n_inst_sites; sprog_ptr n_sprog+1; sent_w/sent_tgt/sfac_ptr(+1)/
+ * pent_row/pent_row2 n_sent; sfac_row/sfac_slot n_sfac; eprog_ptr n_terms+1;
+ * eent_w/efac_ptr(+1) n_eent; efac_row n_efac; term_coef n_terms; color_ptr
+ * n_colors+1; color_sites n_active; site_has_l1/site_active n_sites.
+ * term_body/term_ls give each template's body order and per-member l (ls
+ * concatenated over templates); they let the library pick its dense fast paths. */
+typedef struct scemc_tables_desc {
+  int32_t n_sites, nlm, lmax, n_colors, n_active, n_cell_atoms;
+  int64_t n_adj, n_inst, n_inst_sites, n_sprog, n_sent, n_sfac, n_terms, n_eent, n_efac;
+  const int32_t* site_ptr;
+  const int32_t* site_inst;
+  const int8_t* site_slot;
+  const int32_t* inst_term;
+  const int32_t* inst_ptr;
+  const int32_t* inst_sites;
+  const int32_t* site_prog;
+  const int32_t* sprog_ptr;
+  const double* sent_w;
+  const int32_t* sent_tgt;
+  const int32_t* sfac_ptr;
+  const int32_t* sfac_row;
+  const int8_t* sfac_slot;
+  const int32_t* site_col;
+  const int32_t* site_col2;
+  const int32_t* pent_row;
+  const int32_t* pent_row2;
+  const int32_t* eprog_ptr;
+  const double* eent_w;
+  const int32_t* efac_ptr;
+  const int32_t* efac_row;
+  const double* term_coef;
+  const int32_t* term_body;
+  const int32_t* term_ls;
+  const int32_t* color_ptr;
+  const int32_t* color_sites;
+  const uint8_t* site_has_l1;
+  const uint8_t* site_active;
+} scemc_tables_desc;
+
+/* Copies the last error message of this host thread (NUL-terminated). */
+int32_t scemc_last_error(char* buf, size_t len);
+/* Library version as major*10000 + minor*100 + patch. */
+int32_t scemc_version(void);
+
+/* GPUTiledHamiltonian(backend, H): validates and uploads the tables to the current
+ * CUDA device. lmax > 6 => SCEMC_ERR_UNSUPPORTED. */
+int32_t scemc_tables_create(const scemc_tables_desc* desc, scemc_tables** out);
+int32_t scemc_tables_destroy(scemc_tables* t);
+/* Table statistics used by the roofline: mean distinct neighbours per active site
+ * (d), mean adjacency entries per active site (A), and table bytes on the device. */
+int32_t scemc_tables_stats(const scemc_tables* t, double* d_mean, double* a_mean, int64_t* bytes);
+
+/* GPUChainState(gH, st; seed): uploads config (3 x n_sites FP64, column-major) and
+ * the chain's incremental energy; step is the Metropolis rotation scale. */
+int32_t scemc_chain_create(const scemc_tables* t, const double* config, double energy, uint64_t seed,
+                           double step, scemc_chain** out);
+int32_t scemc_chain_destroy(scemc_chain* c);
+
+/* gpu_metropolis_sweep!: one Metropolis sweep at inverse temperature beta.
+ * lanes_per_site (the reference's workgroupsize) must be a power of two; values
+ * above 32 use 32. *n_accepted receives the number of accepted moves. */
+int32_t scemc_metropolis_sweep(scemc_chain* c, const scemc_tables* t, double beta, int32_t lanes_per_site,
+                               int64_t* n_accepted);
+/* One overrelaxation sweep (reflection about the local l = 1 field + Metropolis
+ * accept on the exact dE; updates.jl:66-87). *n_attempted counts sites with a
+ * non-vanishing l = 1 field. */
+int32_t scemc_overrelaxation_sweep(scemc_chain* c, const scemc_tables* t, double beta,
+                                   int32_t lanes_per_site, int64_t* n_accepted, int64_t* n_attempted);
+/* gpu_run_sweeps! without the trailing download: nsweeps Metropolis sweeps, with a
+ * device renormalisation + FP64 energy recompute every renorm_interval sweeps
+ * (<= 0 disables). Call scemc_download for to_host!. */
+int32_t scemc_run_sweeps(scemc_chain* c, const scemc_tables* t, double beta, int64_t nsweeps,
+                         int64_t renorm_interval, int32_t lanes_per_site);
+/* to_host!: config (3 x n_sites FP64), incremental energy, completed sweeps and
+ * counters {acc_metro, att_metro, acc_or, att_or}. Any pointer may be NULL. */
+int32_t scemc_download(const scemc_chain* c, double* config, double* energy, int64_t* sweep_index,
+                       int64_t* counters);
+/* _from_host!: replaces config and energy; seed, sweep_index, step and counters stay. */
+int32_t scemc_upload(scemc_chain* c, const double* config, double energy);
+/* Step (Metropolis rotation scale) of a chain. */
+int32_t scemc_set_step(scemc_chain* c, double step);
+/* _swap_payload!: exchanges config and energy between two single-replica chains on
+ * the same tables; seed, sweep_index, step and counters stay with each chain. */
+int32_t scemc_swap_payload(scemc_chain* a, scemc_chain* b);
+/* FP64 total energy of the device state (replica r of the chain or batch),
+ * deterministic fixed-order reduction. */
+int32_t scemc_total_energy(const scemc_ensemble* e, int32_t replica, double* energy);
+/* _renormalize!: normalises active spins, recomputes the FP64 energy of every
+ * replica, re-anchors the incremental energy. drift (per replica, may be NULL)
+ * receives |E_incremental - E_recomputed|. */
+int32_t scemc_renormalize(scemc_ensemble* e, double* drift);
+
+/* ---- batches: many replicas (PT rungs, temperatures, chains of uneven sizes) ---- */
+
+/* A batch over n_tables table sets with replicas[i] replicas each. Replica slots are
+ * numbered table-major (all replicas of table 0, then table 1, ...). configs holds
+ * 3 x n_sites(table) FP64 per slot in that order; energies, seeds and steps one per
+ * slot. */
+int32_t scemc_batch_create(int32_t n_tables, const scemc_tables* const* tables, const int32_t* replicas,
+                           const double* configs, const double* energies, const uint64_t* seeds,
+                           const double* steps, scemc_batch** out);
+int32_t scemc_batch_destroy(scemc_batch* b);
+int32_t scemc_batch_size(const scemc_batch* b, int32_t* n_slots, int64_t* n_sites_total);
+
+/* Run parameters of scemc_batch_run. Rung r of a ladder owns beta, step, seed and
+ * counters; the payload (spins + energy) it currently holds is slot slot_of_rung[r].
+ * Ladders are the replicas of one table set (exchange only within a table). */
+typedef struct scemc_run_params {
+  int64_t nsweeps;           /* compound sweeps to run */
+  int32_t or_per_metropolis; /* overrelaxation sweeps after each Metropolis sweep */
+  int32_t exchange;          /* 1: adjacent-rung swap attempts after every exchange_interval sweeps */
+  int64_t exchange_interval;
+  int64_t adapt_interval;    /* > 0: step adaptation every adapt_interval sweeps (thermalisation) */
+  double adapt_target;
+  int64_t renorm_interval;   /* > 0: renormalise + FP64 recompute every renorm_interval sweeps */
+  int64_t measure_interval;  /* > 0: record observables every measure_interval sweeps */
+  int32_t lanes_per_site;    /* 0 = autotuned */
+  int32_t mode;              /* 0 = auto, 1 = one launch per colour, 2 = persistent grid kernel */
+  /* Phase bookkeeping (the reference's lane.phase_sweeps): sweep i of this call is
+   * sweep phase_done + i of its phase; adaptation, renormalisation, measurement and
+   * exchange fire on that count, and no exchange follows the phase's last sweep
+   * (phase_total; 0 means phase_done + nsweeps). */
+  int64_t phase_done;
+  int64_t phase_total;
+} scemc_run_params;
+
+/* Inverse temperatures per rung (n_slots values, table-major like the slots). */
+int32_t scemc_batch_set_betas(scemc_batch* b, const double* betas);
+int32_t scemc_batch_set_steps(scemc_batch* b, const double* steps);
+int32_t scemc_batch_run(scemc_batch* b, const scemc_run_params* p);
+/* State readback. configs: 3 x n_sites per SLOT (payload order); energies per slot;
+ * slot_of_rung per rung; counters 4 per rung {acc_metro, att_metro, acc_or, att_or};
+ * swap counters 2 per rung pair {attempted, accepted} (pair r = rungs r, r+1 of one
+ * table; the last rung of each table has zeros); steps per rung; max_drift per rung. */
+int32_t scemc_batch_download(const scemc_batch* b, double* configs, double* energies, int32_t* slot_of_rung,
+                             int64_t* counters, int64_t* swaps, double* steps, double* max_drift);
+/* Resets the per-rung counters (acc/att metro, acc/att or, swaps) and max_drift. */
+int32_t scemc_batch_reset_counters(scemc_batch* b);
+/* Measurement records written by scemc_batch_run since the last fetch: n_records
+ * rows of (n_slots x record_len) FP64, indexed by RUNG, each
+ * {E, mx, my, mz, sub_x1, sub_y1, sub_z1, ...} with m over active sites and the
+ * sublattice sums per cell as in src/observables.jl:336-360. Pass rec = NULL to
+ * query the count and record_len; a fetch with rec clears the buffer. */
+int32_t scemc_batch_fetch_measurements(scemc_batch* b, double* rec, int64_t capacity, int64_t* n_records,
+                                       int32_t* record_len);
+
+/* Parity recording for the replay gate: with recording on, every pass of a sweep
+ * (pass -1 = Metropolis, 0..2 = overrelaxation passes) stores per site of replica
+ * slot 0 the proposal (3 FP32), the accept uniform, the FP32 dE and a flag
+ * (1 accepted, 0 rejected, 2 not attempted, 3 not visited). Turning it on clears
+ * the record. */
+int32_t scemc_batch_record(scemc_batch* b, int32_t on);
+int32_t scemc_batch_fetch_record(const scemc_batch* b, int32_t pass, float* prop, double* u, float* dE,
+                                 uint8_t* acc);
+
+/* Greedy proper colouring of the site-conflict graph in site order
+ * (hamiltonian.jl:456-499), host-side helper for table builders. 1-based inputs;
+ * colors_out receives one colour (1-based, 0 = inactive) per site; returns the
+ * number of colours in *n_colors. */
+int32_t scemc_color_sites(int32_t n_sites, const int32_t* site_ptr, const int32_t* site_inst,
+                          const int32_t* inst_ptr, const int32_t* inst_sites, const uint8_t* site_active,
+                          int32_t* colors_out, int32_t* n_colors);
+
+/* Failure-detection self test: runs the persistent kernel's grid barrier with one
+ * block that never arrives, bounded by limit_ns; returns SCEMC_ERR_TIMEOUT when the
+ * wait gives up as designed (SCEMC_OK would mean the bound did not fire). */
+int32_t scemc_selftest_barrier_timeout(int64_t limit_ns);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SCEMC_H */

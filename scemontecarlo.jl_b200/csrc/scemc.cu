@@ -1,0 +1,1801 @@
+// scemc.cu — libscemc_cuda.so: the chain-level colour-class Metropolis and
+// overrelaxation sweep of SCEMonteCarlo.jl, written for B200 (sm_100a).
+//
+// Design (see include/scemc.h for the ABI):
+//   * Tables. The reference's CSR-by-site tables (src/hamiltonian.jl:62-91,
+//     234-265) are compiled once into a device adjacency of 16-byte records
+//     {kind|offset, nb0, nb1, nb2}: one per (site, cluster instance), carrying the
+//     neighbour site ids of the other members in ascending slot order. Programs
+//     whose member l's are all in {1,2} and whose body order is <= 4 get a dense
+//     FP32 coefficient tensor (target m first, then the other members' m) and a
+//     fully unrolled contraction; every other program walks the reference's
+//     sparse entry list (sent_w / sent_tgt / sfac_*), so any model the reference
+//     accepts (lmax <= 6, any body order) runs.
+//   * State. Spins are FP32 float4, stored site-major / replica-minor
+//     (spins[site * R + r]) so that the replicas of one site sit in one 16*R-byte
+//     line: the records of a site are read once per warp (broadcast) and the
+//     neighbour gathers of consecutive replicas coalesce. Neighbour Z_lm rows are
+//     recomputed in registers from the gathered spins (no zrows array).
+//   * Sweep. Colour classes are processed in order; inside a class every
+//     (site, replica) item is independent. A group of G lanes (1..32) handles one
+//     item, striding over its records, and reduces the leave-one-out coefficient
+//     vector c (src/energy.jl:100-139) with warp shuffles. dE = sum_k c_k(znew_k -
+//     zold_k) in FP32 (energy.jl:148-157); the accept test uses FP64 exp.
+//     Two launch forms: one kernel per colour (graph-captured), or one persistent
+//     cooperative kernel per compound sweep with a bounded grid barrier between
+//     colours.
+//   * Energies. Accepted FP32 dE are converted to 2^-40 fixed point and summed in
+//     int64 (order-free, so the FP64 running energy is independent of the launch
+//     shape); FP64 is used for the running energy, the periodic full recompute
+//     (fixed 1024-instance chunks, fixed-order reduction) and the observables.
+#include "scemc.h"
+#include "scemc_device.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+using namespace scemc;
+
+namespace {
+
+thread_local std::string t_err;
+
+int32_t fail(int32_t code, const std::string& m) {
+  t_err = m;
+  return code;
+}
+
+#define CUDA_TRY(x)                                                                  \
+  do {                                                                               \
+    cudaError_t e_ = (x);                                                            \
+    if (e_ != cudaSuccess)                                                           \
+      return fail(SCEMC_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+enum Kind : int {
+  K_GEN = 0,
+  K_B1_L1 = 1,
+  K_B1_L2 = 2,
+  K_B2_11 = 3,
+  K_B2_12 = 4,
+  K_B2_21 = 5,
+  K_B2_22 = 6,
+  K_B3_111 = 7,
+  K_B4_1111 = 8
+};
+constexpr int kKindShift = 26;
+constexpr int32_t kOffMask = (1 << kKindShift) - 1;
+constexpr double kFixScale = 1099511627776.0;  // 2^40: fixed-point unit of dE sums
+constexpr int kMaxSlots = 512;
+constexpr int kChunk = 1024;  // fixed reduction chunk (sites or instances)
+constexpr int kMaxCellAtoms = 64;
+constexpr int kRecPasses = 4;  // replay record: Metropolis + up to 3 overrelaxation passes
+
+struct DevProg {
+  int32_t e_lo, e_hi;  // sparse entries, 0-based half-open
+  int32_t own_slot;    // 1-based member slot of the owning site
+  int32_t body;
+};
+
+struct DevLattice {
+  int32_t n_sites, nlm, lmax, n_colors, n_active, n_cell_atoms, R, slot0;
+  int64_t spin_off;  // float4 index of (site 0, replica 0)
+  int64_t n_inst;
+  const int32_t* adj_ptr;  // n_sites+1, 0-based
+  const int4* rec;
+  const DevProg* prog;
+  const float* tensor;
+  const float* sent_w;
+  const int8_t* sent_tgt;   // 0-based row
+  const int32_t* sfac_ptr;  // 0-based, n_sent+1
+  const int8_t* sfac_row;   // 0-based row
+  const int8_t* sfac_slot;  // 1-based member slot
+  const int32_t* inst_ptr;    // 0-based, n_inst+1
+  const int32_t* inst_sites;  // 0-based
+  const int32_t* color_ptr;    // 0-based, n_colors+1
+  const int32_t* color_sites;  // 0-based site ids
+  const uint8_t* has_l1;
+  const uint8_t* active;
+  // energy programs (FP64 recompute)
+  const int32_t* inst_term;  // 0-based
+  const int32_t* eprog_ptr;  // 0-based, n_terms+1
+  const double* eent_w;
+  const int32_t* efac_ptr;  // 0-based
+  const int8_t* efac_row;   // 0-based
+  const double* term_coef;
+};
+
+// Grid barrier state (one per ensemble).
+struct GridSync {
+  unsigned int count;
+  unsigned int gen;
+  int error;
+  int pad;
+};
+
+// Per-ensemble device scalars.
+struct EnsState {
+  int32_t exchange_parity;
+  int32_t exchange_count;
+  int32_t error;
+  int32_t pad;
+};
+
+struct SweepArgs {
+  const DevLattice* lat;
+  int32_t n_lat;
+  int32_t n_slots;
+  float4* spins;
+  const int32_t* seg;  // (max_colors) x (n_lat+1) item prefix per colour
+  int32_t max_colors;
+  int32_t colour;  // per-colour launch form
+  int32_t pass;    // -1 Metropolis, k >= 0 overrelaxation pass k
+  uint32_t sweep;  // 1-based counter word of this sweep
+  const int32_t* rung_of_slot;
+  const double* beta;   // per rung
+  const double* step;   // per rung
+  const unsigned long long* seed;  // per rung
+  unsigned long long* dE_fix;      // per slot
+  unsigned long long* cnt;         // per rung: [acc_metro, att_metro, acc_or, att_or]
+  GridSync* gs;
+  long long barrier_limit_ns;
+  // replay recording (slot 0 of lattice 0), may be null
+  float* rec_prop;
+  double* rec_u;
+  float* rec_dE;
+  uint8_t* rec_acc;
+};
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Sense-free generation barrier across all blocks of a cooperative launch. The
+// wait is bounded: after limit_ns it records an error and returns false; every
+// other block sees the flag and leaves too.
+__device__ __forceinline__ bool grid_barrier(GridSync* gs, unsigned int nblocks, long long limit_ns) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int* vgen = &gs->gen;
+    volatile int* verr = &gs->error;
+    int ok = *verr ? 0 : 1;  // a failed barrier poisons every later one
+    if (ok) {
+      const unsigned int g = *vgen;
+      __threadfence();
+      const unsigned int arrived = atomicAdd(&gs->count, 1u);
+      if (arrived == nblocks - 1) {
+        atomicExch(&gs->count, 0u);
+        __threadfence();
+        atomicAdd(&gs->gen, 1u);
+      } else {
+        const unsigned long long t0 = globaltimer();
+        while (*vgen == g) {
+          if (*verr) {
+            ok = 0;
+            break;
+          }
+          if ((long long)(globaltimer() - t0) > limit_ns) {
+            atomicExch(&gs->error, 1);
+            ok = 0;
+            break;
+          }
+          __nanosleep(64);
+        }
+      }
+      __threadfence();
+    }
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+template <bool PERSIST>
+__device__ __forceinline__ float4 load_spin(const float4* p) {
+  if (PERSIST) return __ldcg(p);  // spins change between colours inside the launch
+  return __ldg(p);
+}
+
+// Predicated add into a register array at a runtime index.
+template <int N>
+__device__ __forceinline__ void add_at(float* c, int k, float v) {
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+    if (i == k) c[i] += v;
+}
+
+// Leave-one-out coefficients of one site over records [j0 + lane, j1) step G.
+template <int LMAX, int G, bool PERSIST>
+__device__ __forceinline__ void accumulate_c(const DevLattice& L, const float4* __restrict__ sp, int R, int r,
+                                             int s, int lane, float* c) {
+  constexpr int NLM = (LMAX + 1) * (LMAX + 1);
+  const int j0 = L.adj_ptr[s], j1 = L.adj_ptr[s + 1];
+  for (int j = j0 + lane; j < j1; j += G) {
+    const int4 rc = __ldg(L.rec + j);
+    const int kind = (int)((unsigned)rc.x >> kKindShift);
+    const float* __restrict__ T = L.tensor + (rc.x & kOffMask);
+    if (LMAX >= 1 && kind == K_B2_11) {
+      const float4 n = load_spin<PERSIST>(sp + (int64_t)rc.y * R + r);
+      float z[3];
+      zrow_l1(n.x, n.y, n.z, z);
+#pragma unroll
+      for (int mt = 0; mt < 3; ++mt) {
+        float a = c[1 + mt];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) a = fmaf(__ldg(T + mt * 3 + m), z[m], a);
+        c[1 + mt] = a;
+      }
+    } else if (LMAX >= 1 && kind == K_B1_L1) {
+#pragma unroll
+      for (int mt = 0; mt < 3; ++mt) c[1 + mt] += __ldg(T + mt);
+    } else if (LMAX >= 1 && kind == K_B3_111) {
+      const float4 n1 = load_spin<PERSIST>(sp + (int64_t)rc.y * R + r);
+      const float4 n2 = load_spin<PERSIST>(sp + (int64_t)rc.z * R + r);
+      float z1[3], z2[3];
+      zrow_l1(n1.x, n1.y, n1.z, z1);
+      zrow_l1(n2.x, n2.y, n2.z, z2);
+#pragma unroll
+      for (int mt = 0; mt < 3; ++mt) {
+        float a = c[1 + mt];
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {
+          float t = 0.0f;
+#pragma unroll
+          for (int q = 0; q < 3; ++q) t = fmaf(__ldg(T + (mt * 3 + p) * 3 + q), z2[q], t);
+          a = fmaf(z1[p], t, a);
+        }
+        c[1 + mt] = a;
+      }
+    } else if (LMAX >= 1 && kind == K_B4_1111) {
+      const float4 n1 = load_spin<PERSIST>(sp + (int64_t)rc.y * R + r);
+      const float4 n2 = load_spin<PERSIST>(sp + (int64_t)rc.z * R + r);
+      const float4 n3 = load_spin<PERSIST>(sp + (int64_t)rc.w * R + r);
+      float z1[3], z2[3], z3[3];
+      zrow_l1(n1.x, n1.y, n1.z, z1);
+      zrow_l1(n2.x, n2.y, n2.z, z2);
+      zrow_l1(n3.x, n3.y, n3.z, z3);
+#pragma unroll
+      for (int mt = 0; mt < 3; ++mt) {
+        float a = c[1 + mt];
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {
+          float t2 = 0.0f;
+#pragma unroll
+          for (int q = 0; q < 3; ++q) {
+            float t3 = 0.0f;
+#pragma unroll
+            for (int u = 0; u < 3; ++u) t3 = fmaf(__ldg(T + ((mt * 3 + p) * 3 + q) * 3 + u), z3[u], t3);
+            t2 = fmaf(z2[q], t3, t2);
+          }
+          a = fmaf(z1[p], t2, a);
+        }
+        c[1 + mt] = a;
+      }
+    } else if (LMAX >= 2 && kind >= K_B2_12 && kind <= K_B2_22) {
+      const float4 n = load_spin<PERSIST>(sp + (int64_t)rc.y * R + r);
+      if (kind == K_B2_12) {  // target l=1, neighbour l=2
+        float z[5];
+        zrow_l2(n.x, n.y, n.z, z);
+#pragma unroll
+        for (int mt = 0; mt < 3; ++mt) {
+          float a = c[1 + mt];
+#pragma unroll
+          for (int m = 0; m < 5; ++m) a = fmaf(__ldg(T + mt * 5 + m), z[m], a);
+          c[1 + mt] = a;
+        }
+      } else if (kind == K_B2_21) {  // target l=2, neighbour l=1
+        float z[3];
+        zrow_l1(n.x, n.y, n.z, z);
+#pragma unroll
+        for (int mt = 0; mt < 5; ++mt) {
+          float a = c[4 + mt];
+#pragma unroll
+          for (int m = 0; m < 3; ++m) a = fmaf(__ldg(T + mt * 3 + m), z[m], a);
+          c[4 + mt] = a;
+        }
+      } else {  // K_B2_22
+        float z[5];
+        zrow_l2(n.x, n.y, n.z, z);
+#pragma unroll
+        for (int mt = 0; mt < 5; ++mt) {
+          float a = c[4 + mt];
+#pragma unroll
+          for (int m = 0; m < 5; ++m) a = fmaf(__ldg(T + mt * 5 + m), z[m], a);
+          c[4 + mt] = a;
+        }
+      }
+    } else if (LMAX >= 2 && kind == K_B1_L2) {
+#pragma unroll
+      for (int mt = 0; mt < 5; ++mt) c[4 + mt] += __ldg(T + mt);
+    } else {
+      // Sparse generic walk: the reference's program entries (energy.jl:126-135).
+      const DevProg pg = L.prog[rc.x & kOffMask];
+      int base = 0;
+      if (rc.y < 0) base = L.inst_ptr[-1 - rc.y];
+      for (int e = pg.e_lo; e < pg.e_hi; ++e) {
+        float p = 1.0f;
+        for (int f = L.sfac_ptr[e]; f < L.sfac_ptr[e + 1]; ++f) {
+          const int slot = L.sfac_slot[f];
+          int nb;
+          if (rc.y >= 0) {
+            const int idx = slot - 1 - (slot > pg.own_slot ? 1 : 0);
+            nb = idx == 0 ? rc.y : (idx == 1 ? rc.z : rc.w);
+          } else {
+            nb = L.inst_sites[base + slot - 1];
+          }
+          const float4 n = load_spin<PERSIST>(sp + (int64_t)nb * R + r);
+          p *= zval_f32(L.sfac_row[f], n.x, n.y, n.z);
+        }
+        add_at<NLM>(c, L.sent_tgt[e], L.sent_w[e] * p);
+      }
+    }
+  }
+}
+
+template <int NLM>
+__device__ __forceinline__ float delta_e(const float* c, const float* zo, const float* zn) {
+  float d = 0.0f;  // energy.jl:148-157 (row-difference form, zero coefficients skipped)
+#pragma unroll
+  for (int k = 0; k < NLM; ++k)
+    if (c[k] != 0.0f) d = fmaf(c[k], zn[k] - zo[k], d);
+  return d;
+}
+
+// Item enumeration of one colour: locate the lattice of a flat item index.
+__device__ __forceinline__ int find_lattice(const int32_t* seg_c, int n_lat, int item) {
+  int l = 0;
+  while (l + 1 < n_lat && item >= seg_c[l + 1]) ++l;
+  return l;
+}
+
+// Process colour `col` of the current pass: all (site, replica) items, G lanes each.
+// Block-local accumulators (shared) collect fixed-point dE and counters per slot.
+template <int LMAX, int G, bool PERSIST>
+__device__ void sweep_colour(const SweepArgs& a, int col, unsigned long long* s_dE, unsigned int* s_cnt) {
+  constexpr int NLM = (LMAX + 1) * (LMAX + 1);
+  const int32_t* seg_c = a.seg + (size_t)col * (a.n_lat + 1);
+  const int n_items = seg_c[a.n_lat];
+  const int lane = threadIdx.x % G;
+  const int group = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const int n_groups = (gridDim.x * blockDim.x) / G;
+  const int rounds = (n_items + n_groups - 1) / n_groups;
+  const unsigned int gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x % 32) / G * G));
+  for (int rd = 0; rd < rounds; ++rd) {
+    const int item = rd * n_groups + group;
+    const bool valid = item < n_items;
+    float c[NLM];
+#pragma unroll
+    for (int k = 0; k < NLM; ++k) c[k] = 0.0f;
+    int li = 0, slot = 0, s = 0, r = 0, R = 1;
+    const DevLattice* Lp = a.lat;
+    if (valid) {
+      li = find_lattice(seg_c, a.n_lat, item);
+      Lp = a.lat + li;
+      const int local = item - seg_c[li];
+      R = Lp->R;
+      const int q = local / R;
+      r = local - q * R;
+      s = Lp->color_sites[Lp->color_ptr[col] + q];
+      slot = Lp->slot0 + r;
+    }
+    const DevLattice& L = *Lp;
+    const float4* __restrict__ sp = a.spins + L.spin_off;
+    const bool do_or = a.pass >= 0;
+    const bool skip = !valid || (do_or && !L.has_l1[s]);
+    if (!skip) accumulate_c<LMAX, G, PERSIST>(L, sp, R, r, s, lane, c);
+    if (G > 1) {
+#pragma unroll
+      for (int o = G / 2; o >= 1; o >>= 1)
+#pragma unroll
+        for (int k = 0; k < NLM; ++k) c[k] += __shfl_xor_sync(gmask, c[k], o);
+    }
+    if (skip || lane != 0) continue;
+    const int rung = a.rung_of_slot[slot];
+    const double beta = a.beta[rung];
+    const float4 e = load_spin<PERSIST>(sp + (int64_t)s * R + r);
+    float px, py, pz;
+    double u;
+    bool attempted = true;
+    if (!do_or) {
+      u = keyed_proposal(a.seed[rung], (uint32_t)(s + 1), a.sweep, e.x, e.y, e.z, a.step[rung], px, py, pz);
+    } else {
+      // Reflection about the l = 1 field axis h = (c4, c2, c3) (updates.jl:66-87).
+      const double h0 = c[3], h1 = c[1], h2 = c[2];
+      const double hn = sqrt((h0 * h0 + h1 * h1) + h2 * h2);
+      if (hn < 1e-12) {
+        attempted = false;
+        px = e.x, py = e.y, pz = e.z;
+      } else {
+        const double a0 = h0 / hn, a1 = h1 / hn, a2 = h2 / hn;
+        const double d2 = 2.0 * (((double)e.x * a0 + (double)e.y * a1) + (double)e.z * a2);
+        double r0 = d2 * a0 - e.x, r1 = d2 * a1 - e.y, r2 = d2 * a2 - e.z;
+        const double rn = sqrt((r0 * r0 + r1 * r1) + r2 * r2);
+        px = (float)(r0 / rn);
+        py = (float)(r1 / rn);
+        pz = (float)(r2 / rn);
+      }
+      const Blk b = philox_block(a.seed[rung], (uint32_t)(s + 1), a.sweep, (uint32_t)a.pass, kTagOR);
+      u = philox_uniform(b.w0, b.w1);
+    }
+    float dE = 0.0f;
+    bool acc = false;
+    if (attempted) {
+      float zo[NLM], zn[NLM];
+      zrow_f32<LMAX>(e.x, e.y, e.z, zo);
+      zrow_f32<LMAX>(px, py, pz, zn);
+      dE = delta_e<NLM>(c, zo, zn);
+      acc = dE <= 0.0f || u < exp(-beta * (double)dE);
+    }
+    if (acc) {
+      a.spins[L.spin_off + (int64_t)s * R + r] = make_float4(px, py, pz, 0.0f);
+      const long long fx = llrint((double)dE * kFixScale);
+      atomicAdd(s_dE + slot, (unsigned long long)fx);
+    }
+    if (do_or) {
+      if (attempted) atomicAdd(s_cnt + 3 * slot + 2, 1u);
+      if (acc) atomicAdd(s_cnt + 3 * slot + 1, 1u);
+    } else if (acc) {
+      atomicAdd(s_cnt + 3 * slot + 0, 1u);
+    }
+    if (a.rec_prop != nullptr && li == 0 && r == 0 && a.pass + 1 < kRecPasses) {
+      const int64_t q = (int64_t)(a.pass + 1) * L.n_sites + s;
+      a.rec_prop[3 * q + 0] = px;
+      a.rec_prop[3 * q + 1] = py;
+      a.rec_prop[3 * q + 2] = pz;
+      a.rec_u[q] = u;
+      a.rec_dE[q] = dE;
+      a.rec_acc[q] = (uint8_t)(acc ? 1 : (attempted ? 0 : 2));
+    }
+  }
+}
+
+__device__ __forceinline__ void flush_block(const SweepArgs& a, unsigned long long* s_dE, unsigned int* s_cnt) {
+  __syncthreads();
+  for (int i = threadIdx.x; i < a.n_slots; i += blockDim.x) {
+    if (s_dE[i]) atomicAdd(a.dE_fix + i, s_dE[i]);
+    const int rung = a.rung_of_slot[i];
+    if (s_cnt[3 * i + 0]) atomicAdd(a.cnt + 4 * rung + 0, (unsigned long long)s_cnt[3 * i + 0]);
+    if (s_cnt[3 * i + 1]) atomicAdd(a.cnt + 4 * rung + 2, (unsigned long long)s_cnt[3 * i + 1]);
+    if (s_cnt[3 * i + 2]) atomicAdd(a.cnt + 4 * rung + 3, (unsigned long long)s_cnt[3 * i + 2]);
+    s_dE[i] = 0ull;
+    s_cnt[3 * i + 0] = s_cnt[3 * i + 1] = s_cnt[3 * i + 2] = 0u;
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void zero_block(int n_slots, unsigned long long* s_dE, unsigned int* s_cnt) {
+  for (int i = threadIdx.x; i < n_slots; i += blockDim.x) {
+    s_dE[i] = 0ull;
+    s_cnt[3 * i + 0] = s_cnt[3 * i + 1] = s_cnt[3 * i + 2] = 0u;
+  }
+  __syncthreads();
+}
+
+// One colour of one pass per launch.
+template <int LMAX, int G>
+__global__ void __launch_bounds__(256) k_sweep_colour(SweepArgs a) {
+  __shared__ unsigned long long s_dE[kMaxSlots];
+  __shared__ unsigned int s_cnt[3 * kMaxSlots];
+  zero_block(a.n_slots, s_dE, s_cnt);
+  sweep_colour<LMAX, G, false>(a, a.colour, s_dE, s_cnt);
+  flush_block(a, s_dE, s_cnt);
+}
+
+// One compound pass (every colour) per cooperative launch, bounded grid barrier
+// between colours.
+template <int LMAX, int G>
+__global__ void __launch_bounds__(256) k_sweep_persistent(SweepArgs a) {
+  __shared__ unsigned long long s_dE[kMaxSlots];
+  __shared__ unsigned int s_cnt[3 * kMaxSlots];
+  zero_block(a.n_slots, s_dE, s_cnt);
+  for (int col = 0; col < a.max_colors; ++col) {
+    sweep_colour<LMAX, G, true>(a, col, s_dE, s_cnt);
+    if (col + 1 < a.max_colors)
+      if (!grid_barrier(a.gs, gridDim.x, a.barrier_limit_ns)) break;
+  }
+  flush_block(a, s_dE, s_cnt);
+}
+
+// Barrier self-test: nblocks_expected = gridDim.x + 1 can never be reached.
+__global__ void k_barrier_selftest(GridSync* gs, long long limit_ns) {
+  grid_barrier(gs, gridDim.x + 1, limit_ns);
+}
+
+struct TailArgs {
+  int32_t n_slots, n_rungs, n_lat;
+  const DevLattice* lat;
+  double* energy;               // per slot
+  unsigned long long* dE_fix;   // per slot
+  unsigned long long* cnt;      // per rung x4
+  unsigned long long* win;      // per rung x2 adaptation window {acc, att}
+  int add_att;                  // add n_active to att_metro (a Metropolis pass ran)
+  int adapt;                    // adapt the step now
+  double adapt_target;
+  double* step;                 // per rung
+  int exchange;                 // attempt swaps now
+  int32_t* slot_of_rung;
+  int32_t* rung_of_slot;
+  const double* beta;
+  unsigned long long* swaps;    // per rung x2 {att, acc}
+  uint64_t exchange_seed;
+  EnsState* st;
+};
+
+// Energy fold, counters, adaptation and replica exchange (one block).
+// Exchange: src/gpu/gpu_pt.jl:129-134 schedule with the swap rule of src/pt.jl:92-96.
+__global__ void k_tail(TailArgs t) {
+  for (int i = threadIdx.x; i < t.n_slots; i += blockDim.x) {
+    const long long fx = (long long)t.dE_fix[i];
+    t.dE_fix[i] = 0ull;
+    t.energy[i] += (double)fx / kFixScale;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  for (int li = 0; li < t.n_lat; ++li) {
+    const DevLattice& L = t.lat[li];
+    for (int k = 0; k < L.R; ++k) {
+      const int rung = L.slot0 + k;
+      if (t.add_att) {
+        t.cnt[4 * rung + 1] += (unsigned long long)L.n_active;
+        t.win[2 * rung + 1] += (unsigned long long)L.n_active;
+      }
+    }
+  }
+  // acceptance window for adaptation = metro counters since the last adaptation
+  if (t.adapt) {
+    for (int rung = 0; rung < t.n_rungs; ++rung) {
+      const unsigned long long att = t.win[2 * rung + 1];
+      const unsigned long long acc = t.cnt[4 * rung + 0] - t.win[2 * rung + 0];
+      if (att > 0) {
+        const double a = (double)acc / (double)att;
+        double s = t.step[rung] * exp(0.5 * (a - t.adapt_target));
+        s = s < 1e-3 ? 1e-3 : (s > 3.141592653589793 ? 3.141592653589793 : s);
+        t.step[rung] = s;
+      }
+      t.win[2 * rung + 0] = t.cnt[4 * rung + 0];
+      t.win[2 * rung + 1] = 0ull;
+    }
+  }
+  if (t.exchange) {
+    const int parity = t.st->exchange_parity;
+    const int count = ++t.st->exchange_count;
+    for (int li = 0; li < t.n_lat; ++li) {
+      const DevLattice& L = t.lat[li];
+      for (int i = parity; i < L.R - 1; i += 2) {
+        const int ra = L.slot0 + i, rb = ra + 1;
+        const Blk b = philox_block(t.exchange_seed, (uint32_t)(i + 1), (uint32_t)count, (uint32_t)li, kTagExchange);
+        const double u = philox_uniform(b.w0, b.w1);
+        const int sa = t.slot_of_rung[ra], sb = t.slot_of_rung[rb];
+        const double logw = (t.beta[ra] - t.beta[rb]) * (t.energy[sa] - t.energy[sb]);
+        t.swaps[2 * ra + 0] += 1ull;
+        if (u < exp(logw < 0.0 ? logw : 0.0)) {
+          t.slot_of_rung[ra] = sb;
+          t.slot_of_rung[rb] = sa;
+          t.rung_of_slot[sb] = ra;
+          t.rung_of_slot[sa] = rb;
+          t.swaps[2 * ra + 1] += 1ull;
+        }
+      }
+    }
+    t.st->exchange_parity = 1 - parity;
+  }
+}
+
+// ---- FP64 energy recompute and renormalisation ------------------------------
+
+// Partial energies of fixed 1024-instance chunks for every slot of lattice li.
+// grid: (chunks, R); block 256 (each thread 4 instances, fixed-order reduction).
+__global__ void __launch_bounds__(256) k_energy_chunks(const DevLattice* lat, int li, const float4* spins,
+                                                       double* partial, int n_chunks) {
+  const DevLattice& L = lat[li];
+  const int chunk = blockIdx.x, r = blockIdx.y;
+  const float4* sp = spins + L.spin_off;
+  double acc = 0.0;
+  for (int k = 0; k < kChunk / 256; ++k) {
+    const int64_t i = (int64_t)chunk * kChunk + k * 256 + threadIdx.x;
+    if (i >= L.n_inst) break;
+    const int t = L.inst_term[i];
+    const int off = L.inst_ptr[i];
+    double Ei = 0.0;
+    for (int e = L.eprog_ptr[t]; e < L.eprog_ptr[t + 1]; ++e) {
+      double p = 1.0;
+      const int f0 = L.efac_ptr[e], nf = L.efac_ptr[e + 1] - f0;
+      for (int m = 0; m < nf; ++m) {
+        const float4 v = sp[(int64_t)L.inst_sites[off + m] * L.R + r];
+        p *= zval_f64(L.efac_row[f0 + m], (double)v.x, (double)v.y, (double)v.z);
+      }
+      Ei += L.eent_w[e] * p;
+    }
+    acc += L.term_coef[t] * Ei;
+  }
+  __shared__ double red[256];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = 128; o >= 1; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[(size_t)r * n_chunks + chunk] = red[0];
+}
+
+// Sum chunk partials in order; mode 0: write E_out; mode 1: renormalisation
+// (drift, max_drift, re-anchor the running energy).
+__global__ void k_energy_fold(const DevLattice* lat, int li, const double* partial, int n_chunks, double* energy,
+                              double* e_out, double* drift, double* max_drift, const int32_t* rung_of_slot,
+                              int mode) {
+  const DevLattice& L = lat[li];
+  const int r = threadIdx.x;
+  if (r >= L.R) return;
+  double E = 0.0;
+  for (int c = 0; c < n_chunks; ++c) E += partial[(size_t)r * n_chunks + c];
+  const int slot = L.slot0 + r;
+  if (e_out) e_out[slot] = E;
+  if (mode == 1) {
+    const double d = fabs(energy[slot] - E);
+    const int rung = rung_of_slot[slot];
+    if (drift) drift[slot] = d;
+    if (d > max_drift[rung] || d != d) max_drift[rung] = d;
+    energy[slot] = E;
+  }
+}
+
+// Normalise active spins in FP64 and round to FP32 (state.jl:168-175).
+__global__ void k_normalize(const DevLattice* lat, int li, float4* spins) {
+  const DevLattice& L = lat[li];
+  const int64_t n = (int64_t)L.n_sites * L.R;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int s = (int)(i / L.R);
+    if (!L.active[s]) continue;
+    float4 v = spins[L.spin_off + i];
+    const double x = v.x, y = v.y, z = v.z;
+    const double nn = sqrt((x * x + y * y) + z * z);
+    spins[L.spin_off + i] = make_float4((float)(x / nn), (float)(y / nn), (float)(z / nn), 0.0f);
+  }
+}
+
+// ---- measurements (observables.jl:303-360) -----------------------------------
+
+// Partial sums per (chunk, replica): {m_x, m_y, m_z} over active sites and the
+// sublattice sums {x_a, y_a, z_a}; record layout per slot: 3 + 3*n_cell_atoms.
+__global__ void __launch_bounds__(256) k_measure_chunks(const DevLattice* lat, int li, const float4* spins,
+                                                        double* partial, int n_chunks, int rlen) {
+  const DevLattice& L = lat[li];
+  const int chunk = blockIdx.x, r = blockIdx.y;
+  const int A = L.n_cell_atoms;
+  __shared__ double red[256][4];
+  __shared__ double out[3 + 3 * kMaxCellAtoms];
+  for (int k = threadIdx.x; k < 3 + 3 * A; k += blockDim.x) out[k] = 0.0;
+  __syncthreads();
+  // each thread sums sites of one sublattice at a time: sites of chunk are
+  // [chunk*1024, +1024); sublattice a = s % A.
+  for (int a = 0; a < A; ++a) {
+    double sx = 0, sy = 0, sz = 0, dummy = 0;
+    for (int k = 0; k < kChunk / 256; ++k) {
+      const int s = chunk * kChunk + k * 256 + threadIdx.x;
+      if (s >= L.n_sites || (s % A) != a || !L.active[s]) continue;
+      const float4 v = spins[L.spin_off + (int64_t)s * L.R + r];
+      sx += v.x, sy += v.y, sz += v.z;
+    }
+    red[threadIdx.x][0] = sx, red[threadIdx.x][1] = sy, red[threadIdx.x][2] = sz, red[threadIdx.x][3] = dummy;
+    __syncthreads();
+    for (int o = 128; o >= 1; o >>= 1) {
+      if (threadIdx.x < o)
+        for (int q = 0; q < 3; ++q) red[threadIdx.x][q] += red[threadIdx.x + o][q];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      for (int q = 0; q < 3; ++q) {
+        out[3 + 3 * a + q] = red[0][q];
+        out[q] += red[0][q];
+      }
+    }
+    __syncthreads();
+  }
+  for (int k = threadIdx.x; k < 3 + 3 * A; k += blockDim.x)
+    partial[((size_t)r * n_chunks + chunk) * rlen + k] = out[k];
+}
+
+// Fold the chunk partials in order into one record row per rung:
+// {E, m_x, m_y, m_z, sub...} (m averaged over active sites, sub over cells).
+__global__ void k_measure_fold(const DevLattice* lat, int li, const double* partial, int n_chunks, int rlen,
+                               const double* energy, const int32_t* rung_of_slot, double* rec_row,
+                               int rec_len) {
+  const DevLattice& L = lat[li];
+  const int r = blockIdx.x;
+  const int slot = L.slot0 + r;
+  const int rung = rung_of_slot[slot];
+  const int A = L.n_cell_atoms;
+  const double ncells = (double)(L.n_sites / A);
+  for (int k = threadIdx.x; k < 3 + 3 * A; k += blockDim.x) {
+    double v = 0.0;
+    for (int c = 0; c < n_chunks; ++c) v += partial[((size_t)r * n_chunks + c) * rlen + k];
+    const double outv = k < 3 ? v / (double)L.n_active : v / ncells;
+    rec_row[(size_t)rung * rec_len + 1 + k] = outv;
+  }
+  if (threadIdx.x == 0) rec_row[(size_t)rung * rec_len] = energy[slot];
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+template <typename T>
+int32_t upload(std::vector<void*>& allocs, const std::vector<T>& v, const T** out) {
+  void* p = nullptr;
+  const size_t bytes = std::max<size_t>(v.size() * sizeof(T), 16);
+  CUDA_TRY(cudaMalloc(&p, bytes));
+  allocs.push_back(p);
+  if (!v.empty()) CUDA_TRY(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  *out = static_cast<const T*>(p);
+  return SCEMC_OK;
+}
+
+}  // namespace
+
+struct scemc_tables {
+  int device = 0;
+  DevLattice dl{};
+  std::vector<void*> allocs;
+  std::vector<int32_t> color_ptr;  // 0-based host copy
+  std::vector<uint8_t> active;
+  int32_t n_sites = 0, nlm = 0, lmax = 0, n_colors = 0, n_active = 0, n_cell_atoms = 1;
+  int64_t n_inst = 0;
+  double d_mean = 0, a_mean = 0;
+  int64_t bytes = 0;
+  ~scemc_tables() {
+    for (void* p : allocs) cudaFree(p);
+  }
+};
+
+struct scemc_ensemble {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<const scemc_tables*> tabs;
+  std::vector<int32_t> R;          // replicas per table
+  std::vector<int32_t> slot0;      // first slot per table
+  std::vector<int64_t> spin_off;   // float4 offset per table
+  int32_t n_slots = 0;
+  int64_t n_spins = 0;
+  int32_t lmax = 0;
+  int32_t max_colors = 0;
+  int64_t sweep_index = 0;
+  uint64_t exchange_seed = 0x5ce3c0ffee5eedull;
+  // device
+  DevLattice* d_lat = nullptr;
+  float4* d_spins = nullptr;
+  int32_t* d_seg = nullptr;
+  std::vector<int32_t> seg;  // host copy
+  double* d_energy = nullptr;
+  unsigned long long* d_dEfix = nullptr;
+  unsigned long long* d_cnt = nullptr;
+  unsigned long long* d_win = nullptr;
+  unsigned long long* d_swaps = nullptr;
+  double* d_beta = nullptr;
+  double* d_step = nullptr;
+  unsigned long long* d_seed = nullptr;
+  int32_t* d_slot_of_rung = nullptr;
+  int32_t* d_rung_of_slot = nullptr;
+  double* d_max_drift = nullptr;
+  double* d_drift = nullptr;
+  double* d_eout = nullptr;
+  GridSync* d_gs = nullptr;
+  EnsState* d_st = nullptr;
+  double* d_partial = nullptr;
+  size_t partial_cap = 0;
+  // measurements
+  double* d_meas = nullptr;
+  int64_t meas_cap = 0, meas_n = 0;
+  int32_t rec_len = 0;
+  // replay record
+  bool recording = false;
+  float* d_rprop = nullptr;
+  double* d_ru = nullptr;
+  float* d_rdE = nullptr;
+  uint8_t* d_racc = nullptr;
+  long long barrier_limit_ns = 2000000000ll;
+  int coop_blocks = 0;  // cached co-resident grid size for the persistent form
+  int coop_G = -1;
+  ~scemc_ensemble() {
+    void* ps[] = {d_lat,   d_spins, d_seg,  d_energy,       d_dEfix,        d_cnt,       d_win,    d_swaps,
+                  d_beta,  d_step,  d_seed, d_slot_of_rung, d_rung_of_slot, d_max_drift, d_drift,  d_eout,
+                  d_gs,    d_st,    d_partial, d_meas,      d_rprop,        d_ru,        d_rdE,    d_racc};
+    for (void* p : ps)
+      if (p) cudaFree(p);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+// ---- table compilation --------------------------------------------------------
+int32_t check_ptr(const int32_t* p, int64_t n, int64_t first, int64_t last, const char* name) {
+  if (!p) return fail(SCEMC_ERR_ARG, std::string(name) + " is NULL");
+  if (p[0] != first) return fail(SCEMC_ERR_ARG, std::string(name) + "[1] must be " + std::to_string(first));
+  for (int64_t i = 0; i < n; ++i)
+    if (p[i + 1] < p[i]) return fail(SCEMC_ERR_ARG, std::string(name) + " is not monotone");
+  if (p[n] != last) return fail(SCEMC_ERR_ARG, std::string(name) + " does not end at its array length + 1");
+  return SCEMC_OK;
+}
+
+int32_t compile_tables(const scemc_tables_desc* d, scemc_tables* T) {
+  if (!d) return fail(SCEMC_ERR_ARG, "desc is NULL");
+  if (d->lmax > 6) return fail(SCEMC_ERR_UNSUPPORTED, "lmax = " + std::to_string(d->lmax) +
+                                                         " unsupported on the device path (<= 6)");
+  if (d->lmax < 0 || d->nlm != (d->lmax + 1) * (d->lmax + 1))
+    return fail(SCEMC_ERR_ARG, "nlm must equal (lmax+1)^2");
+  if (d->n_sites < 1 || d->n_colors < 0 || d->n_cell_atoms < 1 || d->n_cell_atoms > kMaxCellAtoms ||
+      d->n_sites % d->n_cell_atoms != 0)
+    return fail(SCEMC_ERR_ARG, "bad n_sites / n_colors / n_cell_atoms");
+  const int32_t ns = d->n_sites;
+  int32_t rc;
+  if ((rc = check_ptr(d->site_ptr, ns, 1, d->n_adj + 1, "site_ptr"))) return rc;
+  if ((rc = check_ptr(d->inst_ptr, d->n_inst, 1, d->n_inst_sites + 1, "inst_ptr"))) return rc;
+  if ((rc = check_ptr(d->sprog_ptr, d->n_sprog, 1, d->n_sent + 1, "sprog_ptr"))) return rc;
+  if ((rc = check_ptr(d->sfac_ptr, d->n_sent, 1, d->n_sfac + 1, "sfac_ptr"))) return rc;
+  if ((rc = check_ptr(d->eprog_ptr, d->n_terms, 1, d->n_eent + 1, "eprog_ptr"))) return rc;
+  if ((rc = check_ptr(d->efac_ptr, d->n_eent, 1, d->n_efac + 1, "efac_ptr"))) return rc;
+  if ((rc = check_ptr(d->color_ptr, d->n_colors, 1, d->n_active + 1, "color_ptr"))) return rc;
+  if (!d->term_body || !d->term_ls || !d->site_inst || !d->site_slot || !d->inst_term || !d->inst_sites ||
+      !d->site_prog || !d->sent_w || !d->sent_tgt || !d->sfac_row || !d->sfac_slot || !d->eent_w ||
+      !d->efac_row || !d->term_coef || !d->color_sites || !d->site_has_l1 || !d->site_active)
+    return fail(SCEMC_ERR_ARG, "a table pointer is NULL");
+  // templates -> program ids
+  std::vector<int32_t> pbase(d->n_terms + 1, 0), lsbase(d->n_terms + 1, 0);
+  for (int64_t k = 0; k < d->n_terms; ++k) {
+    if (d->term_body[k] < 1) return fail(SCEMC_ERR_ARG, "term_body must be >= 1");
+    pbase[k + 1] = pbase[k] + d->term_body[k];
+    lsbase[k + 1] = lsbase[k] + d->term_body[k];
+  }
+  if (pbase[d->n_terms] != d->n_sprog) return fail(SCEMC_ERR_ARG, "sum(term_body) != number of site programs");
+  for (int64_t k = 0; k < lsbase[d->n_terms]; ++k)
+    if (d->term_ls[k] < 0 || d->term_ls[k] > d->lmax) return fail(SCEMC_ERR_ARG, "term_ls outside 0:lmax");
+  for (int64_t e = 0; e < d->n_sent; ++e)
+    if (d->sent_tgt[e] < 1 || d->sent_tgt[e] > d->nlm) return fail(SCEMC_ERR_ARG, "sent_tgt outside 1:nlm");
+  for (int64_t f = 0; f < d->n_sfac; ++f)
+    if (d->sfac_row[f] < 1 || d->sfac_row[f] > d->nlm) return fail(SCEMC_ERR_ARG, "sfac_row outside 1:nlm");
+  for (int64_t f = 0; f < d->n_efac; ++f)
+    if (d->efac_row[f] < 1 || d->efac_row[f] > d->nlm) return fail(SCEMC_ERR_ARG, "efac_row outside 1:nlm");
+  for (int64_t i = 0; i < d->n_inst; ++i)
+    if (d->inst_term[i] < 1 || d->inst_term[i] > d->n_terms) return fail(SCEMC_ERR_ARG, "inst_term out of range");
+  for (int64_t q = 0; q < d->n_inst_sites; ++q)
+    if (d->inst_sites[q] < 1 || d->inst_sites[q] > ns) return fail(SCEMC_ERR_ARG, "inst_sites out of range");
+  for (int64_t q = 0; q < d->n_active; ++q)
+    if (d->color_sites[q] < 1 || d->color_sites[q] > ns) return fail(SCEMC_ERR_ARG, "color_sites out of range");
+  for (int64_t i = 0; i < d->n_inst; ++i) {
+    const int32_t k = d->inst_term[i] - 1;
+    if (d->inst_ptr[i + 1] - d->inst_ptr[i] != d->term_body[k])
+      return fail(SCEMC_ERR_ARG, "instance size differs from its template's body order");
+  }
+  // programs: kind + dense tensor (fast kinds), sparse descriptors (all)
+  std::vector<int32_t> prog_kind(d->n_sprog, K_GEN), prog_toff(d->n_sprog, 0);
+  std::vector<DevProg> progs(d->n_sprog);
+  std::vector<float> tensor;
+  for (int64_t k = 0; k < d->n_terms; ++k) {
+    const int D = d->term_body[k];
+    const int32_t* ls = d->term_ls + lsbase[k];
+    for (int v = 1; v <= D; ++v) {
+      const int32_t pid = pbase[k] + v - 1;  // 0-based
+      DevProg pg;
+      pg.e_lo = d->sprog_ptr[pid] - 1;
+      pg.e_hi = d->sprog_ptr[pid + 1] - 1;
+      pg.own_slot = v;
+      pg.body = D;
+      progs[pid] = pg;
+      // factor l's in ascending slot order excluding v
+      int lf[8];
+      int nf = 0;
+      bool small = D <= 4;
+      for (int q = 1; q <= D && small; ++q)
+        if (q != v) lf[nf++] = ls[q - 1];
+      const int lt = ls[v - 1];
+      int kind = K_GEN;
+      if (small) {
+        auto in12 = [](int l) { return l == 1 || l == 2; };
+        bool ok = in12(lt);
+        for (int q = 0; q < nf; ++q) ok = ok && in12(lf[q]);
+        if (ok) {
+          if (D == 1) kind = lt == 1 ? K_B1_L1 : K_B1_L2;
+          else if (D == 2) kind = lt == 1 ? (lf[0] == 1 ? K_B2_11 : K_B2_12) : (lf[0] == 1 ? K_B2_21 : K_B2_22);
+          else if (D == 3 && lt == 1 && lf[0] == 1 && lf[1] == 1) kind = K_B3_111;
+          else if (D == 4 && lt == 1 && lf[0] == 1 && lf[1] == 1 && lf[2] == 1) kind = K_B4_1111;
+        }
+      }
+      if (kind != K_GEN) {
+        int dims[4];
+        dims[0] = 2 * lt + 1;
+        int size = dims[0];
+        for (int q = 0; q < nf; ++q) {
+          dims[q + 1] = 2 * lf[q] + 1;
+          size *= dims[q + 1];
+        }
+        const int32_t off = (int32_t)tensor.size();
+        tensor.resize(tensor.size() + size, 0.0f);
+        for (int e = pg.e_lo; e < pg.e_hi; ++e) {
+          int idx = d->sent_tgt[e] - 1 - lt * lt;
+          const int f0 = d->sfac_ptr[e] - 1, f1 = d->sfac_ptr[e + 1] - 1;
+          if (f1 - f0 != nf) return fail(SCEMC_ERR_ARG, "program entry factor count differs from body - 1");
+          for (int f = f0; f < f1; ++f) {
+            const int q = f - f0;
+            const int m = d->sfac_row[f] - 1 - lf[q] * lf[q];
+            if (m < 0 || m >= dims[q + 1]) return fail(SCEMC_ERR_ARG, "factor row outside its l block");
+            idx = idx * dims[q + 1] + m;
+          }
+          if (idx < 0 || idx >= size) return fail(SCEMC_ERR_ARG, "target row outside its l block");
+          tensor[off + idx] += (float)d->sent_w[e];
+        }
+        if (off > kOffMask) return fail(SCEMC_ERR_UNSUPPORTED, "coefficient tensors too large");
+        prog_toff[pid] = off;
+      }
+      prog_kind[pid] = kind;
+    }
+  }
+  if (d->n_sprog > kOffMask) return fail(SCEMC_ERR_UNSUPPORTED, "too many site programs");
+  // adjacency records
+  std::vector<int4> rec(d->n_adj);
+  std::vector<int32_t> adj_ptr(ns + 1);
+  int64_t d_sum = 0, a_sum = 0;
+  std::vector<int32_t> seen;
+  for (int32_t s = 0; s < ns; ++s) {
+    adj_ptr[s] = d->site_ptr[s] - 1;
+    seen.clear();
+    for (int64_t j = d->site_ptr[s] - 1; j < d->site_ptr[s + 1] - 1; ++j) {
+      const int32_t inst = d->site_inst[j] - 1;
+      if (inst < 0 || inst >= d->n_inst) return fail(SCEMC_ERR_ARG, "site_inst out of range");
+      const int32_t pid = d->site_prog[j] - 1;
+      if (pid < 0 || pid >= d->n_sprog) return fail(SCEMC_ERR_ARG, "site_prog out of range");
+      const int32_t k = d->inst_term[inst] - 1;
+      const int D = d->term_body[k];
+      const int own = d->site_slot[j];
+      if (own < 1 || own > D || pid != pbase[k] + own - 1)
+        return fail(SCEMC_ERR_ARG, "site_prog/site_slot inconsistent with the instance's template");
+      if (d->inst_sites[d->inst_ptr[inst] - 1 + own - 1] != s + 1)
+        return fail(SCEMC_ERR_ARG, "site_slot does not point back at the site");
+      int4 r4;
+      const int kind = prog_kind[pid];
+      r4.x = (kind << kKindShift) | (kind == K_GEN ? pid : prog_toff[pid]);
+      r4.y = r4.z = r4.w = -1;
+      if (D <= 4) {
+        int nb[3] = {-1, -1, -1}, q = 0;
+        for (int sl = 1; sl <= D; ++sl) {
+          if (sl == own) continue;
+          nb[q++] = d->inst_sites[d->inst_ptr[inst] - 1 + sl - 1] - 1;
+        }
+        r4.y = nb[0], r4.z = nb[1], r4.w = nb[2];
+        for (int t = 0; t < q; ++t) seen.push_back(nb[t]);
+      } else {
+        r4.y = -1 - inst;
+        for (int sl = 1; sl <= D; ++sl)
+          if (sl != own) seen.push_back(d->inst_sites[d->inst_ptr[inst] - 1 + sl - 1] - 1);
+      }
+      rec[j] = r4;
+    }
+    if (d->site_active[s]) {
+      std::sort(seen.begin(), seen.end());
+      d_sum += std::unique(seen.begin(), seen.end()) - seen.begin();
+      a_sum += d->site_ptr[s + 1] - d->site_ptr[s];
+    }
+  }
+  adj_ptr[ns] = (int32_t)d->n_adj;
+  // 0-based copies of the remaining tables
+  auto rebase = [](const int32_t* p, int64_t n) {
+    std::vector<int32_t> v(n);
+    for (int64_t i = 0; i < n; ++i) v[i] = p[i] - 1;
+    return v;
+  };
+  std::vector<float> sent_w(d->n_sent);
+  std::vector<int8_t> sent_tgt(d->n_sent), sfac_row(d->n_sfac), sfac_slot(d->n_sfac), efac_row(d->n_efac);
+  for (int64_t e = 0; e < d->n_sent; ++e) {
+    sent_w[e] = (float)d->sent_w[e];
+    sent_tgt[e] = (int8_t)(d->sent_tgt[e] - 1);
+  }
+  for (int64_t f = 0; f < d->n_sfac; ++f) {
+    sfac_row[f] = (int8_t)(d->sfac_row[f] - 1);
+    sfac_slot[f] = d->sfac_slot[f];
+  }
+  for (int64_t f = 0; f < d->n_efac; ++f) efac_row[f] = (int8_t)(d->efac_row[f] - 1);
+  std::vector<int4> rec_v = rec;
+  std::vector<uint8_t> has_l1(d->site_has_l1, d->site_has_l1 + ns), active(d->site_active, d->site_active + ns);
+  std::vector<double> eent_w(d->eent_w, d->eent_w + d->n_eent), term_coef(d->term_coef, d->term_coef + d->n_terms);
+  DevLattice& L = T->dl;
+  L.n_sites = ns;
+  L.nlm = d->nlm;
+  L.lmax = d->lmax;
+  L.n_colors = d->n_colors;
+  L.n_active = d->n_active;
+  L.n_cell_atoms = d->n_cell_atoms;
+  L.n_inst = d->n_inst;
+  int32_t r = 0;
+  if ((r = upload(T->allocs, adj_ptr, &L.adj_ptr))) return r;
+  if ((r = upload(T->allocs, rec_v, &L.rec))) return r;
+  if ((r = upload(T->allocs, progs, &L.prog))) return r;
+  if ((r = upload(T->allocs, tensor, &L.tensor))) return r;
+  if ((r = upload(T->allocs, sent_w, &L.sent_w))) return r;
+  if ((r = upload(T->allocs, sent_tgt, &L.sent_tgt))) return r;
+  if ((r = upload(T->allocs, rebase(d->sfac_ptr, d->n_sent + 1), &L.sfac_ptr))) return r;
+  if ((r = upload(T->allocs, sfac_row, &L.sfac_row))) return r;
+  if ((r = upload(T->allocs, sfac_slot, &L.sfac_slot))) return r;
+  if ((r = upload(T->allocs, rebase(d->inst_ptr, d->n_inst + 1), &L.inst_ptr))) return r;
+  if ((r = upload(T->allocs, rebase(d->inst_sites, d->n_inst_sites), &L.inst_sites))) return r;
+  std::vector<int32_t> cp = rebase(d->color_ptr, d->n_colors + 1);
+  if ((r = upload(T->allocs, cp, &L.color_ptr))) return r;
+  if ((r = upload(T->allocs, rebase(d->color_sites, d->n_active), &L.color_sites))) return r;
+  if ((r = upload(T->allocs, has_l1, &L.has_l1))) return r;
+  if ((r = upload(T->allocs, active, &L.active))) return r;
+  if ((r = upload(T->allocs, rebase(d->inst_term, d->n_inst), &L.inst_term))) return r;
+  if ((r = upload(T->allocs, rebase(d->eprog_ptr, d->n_terms + 1), &L.eprog_ptr))) return r;
+  if ((r = upload(T->allocs, eent_w, &L.eent_w))) return r;
+  if ((r = upload(T->allocs, rebase(d->efac_ptr, d->n_eent + 1), &L.efac_ptr))) return r;
+  if ((r = upload(T->allocs, efac_row, &L.efac_row))) return r;
+  if ((r = upload(T->allocs, term_coef, &L.term_coef))) return r;
+  T->color_ptr = cp;
+  T->active = active;
+  T->n_sites = ns;
+  T->nlm = d->nlm;
+  T->lmax = d->lmax;
+  T->n_colors = d->n_colors;
+  T->n_active = d->n_active;
+  T->n_cell_atoms = d->n_cell_atoms;
+  T->n_inst = d->n_inst;
+  T->d_mean = d->n_active ? (double)d_sum / d->n_active : 0.0;
+  T->a_mean = d->n_active ? (double)a_sum / d->n_active : 0.0;
+  T->bytes = (int64_t)(rec_v.size() * 16 + adj_ptr.size() * 4 + tensor.size() * 4 + sent_w.size() * 6 +
+                       d->n_inst_sites * 4 + d->n_inst * 8);
+  return SCEMC_OK;
+}
+
+// ---- ensemble helpers ----------------------------------------------------------
+template <typename T>
+int32_t dalloc(T** p, size_t n) {
+  CUDA_TRY(cudaMalloc((void**)p, std::max<size_t>(n * sizeof(T), 16)));
+  CUDA_TRY(cudaMemset(*p, 0, std::max<size_t>(n * sizeof(T), 16)));
+  return SCEMC_OK;
+}
+
+bool finite3(const double* v) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]); }
+
+int32_t upload_config(scemc_ensemble* E, int ti, int r, const double* config) {
+  const scemc_tables* T = E->tabs[ti];
+  const int R = E->R[ti];
+  std::vector<float4> tmp(T->n_sites);
+  for (int s = 0; s < T->n_sites; ++s) {
+    if (!finite3(config + 3 * s)) return fail(SCEMC_ERR_NUMERIC, "spin column " + std::to_string(s + 1) + " is not finite");
+    tmp[s] = make_float4((float)config[3 * s], (float)config[3 * s + 1], (float)config[3 * s + 2], 0.0f);
+  }
+  // strided copy into spins[spin_off + s*R + r]
+  CUDA_TRY(cudaMemcpy2DAsync(E->d_spins + E->spin_off[ti] + r, sizeof(float4) * R, tmp.data(), sizeof(float4),
+                             sizeof(float4), T->n_sites, cudaMemcpyHostToDevice, E->stream));
+  CUDA_TRY(cudaStreamSynchronize(E->stream));
+  return SCEMC_OK;
+}
+
+int32_t download_config(const scemc_ensemble* E, int ti, int r, double* config) {
+  const scemc_tables* T = E->tabs[ti];
+  const int R = E->R[ti];
+  std::vector<float4> tmp(T->n_sites);
+  CUDA_TRY(cudaMemcpy2DAsync(tmp.data(), sizeof(float4), E->d_spins + E->spin_off[ti] + r, sizeof(float4) * R,
+                             sizeof(float4), T->n_sites, cudaMemcpyDeviceToHost, E->stream));
+  CUDA_TRY(cudaStreamSynchronize(E->stream));
+  for (int s = 0; s < T->n_sites; ++s) {
+    config[3 * s] = tmp[s].x;
+    config[3 * s + 1] = tmp[s].y;
+    config[3 * s + 2] = tmp[s].z;
+  }
+  return SCEMC_OK;
+}
+
+int32_t create_ensemble(int32_t n_tables, const scemc_tables* const* tables, const int32_t* replicas,
+                        const double* configs, const double* energies, const uint64_t* seeds, const double* steps,
+                        scemc_ensemble** out) {
+  if (!out) return fail(SCEMC_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  if (n_tables < 1 || !tables || !replicas || !configs || !energies || !seeds || !steps)
+    return fail(SCEMC_ERR_ARG, "bad batch arguments");
+  auto* E = new scemc_ensemble();
+  std::unique_ptr<scemc_ensemble> guard(E);
+  CUDA_TRY(cudaGetDevice(&E->device));
+  CUDA_TRY(cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking));
+  int64_t off = 0;
+  int32_t slots = 0;
+  for (int i = 0; i < n_tables; ++i) {
+    if (!tables[i]) return fail(SCEMC_ERR_ARG, "a table set is NULL");
+    if (replicas[i] < 1) return fail(SCEMC_ERR_ARG, "replicas must be >= 1");
+    E->tabs.push_back(tables[i]);
+    E->R.push_back(replicas[i]);
+    E->slot0.push_back(slots);
+    E->spin_off.push_back(off);
+    off += (int64_t)tables[i]->n_sites * replicas[i];
+    slots += replicas[i];
+    E->lmax = std::max(E->lmax, tables[i]->lmax);
+    E->max_colors = std::max(E->max_colors, tables[i]->n_colors);
+  }
+  if (slots > kMaxSlots) return fail(SCEMC_ERR_ARG, "at most 512 replica slots per batch");
+  E->n_slots = slots;
+  E->n_spins = off;
+  for (int i = 0; i < slots; ++i)
+    if (!(steps[i] > 0) || !std::isfinite(energies[i])) return fail(SCEMC_ERR_ARG, "step must be > 0 and energy finite");
+  int32_t rc;
+  if ((rc = dalloc(&E->d_spins, off))) return rc;
+  // lattice descriptors with per-batch geometry
+  std::vector<DevLattice> lats(n_tables);
+  int max_atoms = 1;
+  for (int i = 0; i < n_tables; ++i) {
+    lats[i] = tables[i]->dl;
+    lats[i].R = replicas[i];
+    lats[i].slot0 = E->slot0[i];
+    lats[i].spin_off = E->spin_off[i];
+    max_atoms = std::max(max_atoms, tables[i]->n_cell_atoms);
+  }
+  if ((rc = dalloc(&E->d_lat, n_tables))) return rc;
+  CUDA_TRY(cudaMemcpy(E->d_lat, lats.data(), sizeof(DevLattice) * n_tables, cudaMemcpyHostToDevice));
+  // per-colour item prefixes
+  E->seg.assign((size_t)std::max(E->max_colors, 1) * (n_tables + 1), 0);
+  for (int c = 0; c < E->max_colors; ++c) {
+    int64_t acc = 0;
+    for (int i = 0; i < n_tables; ++i) {
+      E->seg[(size_t)c * (n_tables + 1) + i] = (int32_t)acc;
+      const scemc_tables* T = tables[i];
+      if (c < T->n_colors) acc += (int64_t)(T->color_ptr[c + 1] - T->color_ptr[c]) * replicas[i];
+    }
+    if (acc > 0x7fffffffll) return fail(SCEMC_ERR_UNSUPPORTED, "more than 2^31 items in one colour class");
+    E->seg[(size_t)c * (n_tables + 1) + n_tables] = (int32_t)acc;
+  }
+  if ((rc = dalloc(&E->d_seg, E->seg.size()))) return rc;
+  CUDA_TRY(cudaMemcpy(E->d_seg, E->seg.data(), E->seg.size() * 4, cudaMemcpyHostToDevice));
+  if ((rc = dalloc(&E->d_energy, slots)) || (rc = dalloc(&E->d_dEfix, slots)) || (rc = dalloc(&E->d_cnt, 4 * slots)) ||
+      (rc = dalloc(&E->d_win, 2 * slots)) || (rc = dalloc(&E->d_swaps, 2 * slots)) ||
+      (rc = dalloc(&E->d_beta, slots)) || (rc = dalloc(&E->d_step, slots)) || (rc = dalloc(&E->d_seed, slots)) ||
+      (rc = dalloc(&E->d_slot_of_rung, slots)) || (rc = dalloc(&E->d_rung_of_slot, slots)) ||
+      (rc = dalloc(&E->d_max_drift, slots)) || (rc = dalloc(&E->d_drift, slots)) ||
+      (rc = dalloc(&E->d_eout, slots)) || (rc = dalloc(&E->d_gs, 1)) || (rc = dalloc(&E->d_st, 1)))
+    return rc;
+  std::vector<int32_t> ident(slots);
+  for (int i = 0; i < slots; ++i) ident[i] = i;
+  CUDA_TRY(cudaMemcpy(E->d_slot_of_rung, ident.data(), 4 * slots, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(E->d_rung_of_slot, ident.data(), 4 * slots, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(E->d_energy, energies, 8 * slots, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(E->d_step, steps, 8 * slots, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(E->d_seed, seeds, 8 * slots, cudaMemcpyHostToDevice));
+  std::vector<double> ones(slots, 1.0);
+  CUDA_TRY(cudaMemcpy(E->d_beta, ones.data(), 8 * slots, cudaMemcpyHostToDevice));
+  E->rec_len = 4 + 3 * max_atoms;
+  const double* cfg = configs;
+  for (int i = 0; i < n_tables; ++i)
+    for (int r = 0; r < replicas[i]; ++r) {
+      if ((rc = upload_config(E, i, r, cfg))) return rc;
+      cfg += 3 * (size_t)tables[i]->n_sites;
+    }
+  *out = guard.release();
+  return SCEMC_OK;
+}
+
+// Sweep launch ----------------------------------------------------------------
+using KFn = void (*)(SweepArgs);
+
+template <int LMAX>
+KFn pick_colour(int G) {
+  switch (G) {
+    case 1: return k_sweep_colour<LMAX, 1>;
+    case 2: return k_sweep_colour<LMAX, 2>;
+    case 4: return k_sweep_colour<LMAX, 4>;
+    case 8: return k_sweep_colour<LMAX, 8>;
+    case 16: return k_sweep_colour<LMAX, 16>;
+    default: return k_sweep_colour<LMAX, 32>;
+  }
+}
+template <int LMAX>
+KFn pick_persist(int G) {
+  switch (G) {
+    case 1: return k_sweep_persistent<LMAX, 1>;
+    case 2: return k_sweep_persistent<LMAX, 2>;
+    case 4: return k_sweep_persistent<LMAX, 4>;
+    case 8: return k_sweep_persistent<LMAX, 8>;
+    case 16: return k_sweep_persistent<LMAX, 16>;
+    default: return k_sweep_persistent<LMAX, 32>;
+  }
+}
+
+KFn kernel_for(int lmax, int G, bool persist) {
+  switch (lmax) {
+    case 0: return persist ? pick_persist<0>(G) : pick_colour<0>(G);
+    case 1: return persist ? pick_persist<1>(G) : pick_colour<1>(G);
+    case 2: return persist ? pick_persist<2>(G) : pick_colour<2>(G);
+    case 3: return persist ? pick_persist<3>(G) : pick_colour<3>(G);
+    case 4: return persist ? pick_persist<4>(G) : pick_colour<4>(G);
+    case 5: return persist ? pick_persist<5>(G) : pick_colour<5>(G);
+    default: return persist ? pick_persist<6>(G) : pick_colour<6>(G);
+  }
+}
+
+int norm_lanes(int lanes) {
+  if (lanes <= 1) return 1;
+  int g = 1;
+  while (g < lanes && g < 32) g <<= 1;
+  return g;
+}
+
+SweepArgs make_args(scemc_ensemble* E, int pass) {
+  SweepArgs a{};
+  a.lat = E->d_lat;
+  a.n_lat = (int32_t)E->tabs.size();
+  a.n_slots = E->n_slots;
+  a.spins = E->d_spins;
+  a.seg = E->d_seg;
+  a.max_colors = E->max_colors;
+  a.pass = pass;
+  a.sweep = (uint32_t)(E->sweep_index + 1);
+  a.rung_of_slot = E->d_rung_of_slot;
+  a.beta = E->d_beta;
+  a.step = E->d_step;
+  a.seed = E->d_seed;
+  a.dE_fix = E->d_dEfix;
+  a.cnt = E->d_cnt;
+  a.gs = E->d_gs;
+  a.barrier_limit_ns = E->barrier_limit_ns;
+  if (E->recording) {
+    a.rec_prop = E->d_rprop;
+    a.rec_u = E->d_ru;
+    a.rec_dE = E->d_rdE;
+    a.rec_acc = E->d_racc;
+  }
+  return a;
+}
+
+int sm_count(int dev) {
+  int n = 0;
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n > 0 ? n : 1;
+}
+
+// One pass (Metropolis or OR pass k) over every colour.
+int32_t run_pass(scemc_ensemble* E, int pass, int G, int mode) {
+  const int lmax = E->lmax;
+  const int threads = 256;
+  SweepArgs a = make_args(E, pass);
+  if (mode == 2) {
+    KFn fn = kernel_for(lmax, G, true);
+    if (E->coop_G != G) {
+      int per_sm = 0;
+      CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, threads, 0));
+      if (per_sm < 1) return fail(SCEMC_ERR_CUDA, "persistent sweep kernel cannot be resident");
+      E->coop_blocks = per_sm * sm_count(E->device);
+      E->coop_G = G;
+    }
+    // no more blocks than there are item groups in the widest colour
+    int max_items = 1;
+    for (int c = 0; c < E->max_colors; ++c)
+      max_items = std::max(max_items, E->seg[(size_t)c * (E->tabs.size() + 1) + E->tabs.size()]);
+    const int want = (int)std::min<int64_t>(E->coop_blocks, ((int64_t)max_items * G + threads - 1) / threads);
+    const int blocks = std::max(1, want);
+    void* params[] = {&a};
+    CUDA_TRY(cudaLaunchCooperativeKernel((const void*)fn, dim3(blocks), dim3(threads), params, 0, E->stream));
+    return SCEMC_OK;
+  }
+  KFn fn = kernel_for(lmax, G, false);
+  const int cap = sm_count(E->device) * 8;
+  for (int c = 0; c < E->max_colors; ++c) {
+    const int n = E->seg[(size_t)c * (E->tabs.size() + 1) + E->tabs.size()];
+    if (n == 0) continue;
+    a.colour = c;
+    const int blocks = (int)std::min<int64_t>(cap, ((int64_t)n * G + threads - 1) / threads);
+    fn<<<std::max(blocks, 1), threads, 0, E->stream>>>(a);
+    CUDA_TRY(cudaGetLastError());
+  }
+  return SCEMC_OK;
+}
+
+int32_t launch_tail(scemc_ensemble* E, bool add_att, bool adapt, double target, bool exchange) {
+  TailArgs t{};
+  t.n_slots = E->n_slots;
+  t.n_rungs = E->n_slots;
+  t.n_lat = (int32_t)E->tabs.size();
+  t.lat = E->d_lat;
+  t.energy = E->d_energy;
+  t.dE_fix = E->d_dEfix;
+  t.cnt = E->d_cnt;
+  t.win = E->d_win;
+  t.add_att = add_att;
+  t.adapt = adapt;
+  t.adapt_target = target;
+  t.step = E->d_step;
+  t.exchange = exchange;
+  t.slot_of_rung = E->d_slot_of_rung;
+  t.rung_of_slot = E->d_rung_of_slot;
+  t.beta = E->d_beta;
+  t.swaps = E->d_swaps;
+  t.exchange_seed = E->exchange_seed;
+  t.st = E->d_st;
+  k_tail<<<1, 128, 0, E->stream>>>(t);
+  CUDA_TRY(cudaGetLastError());
+  return SCEMC_OK;
+}
+
+int32_t ensure_partial(scemc_ensemble* E, size_t n) {
+  if (E->partial_cap >= n) return SCEMC_OK;
+  if (E->d_partial) cudaFree(E->d_partial);
+  E->d_partial = nullptr;
+  int32_t rc;
+  if ((rc = dalloc(&E->d_partial, n))) return rc;
+  E->partial_cap = n;
+  return SCEMC_OK;
+}
+
+// FP64 recompute for every slot. mode 0: energies into d_eout; mode 1: renormalise.
+int32_t recompute(scemc_ensemble* E, int mode) {
+  for (size_t li = 0; li < E->tabs.size(); ++li) {
+    const scemc_tables* T = E->tabs[li];
+    const int R = E->R[li];
+    if (mode == 1) {
+      const int64_t n = (int64_t)T->n_sites * R;
+      const int blocks = (int)std::min<int64_t>(sm_count(E->device) * 4, (n + 255) / 256);
+      k_normalize<<<std::max(blocks, 1), 256, 0, E->stream>>>(E->d_lat, (int)li, E->d_spins);
+      CUDA_TRY(cudaGetLastError());
+    }
+    const int n_chunks = (int)std::max<int64_t>(1, (T->n_inst + kChunk - 1) / kChunk);
+    int32_t rc;
+    if ((rc = ensure_partial(E, (size_t)n_chunks * R))) return rc;
+    k_energy_chunks<<<dim3(n_chunks, R), 256, 0, E->stream>>>(E->d_lat, (int)li, E->d_spins, E->d_partial, n_chunks);
+    CUDA_TRY(cudaGetLastError());
+    k_energy_fold<<<1, 512, 0, E->stream>>>(E->d_lat, (int)li, E->d_partial, n_chunks, E->d_energy, E->d_eout,
+                                            E->d_drift, E->d_max_drift, E->d_rung_of_slot, mode);
+    CUDA_TRY(cudaGetLastError());
+  }
+  return SCEMC_OK;
+}
+
+int32_t ensure_meas(scemc_ensemble* E, int64_t rows) {
+  if (E->meas_n + rows <= E->meas_cap) return SCEMC_OK;
+  const int64_t cap = std::max<int64_t>(E->meas_cap * 2, E->meas_n + rows + 64);
+  double* p = nullptr;
+  int32_t rc;
+  if ((rc = dalloc(&p, (size_t)cap * E->n_slots * E->rec_len))) return rc;
+  if (E->d_meas && E->meas_n > 0)
+    CUDA_TRY(cudaMemcpyAsync(p, E->d_meas, sizeof(double) * E->meas_n * E->n_slots * E->rec_len,
+                             cudaMemcpyDeviceToDevice, E->stream));
+  CUDA_TRY(cudaStreamSynchronize(E->stream));
+  if (E->d_meas) cudaFree(E->d_meas);
+  E->d_meas = p;
+  E->meas_cap = cap;
+  return SCEMC_OK;
+}
+
+int32_t measure(scemc_ensemble* E) {
+  int32_t rc;
+  if ((rc = ensure_meas(E, 1))) return rc;
+  double* row = E->d_meas + (size_t)E->meas_n * E->n_slots * E->rec_len;
+  for (size_t li = 0; li < E->tabs.size(); ++li) {
+    const scemc_tables* T = E->tabs[li];
+    const int R = E->R[li];
+    const int n_chunks = (T->n_sites + kChunk - 1) / kChunk;
+    const int rlen = 3 + 3 * T->n_cell_atoms;
+    if ((rc = ensure_partial(E, (size_t)n_chunks * R * rlen))) return rc;
+    k_measure_chunks<<<dim3(n_chunks, R), 256, 0, E->stream>>>(E->d_lat, (int)li, E->d_spins, E->d_partial, n_chunks,
+                                                               rlen);
+    CUDA_TRY(cudaGetLastError());
+    k_measure_fold<<<R, 128, 0, E->stream>>>(E->d_lat, (int)li, E->d_partial, n_chunks, rlen, E->d_energy,
+                                             E->d_rung_of_slot, row, E->rec_len);
+    CUDA_TRY(cudaGetLastError());
+  }
+  E->meas_n += 1;
+  return SCEMC_OK;
+}
+
+int32_t check_error(scemc_ensemble* E) {
+  GridSync gs;
+  CUDA_TRY(cudaMemcpyAsync(&gs, E->d_gs, sizeof(gs), cudaMemcpyDeviceToHost, E->stream));
+  CUDA_TRY(cudaStreamSynchronize(E->stream));
+  if (gs.error) {
+    GridSync z{};
+    cudaMemcpy(E->d_gs, &z, sizeof(z), cudaMemcpyHostToDevice);
+    return fail(SCEMC_ERR_TIMEOUT, "grid barrier wait gave up (bounded spin); state of this sweep is torn");
+  }
+  return SCEMC_OK;
+}
+
+int auto_lanes(const scemc_ensemble* E) {
+  // Items per colour vs. ~16 resident warps per SM: give each item more lanes when
+  // a colour class alone cannot fill the device.
+  int64_t items = 0;
+  for (int c = 0; c < E->max_colors; ++c)
+    items = std::max<int64_t>(items, E->seg[(size_t)c * (E->tabs.size() + 1) + E->tabs.size()]);
+  const int64_t target = (int64_t)sm_count(E->device) * 1024;
+  int G = 1;
+  while (G < 32 && items * G < target) G <<= 1;
+  return G;
+}
+
+int32_t sweep_once(scemc_ensemble* E, int n_or, int G, int mode) {
+  if (E->sweep_index >= 0x7ffffffell - 1)
+    return fail(SCEMC_ERR_EXHAUSTED, "sweep_index exhausted the 32-bit RNG counter word");
+  int32_t rc;
+  if ((rc = run_pass(E, -1, G, mode))) return rc;
+  for (int k = 0; k < n_or; ++k)
+    if ((rc = run_pass(E, k, G, mode))) return rc;
+  return SCEMC_OK;
+}
+
+}  // namespace
+
+// =============================================================================
+// C ABI
+// =============================================================================
+extern "C" {
+
+int32_t scemc_last_error(char* buf, size_t len) {
+  if (!buf || len == 0) return SCEMC_ERR_ARG;
+  std::snprintf(buf, len, "%s", t_err.c_str());
+  return SCEMC_OK;
+}
+
+int32_t scemc_version(void) { return 100; }
+
+int32_t scemc_tables_create(const scemc_tables_desc* desc, scemc_tables** out) {
+  if (!out) return fail(SCEMC_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  auto* T = new scemc_tables();
+  cudaGetDevice(&T->device);
+  const int32_t rc = compile_tables(desc, T);
+  if (rc != SCEMC_OK) {
+    delete T;
+    return rc;
+  }
+  *out = T;
+  return SCEMC_OK;
+}
+
+int32_t scemc_tables_destroy(scemc_tables* t) {
+  delete t;
+  return SCEMC_OK;
+}
+
+int32_t scemc_tables_stats(const scemc_tables* t, double* d_mean, double* a_mean, int64_t* bytes) {
+  if (!t) return fail(SCEMC_ERR_ARG, "tables is NULL");
+  if (d_mean) *d_mean = t->d_mean;
+  if (a_mean) *a_mean = t->a_mean;
+  if (bytes) *bytes = t->bytes;
+  return SCEMC_OK;
+}
+
+int32_t scemc_chain_create(const scemc_tables* t, const double* config, double energy, uint64_t seed, double step,
+                           scemc_chain** out) {
+  const int32_t one = 1;
+  return create_ensemble(1, &t, &one, config, &energy, &seed, &step, out);
+}
+
+int32_t scemc_chain_destroy(scemc_chain* c) {
+  delete c;
+  return SCEMC_OK;
+}
+
+int32_t scemc_batch_create(int32_t n_tables, const scemc_tables* const* tables, const int32_t* replicas,
+                           const double* configs, const double* energies, const uint64_t* seeds, const double* steps,
+                           scemc_batch** out) {
+  return create_ensemble(n_tables, tables, replicas, configs, energies, seeds, steps, out);
+}
+
+int32_t scemc_batch_destroy(scemc_batch* b) {
+  delete b;
+  return SCEMC_OK;
+}
+
+int32_t scemc_batch_size(const scemc_batch* b, int32_t* n_slots, int64_t* n_sites_total) {
+  if (!b) return fail(SCEMC_ERR_ARG, "batch is NULL");
+  if (n_slots) *n_slots = b->n_slots;
+  if (n_sites_total) *n_sites_total = b->n_spins;
+  return SCEMC_OK;
+}
+
+static int32_t check_single(const scemc_ensemble* c, const scemc_tables* t) {
+  if (!c) return fail(SCEMC_ERR_ARG, "chain is NULL");
+  if (c->n_slots != 1 || c->tabs.size() != 1) return fail(SCEMC_ERR_ARG, "expected a single-replica chain");
+  if (t && c->tabs[0] != t) return fail(SCEMC_ERR_ARG, "chain was created on other tables");
+  return SCEMC_OK;
+}
+
+static int32_t check_lanes(int32_t lanes) {
+  if (lanes < 1 || (lanes & (lanes - 1)) != 0)
+    return fail(SCEMC_ERR_ARG, "lanes_per_site must be a power of two (got " + std::to_string(lanes) + ")");
+  return SCEMC_OK;
+}
+
+int32_t scemc_metropolis_sweep(scemc_chain* c, const scemc_tables* t, double beta, int32_t lanes_per_site,
+                               int64_t* n_accepted) {
+  int32_t rc;
+  if ((rc = check_single(c, t)) || (rc = check_lanes(lanes_per_site))) return rc;
+  if (!std::isfinite(beta)) return fail(SCEMC_ERR_ARG, "beta must be finite");
+  CUDA_TRY(cudaMemcpyAsync(c->d_beta, &beta, 8, cudaMemcpyHostToDevice, c->stream));
+  unsigned long long before = 0;
+  CUDA_TRY(cudaMemcpyAsync(&before, c->d_cnt, 8, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if ((rc = sweep_once(c, 0, norm_lanes(lanes_per_site), 1))) return rc;
+  if ((rc = launch_tail(c, true, false, 0.5, false))) return rc;
+  unsigned long long after = 0;
+  CUDA_TRY(cudaMemcpyAsync(&after, c->d_cnt, 8, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->sweep_index += 1;
+  if (n_accepted) *n_accepted = (int64_t)(after - before);
+  return SCEMC_OK;
+}
+
+int32_t scemc_overrelaxation_sweep(scemc_chain* c, const scemc_tables* t, double beta, int32_t lanes_per_site,
+                                   int64_t* n_accepted, int64_t* n_attempted) {
+  int32_t rc;
+  if ((rc = check_single(c, t)) || (rc = check_lanes(lanes_per_site))) return rc;
+  if (!std::isfinite(beta)) return fail(SCEMC_ERR_ARG, "beta must be finite");
+  if (c->sweep_index >= 0x7ffffffell - 1)
+    return fail(SCEMC_ERR_EXHAUSTED, "sweep_index exhausted the 32-bit RNG counter word");
+  CUDA_TRY(cudaMemcpyAsync(c->d_beta, &beta, 8, cudaMemcpyHostToDevice, c->stream));
+  unsigned long long before[4], after[4];
+  CUDA_TRY(cudaMemcpyAsync(before, c->d_cnt, 32, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  // a stand-alone OR sweep uses pass 0 of the next sweep counter word
+  if ((rc = run_pass(c, 0, norm_lanes(lanes_per_site), 1))) return rc;
+  if ((rc = launch_tail(c, false, false, 0.5, false))) return rc;
+  CUDA_TRY(cudaMemcpyAsync(after, c->d_cnt, 32, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->sweep_index += 1;
+  if (n_accepted) *n_accepted = (int64_t)(after[2] - before[2]);
+  if (n_attempted) *n_attempted = (int64_t)(after[3] - before[3]);
+  return SCEMC_OK;
+}
+
+int32_t scemc_run_sweeps(scemc_chain* c, const scemc_tables* t, double beta, int64_t nsweeps, int64_t renorm_interval,
+                         int32_t lanes_per_site) {
+  int32_t rc;
+  if ((rc = check_single(c, t)) || (rc = check_lanes(lanes_per_site))) return rc;
+  if (!std::isfinite(beta) || nsweeps < 0) return fail(SCEMC_ERR_ARG, "bad beta or nsweeps");
+  CUDA_TRY(cudaMemcpyAsync(c->d_beta, &beta, 8, cudaMemcpyHostToDevice, c->stream));
+  const int G = norm_lanes(lanes_per_site);
+  for (int64_t i = 1; i <= nsweeps; ++i) {
+    if ((rc = sweep_once(c, 0, G, 1))) return rc;
+    if ((rc = launch_tail(c, true, false, 0.5, false))) return rc;
+    c->sweep_index += 1;
+    if (renorm_interval > 0 && i % renorm_interval == 0)
+      if ((rc = recompute(c, 1))) return rc;
+  }
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return check_error(c);
+}
+
+int32_t scemc_download(const scemc_chain* c, double* config, double* energy, int64_t* sweep_index,
+                       int64_t* counters) {
+  int32_t rc;
+  if ((rc = check_single(c, nullptr))) return rc;
+  if (config)
+    if ((rc = download_config(c, 0, 0, config))) return rc;
+  if (energy) CUDA_TRY(cudaMemcpy(energy, c->d_energy, 8, cudaMemcpyDeviceToHost));
+  if (sweep_index) *sweep_index = c->sweep_index;
+  if (counters) {
+    unsigned long long v[4];
+    CUDA_TRY(cudaMemcpy(v, c->d_cnt, 32, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < 4; ++i) counters[i] = (int64_t)v[i];
+  }
+  return SCEMC_OK;
+}
+
+int32_t scemc_upload(scemc_chain* c, const double* config, double energy) {
+  int32_t rc;
+  if ((rc = check_single(c, nullptr))) return rc;
+  if (!config || !std::isfinite(energy)) return fail(SCEMC_ERR_ARG, "config NULL or energy not finite");
+  if ((rc = upload_config(c, 0, 0, config))) return rc;
+  CUDA_TRY(cudaMemcpy(c->d_energy, &energy, 8, cudaMemcpyHostToDevice));
+  return SCEMC_OK;
+}
+
+int32_t scemc_set_step(scemc_chain* c, double step) {
+  int32_t rc;
+  if ((rc = check_single(c, nullptr))) return rc;
+  if (!(step > 0) || !std::isfinite(step)) return fail(SCEMC_ERR_ARG, "step must be > 0");
+  CUDA_TRY(cudaMemcpy(c->d_step, &step, 8, cudaMemcpyHostToDevice));
+  return SCEMC_OK;
+}
+
+int32_t scemc_swap_payload(scemc_chain* a, scemc_chain* b) {
+  int32_t rc;
+  if ((rc = check_single(a, nullptr)) || (rc = check_single(b, nullptr))) return rc;
+  if (a->tabs[0] != b->tabs[0]) return fail(SCEMC_ERR_ARG, "chains live on different tables");
+  if (a == b) return SCEMC_OK;
+  CUDA_TRY(cudaStreamSynchronize(a->stream));
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  std::swap(a->d_spins, b->d_spins);
+  double ea, eb;
+  CUDA_TRY(cudaMemcpy(&ea, a->d_energy, 8, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(&eb, b->d_energy, 8, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(a->d_energy, &eb, 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(b->d_energy, &ea, 8, cudaMemcpyHostToDevice));
+  return SCEMC_OK;
+}
+
+int32_t scemc_total_energy(const scemc_ensemble* e, int32_t replica, double* energy) {
+  if (!e || !energy) return fail(SCEMC_ERR_ARG, "NULL argument");
+  if (replica < 0 || replica >= e->n_slots) return fail(SCEMC_ERR_ARG, "replica out of range");
+  auto* E = const_cast<scemc_ensemble*>(e);
+  int32_t rc;
+  if ((rc = recompute(E, 0))) return rc;
+  CUDA_TRY(cudaMemcpyAsync(energy, E->d_eout + replica, 8, cudaMemcpyDeviceToHost, E->stream));
+  CUDA_TRY(cudaStreamSynchronize(E->stream));
+  return SCEMC_OK;
+}
+
+int32_t scemc_renormalize(scemc_ensemble* e, double* drift) {
+  if (!e) return fail(SCEMC_ERR_ARG, "NULL argument");
+  int32_t rc;
+  if ((rc = recompute(e, 1))) return rc;
+  if (drift) CUDA_TRY(cudaMemcpyAsync(drift, e->d_drift, 8 * e->n_slots, cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return SCEMC_OK;
+}
+
+int32_t scemc_batch_set_betas(scemc_batch* b, const double* betas) {
+  if (!b || !betas) return fail(SCEMC_ERR_ARG, "NULL argument");
+  for (int i = 0; i < b->n_slots; ++i)
+    if (!std::isfinite(betas[i])) return fail(SCEMC_ERR_ARG, "beta must be finite");
+  CUDA_TRY(cudaMemcpy(b->d_beta, betas, 8 * b->n_slots, cudaMemcpyHostToDevice));
+  return SCEMC_OK;
+}
+
+int32_t scemc_batch_set_steps(scemc_batch* b, const double* steps) {
+  if (!b || !steps) return fail(SCEMC_ERR_ARG, "NULL argument");
+  for (int i = 0; i < b->n_slots; ++i)
+    if (!(steps[i] > 0)) return fail(SCEMC_ERR_ARG, "step must be > 0");
+  CUDA_TRY(cudaMemcpy(b->d_step, steps, 8 * b->n_slots, cudaMemcpyHostToDevice));
+  return SCEMC_OK;
+}
+
+int32_t scemc_batch_run(scemc_batch* b, const scemc_run_params* p) {
+  if (!b || !p) return fail(SCEMC_ERR_ARG, "NULL argument");
+  if (p->nsweeps < 0 || p->or_per_metropolis < 0 || (p->exchange && p->exchange_interval < 1))
+    return fail(SCEMC_ERR_ARG, "bad run parameters");
+  if (p->lanes_per_site != 0) {
+    int32_t rc = check_lanes(p->lanes_per_site);
+    if (rc) return rc;
+  }
+  const int G = p->lanes_per_site ? norm_lanes(p->lanes_per_site) : auto_lanes(b);
+  const int mode = p->mode == 0 ? 2 : p->mode;
+  if (p->phase_done < 0 || p->phase_total < 0) return fail(SCEMC_ERR_ARG, "bad phase bookkeeping");
+  const int64_t total = p->phase_total > 0 ? p->phase_total : p->phase_done + p->nsweeps;
+  int32_t rc;
+  for (int64_t k = 1; k <= p->nsweeps; ++k) {
+    const int64_t i = p->phase_done + k;
+    if ((rc = sweep_once(b, p->or_per_metropolis, G, mode))) return rc;
+    b->sweep_index += 1;
+    const bool adapt = p->adapt_interval > 0 && i % p->adapt_interval == 0;
+    if ((rc = launch_tail(b, true, adapt, p->adapt_target, false))) return rc;
+    if (p->renorm_interval > 0 && i % p->renorm_interval == 0)
+      if ((rc = recompute(b, 1))) return rc;
+    if (p->measure_interval > 0 && i % p->measure_interval == 0)
+      if ((rc = measure(b))) return rc;
+    if (p->exchange && i % p->exchange_interval == 0 && i < total)
+      if ((rc = launch_tail(b, false, false, 0.5, true))) return rc;
+  }
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  return check_error(b);
+}
+
+int32_t scemc_batch_download(const scemc_batch* b, double* configs, double* energies, int32_t* slot_of_rung,
+                             int64_t* counters, int64_t* swaps, double* steps, double* max_drift) {
+  if (!b) return fail(SCEMC_ERR_ARG, "batch is NULL");
+  int32_t rc;
+  if (configs) {
+    double* cfg = configs;
+    for (size_t i = 0; i < b->tabs.size(); ++i)
+      for (int r = 0; r < b->R[i]; ++r) {
+        if ((rc = download_config(b, (int)i, r, cfg))) return rc;
+        cfg += 3 * (size_t)b->tabs[i]->n_sites;
+      }
+  }
+  const int n = b->n_slots;
+  if (energies) CUDA_TRY(cudaMemcpy(energies, b->d_energy, 8 * n, cudaMemcpyDeviceToHost));
+  if (slot_of_rung) CUDA_TRY(cudaMemcpy(slot_of_rung, b->d_slot_of_rung, 4 * n, cudaMemcpyDeviceToHost));
+  if (counters) CUDA_TRY(cudaMemcpy(counters, b->d_cnt, 32 * n, cudaMemcpyDeviceToHost));
+  if (swaps) CUDA_TRY(cudaMemcpy(swaps, b->d_swaps, 16 * n, cudaMemcpyDeviceToHost));
+  if (steps) CUDA_TRY(cudaMemcpy(steps, b->d_step, 8 * n, cudaMemcpyDeviceToHost));
+  if (max_drift) CUDA_TRY(cudaMemcpy(max_drift, b->d_max_drift, 8 * n, cudaMemcpyDeviceToHost));
+  return SCEMC_OK;
+}
+
+int32_t scemc_batch_reset_counters(scemc_batch* b) {
+  if (!b) return fail(SCEMC_ERR_ARG, "batch is NULL");
+  const int n = b->n_slots;
+  CUDA_TRY(cudaMemsetAsync(b->d_cnt, 0, 32 * n, b->stream));
+  CUDA_TRY(cudaMemsetAsync(b->d_win, 0, 16 * n, b->stream));
+  CUDA_TRY(cudaMemsetAsync(b->d_swaps, 0, 16 * n, b->stream));
+  CUDA_TRY(cudaMemsetAsync(b->d_max_drift, 0, 8 * n, b->stream));
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  return SCEMC_OK;
+}
+
+int32_t scemc_batch_fetch_measurements(scemc_batch* b, double* rec, int64_t capacity, int64_t* n_records,
+                                       int32_t* record_len) {
+  if (!b) return fail(SCEMC_ERR_ARG, "batch is NULL");
+  if (record_len) *record_len = b->rec_len;
+  if (n_records) *n_records = b->meas_n;
+  if (!rec) return SCEMC_OK;
+  if (capacity < b->meas_n) return fail(SCEMC_ERR_ARG, "capacity smaller than the number of records");
+  if (b->meas_n > 0)
+    CUDA_TRY(cudaMemcpy(rec, b->d_meas, sizeof(double) * b->meas_n * b->n_slots * b->rec_len, cudaMemcpyDeviceToHost));
+  b->meas_n = 0;
+  return SCEMC_OK;
+}
+
+int32_t scemc_batch_record(scemc_batch* b, int32_t on) {
+  if (!b) return fail(SCEMC_ERR_ARG, "batch is NULL");
+  b->recording = on != 0;
+  const size_t n = (size_t)b->tabs[0]->n_sites * kRecPasses;
+  if (b->recording && !b->d_rprop) {
+    int32_t rc;
+    if ((rc = dalloc(&b->d_rprop, 3 * n)) || (rc = dalloc(&b->d_ru, n)) || (rc = dalloc(&b->d_rdE, n)) ||
+        (rc = dalloc(&b->d_racc, n)))
+      return rc;
+  }
+  if (b->recording) CUDA_TRY(cudaMemset(b->d_racc, 3, n));  // 3 = site not visited
+  return SCEMC_OK;
+}
+
+int32_t scemc_batch_fetch_record(const scemc_batch* b, int32_t pass, float* prop, double* u, float* dE,
+                                 uint8_t* acc) {
+  if (!b || !b->d_rprop) return fail(SCEMC_ERR_ARG, "recording was never enabled");
+  if (pass < -1 || pass + 1 >= kRecPasses) return fail(SCEMC_ERR_ARG, "pass outside -1..2");
+  const size_t n = (size_t)b->tabs[0]->n_sites, o = (size_t)(pass + 1) * n;
+  if (prop) CUDA_TRY(cudaMemcpy(prop, b->d_rprop + 3 * o, 12 * n, cudaMemcpyDeviceToHost));
+  if (u) CUDA_TRY(cudaMemcpy(u, b->d_ru + o, 8 * n, cudaMemcpyDeviceToHost));
+  if (dE) CUDA_TRY(cudaMemcpy(dE, b->d_rdE + o, 4 * n, cudaMemcpyDeviceToHost));
+  if (acc) CUDA_TRY(cudaMemcpy(acc, b->d_racc + o, n, cudaMemcpyDeviceToHost));
+  return SCEMC_OK;
+}
+
+int32_t scemc_color_sites(int32_t n_sites, const int32_t* site_ptr, const int32_t* site_inst, const int32_t* inst_ptr,
+                          const int32_t* inst_sites, const uint8_t* site_active, int32_t* colors_out,
+                          int32_t* n_colors) {
+  if (n_sites < 0 || !site_ptr || !site_inst || !inst_ptr || !inst_sites || !site_active || !colors_out || !n_colors)
+    return fail(SCEMC_ERR_ARG, "NULL argument");
+  std::vector<int32_t> stamp;
+  int32_t ncol = 0;
+  for (int32_t s = 1; s <= n_sites; ++s) {
+    colors_out[s - 1] = 0;
+  }
+  for (int32_t s = 1; s <= n_sites; ++s) {
+    if (!site_active[s - 1]) continue;
+    for (int32_t j = site_ptr[s - 1]; j < site_ptr[s]; ++j) {
+      const int32_t i = site_inst[j - 1];
+      for (int32_t q = inst_ptr[i - 1]; q < inst_ptr[i]; ++q) {
+        const int32_t c = colors_out[inst_sites[q - 1] - 1];
+        if (c > 0) stamp[c - 1] = s;
+      }
+    }
+    int32_t c = 1;
+    while (c <= ncol && stamp[c - 1] == s) ++c;
+    if (c > ncol) {
+      ncol = c;
+      stamp.push_back(0);
+    }
+    colors_out[s - 1] = c;
+  }
+  *n_colors = ncol;
+  return SCEMC_OK;
+}
+
+int32_t scemc_selftest_barrier_timeout(int64_t limit_ns) {
+  GridSync* gs = nullptr;
+  CUDA_TRY(cudaMalloc(&gs, sizeof(GridSync)));
+  CUDA_TRY(cudaMemset(gs, 0, sizeof(GridSync)));
+  void* params[] = {&gs, &limit_ns};
+  cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_barrier_selftest, dim3(2), dim3(32), params, 0, 0);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  GridSync h{};
+  if (e == cudaSuccess) e = cudaMemcpy(&h, gs, sizeof(h), cudaMemcpyDeviceToHost);
+  cudaFree(gs);
+  if (e != cudaSuccess) return fail(SCEMC_ERR_CUDA, cudaGetErrorString(e));
+  if (h.error) return fail(SCEMC_ERR_TIMEOUT, "grid barrier gave up after the bound, as designed");
+  return SCEMC_OK;
+}
+
+}  // extern "C"

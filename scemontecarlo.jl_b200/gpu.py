@@ -1,0 +1,404 @@
+"""The reference's device-path API over libscemc_cuda.so.
+
+Names, argument meaning and error behaviour follow src/gpu/*.jl:
+  GPUTiledHamiltonian  gpu_hamiltonian.jl:433-460
+  GPUChainState        gpu_state.jl:305-347
+  gpu_metropolis_sweep gpu_sweep.jl:158-190
+  gpu_run_sweeps       gpu_sweep.jl:204-218
+  to_host / from_host  gpu_state.jl:357-372
+  swap_payload         gpu_pt.jl:46-51
+  gpu_run_pt           gpu_pt.jl:261-316
+plus the device overrelaxation sweep (the reference has it on the CPU only,
+src/updates.jl:231-248) and the batched ensemble the PT driver runs on.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from .hamiltonian import KB_EV, TiledHamiltonian, resolve_kt
+from .stats import PTResult, StandardAccumulators, TempResult
+
+check = _lib.check
+ptr = _lib.ptr
+
+
+def _ispow2(n: int) -> bool:
+    return n >= 1 and (n & (n - 1)) == 0
+
+
+class GPUTiledHamiltonian:
+    """Device tables of one TiledHamiltonian (the 'backend' is the current CUDA device)."""
+
+    def __init__(self, H: TiledHamiltonian):
+        if H.lmax > 6:
+            raise ValueError(f"lmax = {H.lmax} unsupported on the device path (gated ≤ 6)")
+        self.host = H
+        d = H.desc()
+        h = C.c_void_p()
+        check(_lib.lib().scemc_tables_create(C.byref(d), C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib._lib is not None:
+            _lib._lib.scemc_tables_destroy(self.h)
+            self.h = None
+
+    @property
+    def n_sites(self) -> int:
+        return self.host.n_sites
+
+    def stats(self):
+        """(mean distinct neighbours d, mean adjacency entries A, device table bytes)."""
+        dm, am, by = C.c_double(), C.c_double(), C.c_int64()
+        check(_lib.lib().scemc_tables_stats(self.h, C.byref(dm), C.byref(am), C.byref(by)))
+        return dm.value, am.value, by.value
+
+
+@dataclass
+class ChainState:
+    """Host mirror of a chain (the fields of src/state.jl:17-46 the device path uses)."""
+
+    config: np.ndarray  # (n_sites, 3) FP64
+    energy: float
+    step: float = 0.6
+    acc_metro: int = 0
+    att_metro: int = 0
+    acc_or: int = 0
+    att_or: int = 0
+    max_drift: float = 0.0
+
+
+def _config_array(config, n_sites: int) -> np.ndarray:
+    a = np.ascontiguousarray(config, dtype=np.float64).reshape(-1)
+    if a.size != 3 * n_sites:
+        raise ValueError(f"config has {a.size // 3} sites; expected {n_sites}")
+    return a
+
+
+class GPUChainState:
+    """Device chain: FP32 float4 spins + FP64 running energy; seed, sweep index,
+    step and counters stay with the object (the lane)."""
+
+    def __init__(self, gH: GPUTiledHamiltonian, st, seed: int, step: Optional[float] = None,
+                 energy: Optional[float] = None):
+        if isinstance(st, ChainState):
+            config, energy0, step0 = st.config, st.energy, st.step
+        else:
+            config, energy0, step0 = st, None, 0.6
+        if step is not None:
+            step0 = step
+        if energy is not None:
+            energy0 = energy
+        self.gH = gH
+        self.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+        cfg = _config_array(config, gH.n_sites)
+        h = C.c_void_p()
+        check(_lib.lib().scemc_chain_create(gH.h, ptr(cfg, C.c_double), 0.0 if energy0 is None else float(energy0),
+                                            C.c_uint64(self.seed), float(step0), C.byref(h)))
+        self.h = h
+        if energy0 is None:  # anchor on the FP64 energy of the stored (FP32) spins
+            check(_lib.lib().scemc_renormalize(self.h, None))
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib._lib is not None:
+            _lib._lib.scemc_chain_destroy(self.h)
+            self.h = None
+
+    @property
+    def energy(self) -> float:
+        e = C.c_double()
+        check(_lib.lib().scemc_download(self.h, None, C.byref(e), None, None))
+        return e.value
+
+    @property
+    def sweep_index(self) -> int:
+        s = C.c_int64()
+        check(_lib.lib().scemc_download(self.h, None, None, C.byref(s), None))
+        return s.value
+
+    def counters(self):
+        c = np.zeros(4, np.int64)
+        check(_lib.lib().scemc_download(self.h, None, None, None, ptr(c, C.c_int64)))
+        return c
+
+    def set_step(self, step: float):
+        check(_lib.lib().scemc_set_step(self.h, float(step)))
+
+    def total_energy(self) -> float:
+        """FP64 full recompute of the device state (does not touch the running energy)."""
+        e = C.c_double()
+        check(_lib.lib().scemc_total_energy(self.h, 0, C.byref(e)))
+        return e.value
+
+    def renormalize(self) -> float:
+        d = np.zeros(1)
+        check(_lib.lib().scemc_renormalize(self.h, ptr(d, C.c_double)))
+        return float(d[0])
+
+
+def gpu_metropolis_sweep(gst: GPUChainState, gH: GPUTiledHamiltonian, beta: float, workgroupsize: int = 32) -> int:
+    """One device Metropolis sweep; returns the number of accepted moves."""
+    if not _ispow2(int(workgroupsize)):
+        raise ValueError(f"workgroupsize must be a power of two (got {workgroupsize})")
+    n = C.c_int64()
+    check(_lib.lib().scemc_metropolis_sweep(gst.h, gH.h, float(beta), int(workgroupsize), C.byref(n)))
+    return n.value
+
+
+def gpu_overrelaxation_sweep(gst: GPUChainState, gH: GPUTiledHamiltonian, beta: float,
+                             workgroupsize: int = 32):
+    """One device overrelaxation sweep; returns (accepted, attempted)."""
+    if not _ispow2(int(workgroupsize)):
+        raise ValueError(f"workgroupsize must be a power of two (got {workgroupsize})")
+    a, t = C.c_int64(), C.c_int64()
+    check(_lib.lib().scemc_overrelaxation_sweep(gst.h, gH.h, float(beta), int(workgroupsize), C.byref(a),
+                                                C.byref(t)))
+    return a.value, t.value
+
+
+def to_host(st: ChainState, gst: GPUChainState) -> ChainState:
+    cfg = np.zeros(3 * gst.gH.n_sites)
+    e = C.c_double()
+    check(_lib.lib().scemc_download(gst.h, ptr(cfg, C.c_double), C.byref(e), None, None))
+    st.config = cfg.reshape(-1, 3)
+    st.energy = e.value
+    return st
+
+
+def from_host(gst: GPUChainState, st: ChainState) -> GPUChainState:
+    cfg = _config_array(st.config, gst.gH.n_sites)
+    check(_lib.lib().scemc_upload(gst.h, ptr(cfg, C.c_double), float(st.energy)))
+    return gst
+
+
+def gpu_run_sweeps(gst: GPUChainState, gH: GPUTiledHamiltonian, st: ChainState, beta: float, nsweeps: int,
+                   renorm_interval: int = 1000, workgroupsize: int = 32) -> GPUChainState:
+    """nsweeps device Metropolis sweeps with a device renormalisation + FP64 recompute
+    every renorm_interval sweeps (<= 0 disables); downloads the state into st."""
+    if not _ispow2(int(workgroupsize)):
+        raise ValueError(f"workgroupsize must be a power of two (got {workgroupsize})")
+    check(_lib.lib().scemc_run_sweeps(gst.h, gH.h, float(beta), int(nsweeps), int(renorm_interval),
+                                      int(workgroupsize)))
+    to_host(st, gst)
+    return gst
+
+
+def swap_payload(a: GPUChainState, b: GPUChainState):
+    check(_lib.lib().scemc_swap_payload(a.h, b.h))
+
+
+class GPUBatch:
+    """Replicas of one or more table sets advancing together (PT rungs, temperature
+    sets, chains of uneven supercells). Slots are numbered table-major."""
+
+    def __init__(self, gHs: Sequence[GPUTiledHamiltonian], replicas: Sequence[int], configs, seeds, steps,
+                 energies=None):
+        self.gHs = list(gHs)
+        self.replicas = [int(r) for r in replicas]
+        nslots = sum(self.replicas)
+        cfg = np.ascontiguousarray(np.concatenate([np.asarray(c, np.float64).reshape(-1) for c in configs]))
+        exp = sum(3 * g.n_sites * r for g, r in zip(self.gHs, self.replicas))
+        if cfg.size != exp:
+            raise ValueError("configs do not match the table sizes")
+        en = np.zeros(nslots) if energies is None else np.ascontiguousarray(energies, np.float64)
+        sd = np.ascontiguousarray([int(s) & 0xFFFFFFFFFFFFFFFF for s in seeds], dtype=np.uint64)
+        stp = np.ascontiguousarray(np.broadcast_to(np.asarray(steps, np.float64), (nslots,)))
+        tabs = (C.c_void_p * len(self.gHs))(*[g.h for g in self.gHs])
+        reps = np.ascontiguousarray(self.replicas, np.int32)
+        h = C.c_void_p()
+        check(_lib.lib().scemc_batch_create(len(self.gHs), tabs, ptr(reps, C.c_int32), ptr(cfg, C.c_double),
+                                            ptr(en, C.c_double), ptr(sd, C.c_uint64), ptr(stp, C.c_double),
+                                            C.byref(h)))
+        self.h = h
+        self.n_slots = nslots
+        if energies is None:
+            check(_lib.lib().scemc_renormalize(self.h, None))
+            self.reset_counters()
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib._lib is not None:
+            _lib._lib.scemc_batch_destroy(self.h)
+            self.h = None
+
+    def set_betas(self, betas):
+        b = np.ascontiguousarray(betas, np.float64)
+        check(_lib.lib().scemc_batch_set_betas(self.h, ptr(b, C.c_double)))
+
+    def set_steps(self, steps):
+        s = np.ascontiguousarray(np.broadcast_to(np.asarray(steps, np.float64), (self.n_slots,)))
+        check(_lib.lib().scemc_batch_set_steps(self.h, ptr(s, C.c_double)))
+
+    def run(self, nsweeps, or_per_metropolis=0, exchange=False, exchange_interval=1, adapt_interval=0,
+            adapt_target=0.5, renorm_interval=0, measure_interval=0, lanes_per_site=0, mode=0, phase_done=0,
+            phase_total=0):
+        p = _lib.RunParams(int(nsweeps), int(or_per_metropolis), int(bool(exchange)), int(exchange_interval),
+                           int(adapt_interval), float(adapt_target), int(renorm_interval), int(measure_interval),
+                           int(lanes_per_site), int(mode), int(phase_done), int(phase_total))
+        check(_lib.lib().scemc_batch_run(self.h, C.byref(p)))
+
+    def renormalize(self):
+        d = np.zeros(self.n_slots)
+        check(_lib.lib().scemc_renormalize(self.h, ptr(d, C.c_double)))
+        return d
+
+    def reset_counters(self):
+        check(_lib.lib().scemc_batch_reset_counters(self.h))
+
+    def total_energy(self, slot: int) -> float:
+        e = C.c_double()
+        check(_lib.lib().scemc_total_energy(self.h, int(slot), C.byref(e)))
+        return e.value
+
+    def download(self):
+        n = self.n_slots
+        tot = sum(g.n_sites * r for g, r in zip(self.gHs, self.replicas))
+        cfg = np.zeros(3 * tot)
+        en = np.zeros(n)
+        sor = np.zeros(n, np.int32)
+        cnt = np.zeros(4 * n, np.int64)
+        sw = np.zeros(2 * n, np.int64)
+        st = np.zeros(n)
+        md = np.zeros(n)
+        check(_lib.lib().scemc_batch_download(self.h, ptr(cfg, C.c_double), ptr(en, C.c_double),
+                                              ptr(sor, C.c_int32), ptr(cnt, C.c_int64), ptr(sw, C.c_int64),
+                                              ptr(st, C.c_double), ptr(md, C.c_double)))
+        configs, off = [], 0
+        for g, r in zip(self.gHs, self.replicas):
+            for _ in range(r):
+                configs.append(cfg[off:off + 3 * g.n_sites].reshape(-1, 3))
+                off += 3 * g.n_sites
+        return dict(configs=configs, energies=en, slot_of_rung=sor, counters=cnt.reshape(n, 4),
+                    swaps=sw.reshape(n, 2), steps=st, max_drift=md)
+
+    def fetch_measurements(self):
+        n = C.c_int64()
+        rl = C.c_int32()
+        check(_lib.lib().scemc_batch_fetch_measurements(self.h, None, 0, C.byref(n), C.byref(rl)))
+        buf = np.zeros(max(1, n.value * self.n_slots * rl.value))
+        check(_lib.lib().scemc_batch_fetch_measurements(self.h, ptr(buf, C.c_double), n.value, C.byref(n),
+                                                        C.byref(rl)))
+        return buf[: n.value * self.n_slots * rl.value].reshape(n.value, self.n_slots, rl.value)
+
+    def record(self, on: bool):
+        check(_lib.lib().scemc_batch_record(self.h, int(bool(on))))
+
+    def fetch_record(self, pass_: int = -1):
+        """Recorded (proposal, u, dE32, flag) of slot 0 for pass -1 (Metropolis) or
+        overrelaxation pass k."""
+        n = self.gHs[0].n_sites
+        prop = np.zeros(3 * n, np.float32)
+        u = np.zeros(n)
+        dE = np.zeros(n, np.float32)
+        acc = np.zeros(n, np.uint8)
+        check(_lib.lib().scemc_batch_fetch_record(self.h, int(pass_), ptr(prop, C.c_float), ptr(u, C.c_double),
+                                                  ptr(dE, C.c_float), ptr(acc, C.c_uint8)))
+        return prop.reshape(n, 3), u, dE, acc
+
+
+def _random_configs(n_sites: int, count: int, rng: np.random.Generator):
+    out = []
+    for _ in range(count):
+        v = rng.standard_normal((n_sites, 3))
+        out.append(v / np.linalg.norm(v, axis=1, keepdims=True))
+    return out
+
+
+def gpu_run_pt(gHs, *, temperature=None, kT=None, exchange: bool = True, exchange_interval: int = 10,
+               sweeps_therm: int = 2000, sweeps_measure: int = 10000, measure_interval: int = 1,
+               or_per_metropolis: int = 0, step: float = 0.6, adapt_target: float = 0.5, adapt_interval: int = 50,
+               renorm_interval: int = 1000, nbins: int = 32, init=None, seed: Optional[int] = None,
+               lanes_per_site: int = 0, mode: int = 0, chunk: int = 2000) -> PTResult:
+    """Parallel tempering on the device (gpu_pt.jl:261-316 semantics; exchanges run on
+    the device). `gHs` is one GPUTiledHamiltonian or a list of them: every table set
+    gets its own ladder over the same kT values (chains of uneven supercells), and
+    results are returned ladder-major. With exchange=False the rungs are independent
+    chains at their temperatures (run_mc with one chain per temperature).
+
+    Seeds: a numpy Generator seeded with `seed` draws, in order, the initial spins of
+    every slot (uniform on S^2) and then one 64-bit device key per slot."""
+    if isinstance(gHs, GPUTiledHamiltonian):
+        gHs = [gHs]
+    kts = resolve_kt(temperature, kT)
+    R = len(kts)
+    if exchange:
+        if R < 2:
+            raise ValueError(f"parallel tempering needs a ladder of ≥ 2 temperatures; got {R}")
+        d = np.diff(kts)
+        if not (np.all(d > 0) or np.all(d < 0)):
+            raise ValueError(f"the temperature ladder must be strictly monotone; got {kts}")
+        if exchange_interval < 1:
+            raise ValueError(f"exchange_interval must be ≥ 1; got {exchange_interval}")
+    if sweeps_therm < 0 or sweeps_measure < 1 or not (1 <= measure_interval <= sweeps_measure):
+        raise ValueError("bad sweep counts / measure_interval")
+    if or_per_metropolis < 0 or step <= 0 or not (0 < adapt_target < 1) or adapt_interval < 1 \
+            or renorm_interval < 1 or nbins < 2:
+        raise ValueError("bad run parameters")
+    if or_per_metropolis > 0 and not any(np.any(g.host.site_has_l1) for g in gHs):
+        raise ValueError("or_per_metropolis > 0 needs an l = 1 spin channel somewhere")
+    if lanes_per_site and not _ispow2(int(lanes_per_site)):
+        raise ValueError(f"lanes_per_site must be a power of two (got {lanes_per_site})")
+    if seed is None:
+        seed = int(np.random.SeedSequence().entropy) & 0xFFFFFFFFFFFFFFFF
+    rng = np.random.default_rng(seed)
+    configs = []
+    for g in gHs:
+        if init is None:
+            configs += _random_configs(g.n_sites, R, rng)
+        else:
+            c = np.asarray(init, np.float64).reshape(-1, 3)
+            configs += [c.copy() for _ in range(R)]
+    seeds = rng.integers(0, 2 ** 64, size=R * len(gHs), dtype=np.uint64)
+    batch = GPUBatch(gHs, [R] * len(gHs), configs, seeds, step)
+    batch.set_betas(np.tile(1.0 / kts, len(gHs)))
+    common = dict(or_per_metropolis=or_per_metropolis, exchange=exchange, exchange_interval=exchange_interval,
+                  renorm_interval=renorm_interval, lanes_per_site=lanes_per_site, mode=mode)
+    done = 0
+    while done < sweeps_therm:
+        n = min(chunk, sweeps_therm - done)
+        batch.run(n, adapt_interval=adapt_interval, adapt_target=adapt_target, phase_done=done,
+                  phase_total=sweeps_therm, **common)
+        done += n
+    # thermalisation -> measurement boundary: renormalise, fresh counters (gpu_pt.jl:161-179)
+    batch.renormalize()
+    batch.reset_counters()
+    planned = sweeps_measure // measure_interval
+    accs = [StandardAccumulators(g.host.n_cell_atoms, planned, nbins) for g in gHs for _ in range(R)]
+    rec_off = [0]
+    for g in gHs:
+        rec_off.append(rec_off[-1] + R)
+    done = 0
+    while done < sweeps_measure:
+        n = min(chunk, sweeps_measure - done)
+        batch.run(n, measure_interval=measure_interval, phase_done=done, phase_total=sweeps_measure, **common)
+        done += n
+        rec = batch.fetch_measurements()
+        for i, acc in enumerate(accs):
+            li = np.searchsorted(rec_off, i, side="right") - 1
+            A = gHs[li].host.n_cell_atoms
+            if len(rec):
+                acc.push_records(rec[:, i, : 4 + 3 * A])
+    st = batch.download()
+    points = []
+    for i, acc in enumerate(accs):
+        li = np.searchsorted(rec_off, i, side="right") - 1
+        H = gHs[li].host
+        kt = float(kts[i - rec_off[li]])
+        cnt = st["counters"][i]
+        acc_m = cnt[0] / cnt[1] if cnt[1] else np.nan
+        acc_o = cnt[2] / cnt[3] if cnt[3] else np.nan
+        points.append(TempResult(kt, kt / KB_EV, acc.finalize(kt, H.n_active), acc_m, acc_o, float(st["steps"][i]),
+                                 float(st["max_drift"][i])))
+    sw = st["swaps"]
+    swaps = []
+    for li in range(len(gHs)):
+        for r in range(R - 1):
+            a, b = sw[rec_off[li] + r]
+            swaps.append(b / a if a else np.nan)
+    finals = [st["configs"][st["slot_of_rung"][i]] for i in range(len(accs))]
+    return PTResult(points, np.asarray(swaps), finals, seed,
+                    extra=dict(energies=st["energies"], slot_of_rung=st["slot_of_rung"], batch=batch))
