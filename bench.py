@@ -1,0 +1,316 @@
+#!/usr/bin/env python
+"""Spin-updates/s of the B200 sweep on the bcc 16^3 multipole workload.
+
+Workload (the second benchmark configuration): bcc, 2 sublattices, 16^3 cells
+(8192 spins); l = 1 and l = 2 pair products to the 3rd shell (shell means
+-1.0/-0.3/-0.1 meV, sigma 0.1 meV per (l m, l' m') entry), l = 1 body-4
+plaquettes N(0, 0.05 meV), Zeeman 2 muB in 1 T || z; 5 temperatures uniform in
+[0.2, 2.0] meV; colour-class Metropolis + 1 overrelaxation pass per sweep, FP32
+dE with FP64 running energies; seed 2. Synthetic, seeded (no fitted model).
+
+One step = one compound sweep (1 Metropolis + 1 overrelaxation pass) of all 5
+chains. The metric counts attempts on active sites (Metropolis + overrelaxation)
+per second, summed over chains and GPUs. The working set (~16 MB) fits in L2, so
+L2 is flushed (a 256 MiB write) before every timed step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl scemc|reference]
+
+--impl reference times the FP64 CPU restatement of the reference's
+metropolis_sweep!/overrelaxation_sweep! (oracle/, colour-parallel over all host
+threads like sweep_tasks) on the same workload; under torchrun only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import shutil
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = "bcc16_l2_plaquette_zeeman_5T_metropolis+OR"
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def workload():
+    from scemc import models
+    w = models.config2_bcc_l2(16)
+    return w, w.hamiltonians()[0]
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_cpu_reference(w, H, steps: int, warmup: int, budget_s: float):
+    """Times the oracle's compound sweep (Metropolis + 1 OR) of the 5 chains on all
+    host threads; returns (attempts/s, threads, sample description, per-step ms)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    OH = O.OracleHamiltonian(2, w.terms, (16, 16, 16), magmoms=w.magmoms, field=w.field)
+    threads = max(1, os.cpu_count() or 1)
+    chains = [O.OracleChain(OH, __import__("scemc").models.random_config(H.n_sites, 100 + i), seed=1000 + i)
+              for i in range(len(w.kts))]
+
+    def step():
+        att = 0
+        for ch, kt in zip(chains, w.kts):
+            c0 = ch.get()[3]
+            ch.sweeps(1.0 / kt, 1, n_or=w.or_per_metropolis, threads=threads)
+            c1 = ch.get()[3]
+            att += int((c1[1] - c0[1]) + (c1[3] - c0[3]))
+        return att
+
+    for _ in range(warmup):
+        step()
+    tot_att, tot_t, n = 0, 0.0, 0
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        tot_att += step()
+        tot_t += time.perf_counter() - t0
+        n += 1
+        if tot_t > budget_s:
+            break
+    sample = (f"{n} compound sweeps (Metropolis + {w.or_per_metropolis} OR) of {len(w.kts)} chains x {H.n_sites} "
+              f"spins, FP64 oracle, {threads} threads, {cpu_model()}")
+    return tot_att / tot_t, threads, sample, 1e3 * tot_t / n
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = ROOT / "gpurun_out" / f"clocks_rank{index}.csv"
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        self.path.parent.mkdir(exist_ok=True)
+        self.fh = open(self.path, "w")
+        self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.fh,
+                                     stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="scemc", choices=["scemc", "reference"])
+    ap.add_argument("--mode", type=int, default=0, help="0 auto, 1 per-colour launches, 2 persistent")
+    ap.add_argument("--lanes", type=int, default=0, help="lanes per site (0 = autotuned)")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        w, H = workload()
+        steps = max(1, args.steps if args.steps <= 50 else 50)
+        v, threads, sample, ms = run_cpu_reference(w, H, steps, min(args.warmup, 3), args.cpu_budget)
+        line = {"metric": "spin-updates/s", "value": v, "unit": "attempts/s", "n_gpus": args.gpus,
+                "steps": steps, "warmup": min(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "sites_per_chain": H.n_sites, "chains": len(w.kts)},
+                "impl": "reference",
+                "cpu_baseline": {"value": v, "unit": "attempts/s", "cores": threads, "kind": "port",
+                                 "sample": sample},
+                "e2e": {"value": v, "unit": "attempts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+    import scemc
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist_
+        dist_.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = dist_
+
+    w, H = workload()
+    gH = scemc.GPUTiledHamiltonian(H)
+    d_mean, a_mean, table_bytes = gH.stats()
+    R = len(w.kts)
+    rng = np.random.default_rng(2 + 1000 * rank)
+    configs = [models_random(H.n_sites, rng) for _ in range(R)]
+    seeds = [int(x) for x in rng.integers(0, 2 ** 63, size=R)]
+    batch = scemc.GPUBatch([gH], [R], configs, seeds, 0.6)
+    batch.set_betas(1.0 / w.kts)
+    p = scemc.GPUBatch.params(1, or_per_metropolis=w.or_per_metropolis, lanes_per_site=args.lanes, mode=args.mode)
+    stream = torch.cuda.ExternalStream(batch.stream())
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def one_step():
+        batch.run_async(p)
+        batch.sync()
+
+    # thermalise a little so acceptance rates are representative, then warm up
+    batch.run(200, or_per_metropolis=w.or_per_metropolis, lanes_per_site=args.lanes, mode=args.mode)
+    for _ in range(args.warmup):
+        one_step()
+
+    cnt0 = batch.download()["counters"].copy()
+    clocks = ClockSampler(local)
+    batch.profile(True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    step_ms = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        batch.run_async(p)
+        e1.record(stream)
+        batch.sync()
+        step_ms.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if dist:
+        dist.barrier()
+    kern_ms, passes = batch.kernel_time()
+    batch.profile(False)
+    cnt1 = batch.download()["counters"]
+    att = cnt1 - cnt0
+    attempts = int(att[:, 1].sum() + att[:, 3].sum())
+    total_ms = float(np.sum(step_ms))
+    t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+    a = torch.tensor([attempts], device="cuda", dtype=torch.float64)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(a, op=dist.ReduceOp.SUM)
+    total_ms_max = float(t.item())
+    attempts_all = float(a.item())
+    value = attempts_all / (total_ms_max * 1e-3)
+
+    # roofline of the sweep kernel: algorithmic bytes per attempt (own spin read +
+    # write, d neighbour float4 gathers, one 4-byte adjacency word per entry, site_ptr)
+    B = 16 + 16 + 16 * d_mean + 4 * a_mean + 4
+    hbm, peak_kind = peaks()
+    achieved = attempts * B / (kern_ms * 1e-3) / 1e9 if kern_ms > 0 else None
+
+    # end-to-end through the C ABI with host buffers: upload the 5 chains, one
+    # compound sweep, download the 5 chains + energies
+    host_cfg = np.concatenate([c.reshape(-1) for c in batch.download()["configs"]])
+    host_en = batch.download()["energies"].copy()
+    e2e_steps = max(10, min(args.steps, 100))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_att = 0
+    for _ in range(e2e_steps):
+        batch.upload(host_cfg, host_en)
+        batch.run(1, or_per_metropolis=w.or_per_metropolis, lanes_per_site=args.lanes, mode=args.mode)
+        st = batch.download()
+        host_cfg = np.concatenate([c.reshape(-1) for c in st["configs"]])
+        host_en = st["energies"].copy()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    per_step_att = attempts / args.steps
+    e2e_value = per_step_att * e2e_steps * world / e2e_s
+    h2d = host_cfg.nbytes + host_en.nbytes
+    d2h = host_cfg.nbytes + host_en.nbytes + 8 * 4 * R + 8 * 2 * R + 8 * 3 * R + 4 * R
+
+    cpu = None
+    if rank == 0 and world == 1:
+        v, threads, sample, _ = run_cpu_reference(w, H, 50, 1, args.cpu_budget)
+        cpu = {"value": v, "unit": "attempts/s", "cores": threads, "kind": "port", "sample": sample}
+
+    launches_per_step = (1 + w.or_per_metropolis) * (1 if (args.mode in (0, 2)) else H.n_colors) + 1
+    if rank == 0:
+        line = {
+            "metric": "spin-updates/s", "value": value, "unit": "attempts/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sites_per_chain": H.n_sites, "chains_per_gpu": R,
+                       "compound_sweep": f"1 Metropolis + {w.or_per_metropolis} OR", "l2": "flushed (256 MiB) before every step",
+                       "lanes_per_site": args.lanes or "auto", "mode": args.mode or "auto",
+                       "d_mean": d_mean, "A_mean": a_mean, "table_bytes": table_bytes,
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": (achieved / hbm) if achieved else None, "traffic": None,
+                         "peak_kind": peak_kind, "bytes_per_attempt": B,
+                         "kernel_ms_per_pass": kern_ms / max(passes, 1), "passes": passes},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "attempts/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
+            "gpu_launches": int(launches_per_step * args.steps),
+            "clocks": clk,
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def models_random(n, rng):
+    v = rng.standard_normal((n, 3))
+    return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -188,6 +188,20 @@ typedef struct scemc_run_params {
 int32_t scemc_batch_set_betas(scemc_batch* b, const double* betas);
 int32_t scemc_batch_set_steps(scemc_batch* b, const double* steps);
 int32_t scemc_batch_run(scemc_batch* b, const scemc_run_params* p);
+/* Asynchronous form: enqueues the run on the batch's stream and returns; the
+ * caller must call scemc_batch_sync before touching the batch again. */
+int32_t scemc_batch_run_async(scemc_batch* b, const scemc_run_params* p);
+int32_t scemc_batch_sync(scemc_batch* b);
+/* The batch's cudaStream_t (as void*), for callers that order or time work on it. */
+int32_t scemc_batch_stream(const scemc_batch* b, void** stream);
+/* Replaces every slot's spins (3 x n_sites FP64 per slot, payload order) and, when
+ * energies is not NULL, the running energies. */
+int32_t scemc_batch_upload(scemc_batch* b, const double* configs, const double* energies);
+/* Live timing of the sweep kernels: with profiling on, each pass is bracketed by a
+ * CUDA event pair on the batch stream; scemc_batch_kernel_time returns the summed
+ * device time (ms) and the number of passes since profiling was switched on. */
+int32_t scemc_batch_profile(scemc_batch* b, int32_t on);
+int32_t scemc_batch_kernel_time(const scemc_batch* b, double* ms, int64_t* passes);
 /* State readback. configs: 3 x n_sites per SLOT (payload order); energies per slot;
  * slot_of_rung per rung; counters 4 per rung {acc_metro, att_metro, acc_or, att_or};
  * swap counters 2 per rung pair {attempted, accepted} (pair r = rungs r, r+1 of one

@@ -410,7 +410,8 @@ __device__ void sweep_colour(const SweepArgs& a, int col, unsigned long long* s_
       u = keyed_proposal(a.seed[rung], (uint32_t)(s + 1), a.sweep, e.x, e.y, e.z, a.step[rung], px, py, pz);
     } else {
       // Reflection about the l = 1 field axis h = (c4, c2, c3) (updates.jl:66-87).
-      const double h0 = c[3], h1 = c[1], h2 = c[2];
+      const double h0 = LMAX >= 1 ? c[NLM > 3 ? 3 : 0] : 0.0, h1 = LMAX >= 1 ? c[NLM > 1 ? 1 : 0] : 0.0,
+                   h2 = LMAX >= 1 ? c[NLM > 2 ? 2 : 0] : 0.0;
       const double hn = sqrt((h0 * h0 + h1 * h1) + h2 * h2);
       if (hn < 1e-12) {
         attempted = false;
@@ -804,7 +805,20 @@ struct scemc_ensemble {
   long long barrier_limit_ns = 2000000000ll;
   int coop_blocks = 0;  // cached co-resident grid size for the persistent form
   int coop_G = -1;
+  float4* h_stage = nullptr;  // pinned host staging of the spins (n_spins float4)
+  // live timing of the sweep kernels: one event pair per pass
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending;
+  double prof_ms = 0.0;
+  int64_t prof_passes = 0;
   ~scemc_ensemble() {
+    if (h_stage) cudaFreeHost(h_stage);
+    for (auto& pr : ev_pending) {
+      ev_pool.push_back(pr.first);
+      ev_pool.push_back(pr.second);
+    }
+    for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
     void* ps[] = {d_lat,   d_spins, d_seg,  d_energy,       d_dEfix,        d_cnt,       d_win,    d_swaps,
                   d_beta,  d_step,  d_seed, d_slot_of_rung, d_rung_of_slot, d_max_drift, d_drift,  d_eout,
                   d_gs,    d_st,    d_partial, d_meas,      d_rprop,        d_ru,        d_rdE,    d_racc};
@@ -1062,32 +1076,44 @@ int32_t dalloc(T** p, size_t n) {
 
 bool finite3(const double* v) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]); }
 
-int32_t upload_config(scemc_ensemble* E, int ti, int r, const double* config) {
+// Whole-table transfers through pinned staging: the host (de)interleaves the
+// replicas (spins[site * R + r]) and one contiguous copy moves the table.
+int32_t stage_upload(scemc_ensemble* E, int ti, const double* cfgs) {
   const scemc_tables* T = E->tabs[ti];
   const int R = E->R[ti];
-  std::vector<float4> tmp(T->n_sites);
-  for (int s = 0; s < T->n_sites; ++s) {
-    if (!finite3(config + 3 * s)) return fail(SCEMC_ERR_NUMERIC, "spin column " + std::to_string(s + 1) + " is not finite");
-    tmp[s] = make_float4((float)config[3 * s], (float)config[3 * s + 1], (float)config[3 * s + 2], 0.0f);
+  const int64_t n = T->n_sites;
+  float4* h = E->h_stage + E->spin_off[ti];
+  for (int r = 0; r < R; ++r) {
+    const double* c = cfgs + (size_t)r * 3 * n;
+    for (int64_t s = 0; s < n; ++s) {
+      if (!finite3(c + 3 * s))
+        return fail(SCEMC_ERR_NUMERIC, "spin column " + std::to_string(s + 1) + " of replica " +
+                                           std::to_string(r + 1) + " is not finite");
+      h[s * R + r] = make_float4((float)c[3 * s], (float)c[3 * s + 1], (float)c[3 * s + 2], 0.0f);
+    }
   }
-  // strided copy into spins[spin_off + s*R + r]
-  CUDA_TRY(cudaMemcpy2DAsync(E->d_spins + E->spin_off[ti] + r, sizeof(float4) * R, tmp.data(), sizeof(float4),
-                             sizeof(float4), T->n_sites, cudaMemcpyHostToDevice, E->stream));
+  CUDA_TRY(cudaMemcpyAsync(E->d_spins + E->spin_off[ti], h, sizeof(float4) * n * R, cudaMemcpyHostToDevice,
+                           E->stream));
   CUDA_TRY(cudaStreamSynchronize(E->stream));
   return SCEMC_OK;
 }
 
-int32_t download_config(const scemc_ensemble* E, int ti, int r, double* config) {
+int32_t stage_download(const scemc_ensemble* E, int ti, double* cfgs) {
   const scemc_tables* T = E->tabs[ti];
   const int R = E->R[ti];
-  std::vector<float4> tmp(T->n_sites);
-  CUDA_TRY(cudaMemcpy2DAsync(tmp.data(), sizeof(float4), E->d_spins + E->spin_off[ti] + r, sizeof(float4) * R,
-                             sizeof(float4), T->n_sites, cudaMemcpyDeviceToHost, E->stream));
+  const int64_t n = T->n_sites;
+  float4* h = E->h_stage + E->spin_off[ti];
+  CUDA_TRY(cudaMemcpyAsync(h, E->d_spins + E->spin_off[ti], sizeof(float4) * n * R, cudaMemcpyDeviceToHost,
+                           E->stream));
   CUDA_TRY(cudaStreamSynchronize(E->stream));
-  for (int s = 0; s < T->n_sites; ++s) {
-    config[3 * s] = tmp[s].x;
-    config[3 * s + 1] = tmp[s].y;
-    config[3 * s + 2] = tmp[s].z;
+  for (int r = 0; r < R; ++r) {
+    double* c = cfgs + (size_t)r * 3 * n;
+    for (int64_t s = 0; s < n; ++s) {
+      const float4 v = h[s * R + r];
+      c[3 * s] = v.x;
+      c[3 * s + 1] = v.y;
+      c[3 * s + 2] = v.z;
+    }
   }
   return SCEMC_OK;
 }
@@ -1124,6 +1150,7 @@ int32_t create_ensemble(int32_t n_tables, const scemc_tables* const* tables, con
     if (!(steps[i] > 0) || !std::isfinite(energies[i])) return fail(SCEMC_ERR_ARG, "step must be > 0 and energy finite");
   int32_t rc;
   if ((rc = dalloc(&E->d_spins, off))) return rc;
+  CUDA_TRY(cudaHostAlloc((void**)&E->h_stage, sizeof(float4) * std::max<int64_t>(off, 1), cudaHostAllocDefault));
   // lattice descriptors with per-batch geometry
   std::vector<DevLattice> lats(n_tables);
   int max_atoms = 1;
@@ -1168,11 +1195,10 @@ int32_t create_ensemble(int32_t n_tables, const scemc_tables* const* tables, con
   CUDA_TRY(cudaMemcpy(E->d_beta, ones.data(), 8 * slots, cudaMemcpyHostToDevice));
   E->rec_len = 4 + 3 * max_atoms;
   const double* cfg = configs;
-  for (int i = 0; i < n_tables; ++i)
-    for (int r = 0; r < replicas[i]; ++r) {
-      if ((rc = upload_config(E, i, r, cfg))) return rc;
-      cfg += 3 * (size_t)tables[i]->n_sites;
-    }
+  for (int i = 0; i < n_tables; ++i) {
+    if ((rc = stage_upload(E, i, cfg))) return rc;
+    cfg += 3 * (size_t)tables[i]->n_sites * replicas[i];
+  }
   *out = guard.release();
   return SCEMC_OK;
 }
@@ -1255,8 +1281,45 @@ int sm_count(int dev) {
   return n > 0 ? n : 1;
 }
 
-// One pass (Metropolis or OR pass k) over every colour.
+cudaEvent_t take_event(scemc_ensemble* E) {
+  if (!E->ev_pool.empty()) {
+    cudaEvent_t e = E->ev_pool.back();
+    E->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Folds the elapsed time of completed pass event pairs (after a stream sync).
+void harvest_events(scemc_ensemble* E) {
+  for (auto& pr : E->ev_pending) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, pr.first, pr.second) == cudaSuccess) {
+      E->prof_ms += ms;
+      E->prof_passes += 1;
+    }
+    E->ev_pool.push_back(pr.first);
+    E->ev_pool.push_back(pr.second);
+  }
+  E->ev_pending.clear();
+}
+
+int32_t run_pass_impl(scemc_ensemble* E, int pass, int G, int mode);
+
+// One pass (Metropolis or OR pass k) over every colour, optionally timed.
 int32_t run_pass(scemc_ensemble* E, int pass, int G, int mode) {
+  if (!E->profiling) return run_pass_impl(E, pass, G, mode);
+  cudaEvent_t a = take_event(E), b = take_event(E);
+  CUDA_TRY(cudaEventRecord(a, E->stream));
+  const int32_t rc = run_pass_impl(E, pass, G, mode);
+  CUDA_TRY(cudaEventRecord(b, E->stream));
+  E->ev_pending.emplace_back(a, b);
+  return rc;
+}
+
+int32_t run_pass_impl(scemc_ensemble* E, int pass, int G, int mode) {
   const int lmax = E->lmax;
   const int threads = 256;
   SweepArgs a = make_args(E, pass);
@@ -1570,7 +1633,7 @@ int32_t scemc_download(const scemc_chain* c, double* config, double* energy, int
   int32_t rc;
   if ((rc = check_single(c, nullptr))) return rc;
   if (config)
-    if ((rc = download_config(c, 0, 0, config))) return rc;
+    if ((rc = stage_download(c, 0, config))) return rc;
   if (energy) CUDA_TRY(cudaMemcpy(energy, c->d_energy, 8, cudaMemcpyDeviceToHost));
   if (sweep_index) *sweep_index = c->sweep_index;
   if (counters) {
@@ -1585,7 +1648,7 @@ int32_t scemc_upload(scemc_chain* c, const double* config, double energy) {
   int32_t rc;
   if ((rc = check_single(c, nullptr))) return rc;
   if (!config || !std::isfinite(energy)) return fail(SCEMC_ERR_ARG, "config NULL or energy not finite");
-  if ((rc = upload_config(c, 0, 0, config))) return rc;
+  if ((rc = stage_upload(c, 0, config))) return rc;
   CUDA_TRY(cudaMemcpy(c->d_energy, &energy, 8, cudaMemcpyHostToDevice));
   return SCEMC_OK;
 }
@@ -1650,7 +1713,7 @@ int32_t scemc_batch_set_steps(scemc_batch* b, const double* steps) {
   return SCEMC_OK;
 }
 
-int32_t scemc_batch_run(scemc_batch* b, const scemc_run_params* p) {
+int32_t scemc_batch_run_async(scemc_batch* b, const scemc_run_params* p) {
   if (!b || !p) return fail(SCEMC_ERR_ARG, "NULL argument");
   if (p->nsweeps < 0 || p->or_per_metropolis < 0 || (p->exchange && p->exchange_interval < 1))
     return fail(SCEMC_ERR_ARG, "bad run parameters");
@@ -1676,9 +1739,64 @@ int32_t scemc_batch_run(scemc_batch* b, const scemc_run_params* p) {
     if (p->exchange && i % p->exchange_interval == 0 && i < total)
       if ((rc = launch_tail(b, false, false, 0.5, true))) return rc;
   }
+  return SCEMC_OK;
+}
+
+int32_t scemc_batch_sync(scemc_batch* b) {
+  if (!b) return fail(SCEMC_ERR_ARG, "batch is NULL");
   CUDA_TRY(cudaStreamSynchronize(b->stream));
+  harvest_events(b);
   return check_error(b);
 }
+
+int32_t scemc_batch_run(scemc_batch* b, const scemc_run_params* p) {
+  const int32_t rc = scemc_batch_run_async(b, p);
+  if (rc != SCEMC_OK) {
+    if (b) cudaStreamSynchronize(b->stream);
+    return rc;
+  }
+  return scemc_batch_sync(b);
+}
+
+int32_t scemc_batch_stream(const scemc_batch* b, void** stream) {
+  if (!b || !stream) return fail(SCEMC_ERR_ARG, "NULL argument");
+  *stream = (void*)b->stream;
+  return SCEMC_OK;
+}
+
+int32_t scemc_batch_upload(scemc_batch* b, const double* configs, const double* energies) {
+  if (!b || !configs) return fail(SCEMC_ERR_ARG, "NULL argument");
+  int32_t rc;
+  const double* cfg = configs;
+  for (size_t i = 0; i < b->tabs.size(); ++i) {
+    if ((rc = stage_upload(b, (int)i, cfg))) return rc;
+    cfg += 3 * (size_t)b->tabs[i]->n_sites * b->R[i];
+  }
+  if (energies) {
+    for (int i = 0; i < b->n_slots; ++i)
+      if (!std::isfinite(energies[i])) return fail(SCEMC_ERR_ARG, "energy must be finite");
+    CUDA_TRY(cudaMemcpyAsync(b->d_energy, energies, 8 * b->n_slots, cudaMemcpyHostToDevice, b->stream));
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+  }
+  return SCEMC_OK;
+}
+
+int32_t scemc_batch_profile(scemc_batch* b, int32_t on) {
+  if (!b) return fail(SCEMC_ERR_ARG, "batch is NULL");
+  b->profiling = on != 0;
+  b->prof_ms = 0.0;
+  b->prof_passes = 0;
+  return SCEMC_OK;
+}
+
+int32_t scemc_batch_kernel_time(const scemc_batch* b, double* ms, int64_t* passes) {
+  if (!b) return fail(SCEMC_ERR_ARG, "batch is NULL");
+  if (ms) *ms = b->prof_ms;
+  if (passes) *passes = b->prof_passes;
+  return SCEMC_OK;
+}
+
+
 
 int32_t scemc_batch_download(const scemc_batch* b, double* configs, double* energies, int32_t* slot_of_rung,
                              int64_t* counters, int64_t* swaps, double* steps, double* max_drift) {
@@ -1686,11 +1804,10 @@ int32_t scemc_batch_download(const scemc_batch* b, double* configs, double* ener
   int32_t rc;
   if (configs) {
     double* cfg = configs;
-    for (size_t i = 0; i < b->tabs.size(); ++i)
-      for (int r = 0; r < b->R[i]; ++r) {
-        if ((rc = download_config(b, (int)i, r, cfg))) return rc;
-        cfg += 3 * (size_t)b->tabs[i]->n_sites;
-      }
+    for (size_t i = 0; i < b->tabs.size(); ++i) {
+      if ((rc = stage_download(b, (int)i, cfg))) return rc;
+      cfg += 3 * (size_t)b->tabs[i]->n_sites * b->R[i];
+    }
   }
   const int n = b->n_slots;
   if (energies) CUDA_TRY(cudaMemcpy(energies, b->d_energy, 8 * n, cudaMemcpyDeviceToHost));

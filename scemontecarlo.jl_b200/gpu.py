@@ -233,13 +233,44 @@ class GPUBatch:
         s = np.ascontiguousarray(np.broadcast_to(np.asarray(steps, np.float64), (self.n_slots,)))
         check(_lib.lib().scemc_batch_set_steps(self.h, ptr(s, C.c_double)))
 
-    def run(self, nsweeps, or_per_metropolis=0, exchange=False, exchange_interval=1, adapt_interval=0,
-            adapt_target=0.5, renorm_interval=0, measure_interval=0, lanes_per_site=0, mode=0, phase_done=0,
-            phase_total=0):
-        p = _lib.RunParams(int(nsweeps), int(or_per_metropolis), int(bool(exchange)), int(exchange_interval),
-                           int(adapt_interval), float(adapt_target), int(renorm_interval), int(measure_interval),
-                           int(lanes_per_site), int(mode), int(phase_done), int(phase_total))
+    @staticmethod
+    def params(nsweeps, or_per_metropolis=0, exchange=False, exchange_interval=1, adapt_interval=0,
+               adapt_target=0.5, renorm_interval=0, measure_interval=0, lanes_per_site=0, mode=0, phase_done=0,
+               phase_total=0) -> _lib.RunParams:
+        return _lib.RunParams(int(nsweeps), int(or_per_metropolis), int(bool(exchange)), int(exchange_interval),
+                              int(adapt_interval), float(adapt_target), int(renorm_interval), int(measure_interval),
+                              int(lanes_per_site), int(mode), int(phase_done), int(phase_total))
+
+    def run(self, nsweeps, **kw):
+        """Runs `nsweeps` compound sweeps (see scemc_run_params) and waits for them."""
+        p = self.params(nsweeps, **kw)
         check(_lib.lib().scemc_batch_run(self.h, C.byref(p)))
+
+    def run_async(self, p: _lib.RunParams):
+        """Enqueues a run on the batch stream; call sync() before touching the batch."""
+        check(_lib.lib().scemc_batch_run_async(self.h, C.byref(p)))
+
+    def sync(self):
+        check(_lib.lib().scemc_batch_sync(self.h))
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        check(_lib.lib().scemc_batch_stream(self.h, C.byref(s)))
+        return s.value or 0
+
+    def upload(self, configs, energies=None):
+        cfg = np.ascontiguousarray(configs, np.float64).reshape(-1)
+        en = None if energies is None else np.ascontiguousarray(energies, np.float64)
+        check(_lib.lib().scemc_batch_upload(self.h, ptr(cfg, C.c_double), None if en is None else ptr(en, C.c_double)))
+
+    def profile(self, on: bool):
+        check(_lib.lib().scemc_batch_profile(self.h, int(bool(on))))
+
+    def kernel_time(self):
+        """(summed device ms of the sweep passes, number of passes) since profile(True)."""
+        ms, n = C.c_double(), C.c_int64()
+        check(_lib.lib().scemc_batch_kernel_time(self.h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
 
     def renormalize(self):
         d = np.zeros(self.n_slots)

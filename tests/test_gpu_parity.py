@@ -1,0 +1,413 @@
+"""Parity of the CUDA sweep against the FP64 oracle (run on a B200: -m gpu).
+
+Every gate calls libscemc_cuda.so through the C ABI (via the package's ctypes
+API). Tolerances (the north-star parity bar):
+  * per-proposal dE: |dE32 - dE64| <= 1e-5 * sum|c| (sum|znew| + sum|zold|)
+    (the reference's scaled form, test_gpu.jl:168,174, with 1e-5 for FP32);
+  * accept/reject: identical on replay, except near-threshold ties where the
+    threshold -log(u)/beta (or 0) lies within that dE tolerance of dE64;
+  * proposals: the FP32-rounded reference keyed proposal (<= 1 FP32 ulp);
+  * total energy: FP64 device recompute within 1e-10 relative of the oracle;
+  * statistics: within the combined log-binning / jackknife error bars.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle as O
+import scemc
+from scemc import _lib, models
+
+pytestmark = pytest.mark.gpu
+
+ZB = (0.3, -1.2, 2.0)
+F32_ULP = 2.0 ** -23
+
+MODELS = {
+    "dimer": (4, models.dimer_terms(), (1, 1, 1), {}),
+    "dimer_zeeman": (4, models.dimer_terms(), (2, 1, 1), dict(magmoms=[2.2, 2.2, 1.0, 0.0], field=ZB)),
+    "biquadratic": (2, models.biquadratic_terms(3), (2, 2, 2), {}),
+    "biquadratic_zeeman": (2, models.biquadratic_terms(3), (2, 2, 2), dict(magmoms=[1.5, 0.7], field=ZB)),
+    "zeeman_only": (2, [], (2, 2, 1), dict(magmoms=[1.0, 2.0], field=ZB)),
+    "chain": (1, models.chain_terms(-0.05), (4, 4, 2), {}),
+    "threebody": (1, models.threebody_terms(0.05), (4, 2, 2), {}),
+    "fourbody": (1, models.fourbody_terms(0.03), (4, 2, 2), {}),
+    "mixed": (2, models.mixed_terms(7), (2, 2, 1), {}),
+    "high_l": (1, models.highl_terms(11, 4), (3, 2, 1), {}),
+    "sc_J1J2": (1, models.config1_sc().terms, (4, 4, 4), {}),
+    "bcc_l2_plaq_zeeman": (2, models.config2_bcc_l2().terms, (3, 3, 3), dict(magmoms=[2.0, 2.0], field=[0, 0, 1.0])),
+    "bcc_triangles": (2, models.config3_bcc_pt().terms, (3, 3, 3), {}),
+    "bcc_body4": (2, models.config4_bcc_body4().terms, (3, 3, 3), {}),
+    "fcc_l2_tri_zeeman": (4, models.config5_fcc(n=2).terms, (2, 2, 2), dict(magmoms=[2.0] * 4, field=[0.3] * 3)),
+}
+
+
+def build(name):
+    nca, terms, dims, kw = MODELS[name]
+    H = scemc.TiledHamiltonian(nca, terms, dims=dims, **kw)
+    OH = O.OracleHamiltonian(nca, terms, dims, **kw)
+    return H, OH
+
+
+def rand_cfg(n, seed):
+    return models.random_config(n, seed)
+
+
+def energy_scale(H):
+    """Typical |site energy| of a model: beta is chosen so moves are ~50/50."""
+    return 0.05
+
+
+def f32_normalised(v):
+    v = np.asarray(v, np.float64)
+    return (v / np.sqrt((v[0] * v[0] + v[1] * v[1]) + v[2] * v[2])).astype(np.float32)
+
+
+def check_pass(OH, cfg, rec, beta, kind, seed=None, sweep=None, step=None, orpass=0):
+    """Replays one recorded pass; returns (#ties, #attempted). cfg updated in place."""
+    prop, u, dE32, flag = rec
+    pre = cfg.copy()
+    dev_acc = (flag == 1).astype(np.uint8)
+    dE64, scale, oacc, c = OH.replay_sweep(cfg, prop.astype(np.float64), u, dev_acc, beta, want_c=True)
+    active = OH.array("site_active").astype(bool)
+    has_l1 = OH.array("site_has_l1").astype(bool)
+    visited = flag != 3
+    if kind == "metro":
+        assert np.array_equal(visited, active)
+    else:
+        assert np.array_equal(visited, active & has_l1)
+    att = visited & (flag != 2)
+    tol = 1e-5 * scale + 1e-30
+    # dE within the scaled FP32 tolerance
+    bad = att & (np.abs(dE32.astype(np.float64) - dE64) > tol)
+    assert not bad.any(), (np.nonzero(bad)[0][:5], dE32[bad][:5], dE64[bad][:5], scale[bad][:5])
+    # accept/reject identical except flagged ties
+    with np.errstate(divide="ignore"):
+        thr = -np.log(u) / beta
+    tie = (np.abs(dE64 - thr) <= tol) | (np.abs(dE64) <= tol)
+    mism = att & ((flag == 1) != oacc)
+    assert not (mism & ~tie).any(), np.nonzero(mism & ~tie)[0][:5]
+    n_sites = len(flag)
+    if kind == "metro":
+        for s in np.nonzero(active)[0]:
+            b0 = O.philox_block(seed, int(s) + 1, sweep, 0)
+            if O.philox_uniform(b0[0], b0[1]) < 0.2:
+                exp = (-pre[s]).astype(np.float32)
+            else:
+                e2, _ = O.keyed_proposal(seed, int(s) + 1, sweep, pre[s], step)
+                exp = f32_normalised(e2)
+            assert np.max(np.abs(prop[s] - exp)) <= F32_ULP, (s, prop[s], exp)
+    else:
+        for s in np.nonzero(visited)[0]:
+            h = np.array([c[s, 3], c[s, 1], c[s, 2]])
+            hn = np.linalg.norm(h)
+            if flag[s] == 2:
+                assert hn < 1e-9
+                continue
+            a = h / hn
+            e = pre[s]
+            r = 2.0 * np.dot(e, a) * a - e
+            exp = r / np.linalg.norm(r)
+            assert np.max(np.abs(prop[s] - exp)) <= 1e-4, (s, prop[s], exp)
+            b = O.philox_block(seed, int(s) + 1, sweep, orpass, tag=1)
+            assert u[s] == O.philox_uniform(b[0], b[1])
+    return int(tie[mism].sum()), int(att.sum()), n_sites
+
+
+REPLAY_CASES = [(m, 4, 2) for m in MODELS] + [
+    ("biquadratic", 1, 1), ("biquadratic", 32, 1), ("bcc_l2_plaq_zeeman", 1, 2), ("bcc_l2_plaq_zeeman", 32, 1),
+    ("high_l", 1, 1), ("fourbody", 32, 2), ("sc_J1J2", 8, 1), ("fcc_l2_tri_zeeman", 16, 2),
+]
+
+
+@pytest.mark.parametrize("name,lanes,mode", REPLAY_CASES, ids=[f"{m}-G{g}-mode{d}" for m, g, d in REPLAY_CASES])
+def test_sweep_replay(gpu, name, lanes, mode):
+    H, OH = build(name)
+    gH = scemc.GPUTiledHamiltonian(H)
+    seed, step, beta = 0xC0FFEE + lanes, 0.6, 1 / 0.05
+    n_or = 2 if H.site_has_l1.any() else 0
+    b = scemc.GPUBatch([gH], [1], [rand_cfg(H.n_sites, 7)], [seed], step)
+    b.set_betas([beta])
+    ties = att = 0
+    for sw in range(1, 5):
+        cfg = b.download()["configs"][0].copy()
+        b.record(True)
+        b.run(1, or_per_metropolis=n_or, lanes_per_site=lanes, mode=mode)
+        t, a, _ = check_pass(OH, cfg, b.fetch_record(-1), beta, "metro", seed=seed, sweep=sw, step=step)
+        ties, att = ties + t, att + a
+        for k in range(n_or):
+            t, a, _ = check_pass(OH, cfg, b.fetch_record(k), beta, "or", seed=seed, sweep=sw, orpass=k)
+            ties, att = ties + t, att + a
+        post = b.download()
+        np.testing.assert_array_equal(post["configs"][0], cfg)
+        # FP64 recompute of the device state vs the oracle's total energy of the same spins
+        E_dev = b.total_energy(0)
+        E_or = OH.total_energy(post["configs"][0])
+        assert abs(E_dev - E_or) <= 1e-10 * max(1.0, abs(E_or))
+        # the running (FP32 dE, fixed-point summed) energy tracks the recompute
+        assert abs(post["energies"][0] - E_or) <= 1e-5 * max(1.0, abs(E_or))
+    assert ties <= max(1, att // 100)
+
+
+def test_proposal_stream_is_the_reference_stream(gpu):
+    """A single chain's Metropolis draws are the reference's keyed stream (tag 0)."""
+    H, OH = build("chain")
+    gH = scemc.GPUTiledHamiltonian(H)
+    b = scemc.GPUBatch([gH], [1], [rand_cfg(H.n_sites, 1)], [0xBEEF], 0.6)
+    b.set_betas([1.0])
+    b.record(True)
+    b.run(1, lanes_per_site=1, mode=1)
+    prop, u, _, flag = b.fetch_record(-1)
+    for s in range(H.n_sites):
+        b0 = O.philox_block(0xBEEF, s + 1, 1, 0)
+        assert u[s] == O.philox_uniform(b0[2], b0[3])
+
+
+def test_energy_recompute_and_drift(gpu):
+    H, OH = build("biquadratic")
+    gH = scemc.GPUTiledHamiltonian(H)
+    cfg = rand_cfg(H.n_sites, 7)
+    gst = scemc.GPUChainState(gH, cfg, seed=0xC0FFEE)
+    E0 = OH.total_energy(np.asarray(cfg, np.float32).astype(np.float64))
+    assert abs(gst.energy - E0) <= 1e-10 * max(1, abs(E0))
+    st = scemc.ChainState(cfg, gst.energy)
+    scemc.gpu_run_sweeps(gst, gH, st, 1 / 0.05, 200, renorm_interval=0)
+    E = OH.total_energy(st.config)
+    drift = abs(gst.energy - E)
+    assert drift <= 1e-6 * max(1.0, abs(E)), drift
+    d = gst.renormalize()
+    assert d == pytest.approx(drift, rel=1e-3, abs=1e-15)
+    assert abs(gst.energy - OH.total_energy(scemc.to_host(st, gst).config)) <= 1e-10 * max(1.0, abs(E))
+
+
+def test_repeat_identity_lanes_and_modes(gpu):
+    H, _ = build("bcc_l2_plaq_zeeman")
+    gH = scemc.GPUTiledHamiltonian(H)
+    cfg = rand_cfg(H.n_sites, 3)
+    outs = []
+    for lanes, mode, seed in [(4, 2, 9), (4, 2, 9), (4, 1, 9), (1, 2, 9), (32, 1, 9), (4, 2, 10)]:
+        b = scemc.GPUBatch([gH], [1], [cfg], [seed], 0.6)
+        b.set_betas([1 / 0.05])
+        b.run(6, or_per_metropolis=1, lanes_per_site=lanes, mode=mode)
+        st = b.download()
+        outs.append((st["configs"][0], st["energies"][0], st["counters"][0].copy()))
+    # same seed, lanes and mode: bitwise
+    assert np.array_equal(outs[0][0], outs[1][0]) and outs[0][1] == outs[1][1]
+    assert np.array_equal(outs[0][2], outs[1][2])
+    # the launch form does not change the chain (same per-item arithmetic)
+    assert np.array_equal(outs[0][0], outs[2][0]) and outs[0][1] == outs[2][1]
+    # other lane counts reorder FP32 sums only: same chain unless a tie flips a decision
+    for k in (3, 4):
+        assert np.max(np.abs(outs[0][0] - outs[k][0])) < 1e-4
+    assert not np.array_equal(outs[0][0], outs[5][0])
+
+
+def test_inactive_sites_frozen(gpu):
+    H, _ = build("dimer")
+    gH = scemc.GPUTiledHamiltonian(H)
+    cfg = rand_cfg(H.n_sites, 7)
+    gst = scemc.GPUChainState(gH, cfg, seed=1)
+    st = scemc.ChainState(cfg, gst.energy)
+    scemc.gpu_run_sweeps(gst, gH, st, 1 / 0.05, 50, renorm_interval=20)
+    np.testing.assert_array_equal(st.config[2:], cfg[2:].astype(np.float32).astype(np.float64))
+
+
+def test_batch_of_uneven_lattices_equals_single_chains(gpu):
+    """Chains of different supercells in one batch follow exactly the trajectories
+    they follow alone (keyed RNG, per-item independence)."""
+    w = models.config3_bcc_pt(sizes=(2, 3))
+    Hs = [scemc.TiledHamiltonian(2, w.terms, dims=(s, s, s)) for s in (2, 3)]
+    gHs = [scemc.GPUTiledHamiltonian(H) for H in Hs]
+    cfgs = [rand_cfg(H.n_sites, 20 + i) for i, H in enumerate(Hs) for _ in range(3)]
+    seeds = [100 + i for i in range(6)]
+    betas = np.tile(1 / np.array([0.3e-3, 1e-3, 3e-3]), 2)
+    b = scemc.GPUBatch(gHs, [3, 3], cfgs, seeds, 0.6)
+    b.set_betas(betas)
+    b.run(5, lanes_per_site=2, mode=2)
+    got = b.download()
+    for i in range(6):
+        gH = gHs[i // 3]
+        one = scemc.GPUBatch([gH], [1], [cfgs[i]], [seeds[i]], 0.6)
+        one.set_betas([betas[i]])
+        one.run(5, lanes_per_site=2, mode=2)
+        st = one.download()
+        np.testing.assert_array_equal(got["configs"][i], st["configs"][0])
+        assert got["energies"][i] == st["energies"][0]
+
+
+def test_swap_payload_and_roundtrip(gpu):
+    H, _ = build("biquadratic")
+    gH = scemc.GPUTiledHamiltonian(H)
+    a = scemc.GPUChainState(gH, rand_cfg(H.n_sites, 1), seed=1)
+    b = scemc.GPUChainState(gH, rand_cfg(H.n_sites, 2), seed=2)
+    scemc.gpu_metropolis_sweep(a, gH, 20.0)
+    sa, sb = scemc.ChainState(None, 0), scemc.ChainState(None, 0)
+    scemc.to_host(sa, a), scemc.to_host(sb, b)
+    ca, cb = a.counters().copy(), b.counters().copy()
+    ia, ib = a.sweep_index, b.sweep_index
+    scemc.swap_payload(a, b)
+    ta, tb = scemc.ChainState(None, 0), scemc.ChainState(None, 0)
+    scemc.to_host(ta, a), scemc.to_host(tb, b)
+    np.testing.assert_array_equal(ta.config, sb.config)
+    np.testing.assert_array_equal(tb.config, sa.config)
+    assert ta.energy == sb.energy and tb.energy == sa.energy
+    assert np.array_equal(a.counters(), ca) and np.array_equal(b.counters(), cb)
+    assert (a.sweep_index, b.sweep_index) == (ia, ib)
+    # upload/download round trip keeps FP32 values exactly
+    scemc.from_host(a, sa)
+    scemc.to_host(ta, a)
+    np.testing.assert_array_equal(ta.config, sa.config)
+
+
+def test_guards(gpu):
+    H, _ = build("chain")
+    gH = scemc.GPUTiledHamiltonian(H)
+    gst = scemc.GPUChainState(gH, rand_cfg(H.n_sites, 1), seed=1)
+    with pytest.raises(ValueError):
+        scemc.gpu_metropolis_sweep(gst, gH, 1.0, workgroupsize=3)
+    with pytest.raises(_lib.ScemcArgumentError):
+        _lib.check(_lib.lib().scemc_metropolis_sweep(gst.h, gH.h, 1.0, 3, None))
+    bad = np.full((H.n_sites, 3), np.nan)
+    with pytest.raises(scemc.ScemcError):
+        scemc.GPUChainState(gH, bad, seed=1, energy=0.0)
+    # lmax > 6 refused at table upload (gpu_hamiltonian.jl:439-440)
+    f = np.zeros((15, 3))
+    f[0, 0] = 1.0
+    H7 = scemc.TiledHamiltonian(1, [scemc.MultipoleTerm(1.0, [1, 1], [(0, 0, 0), (1, 0, 0)], [7, 1], f)],
+                                dims=(3, 1, 1))
+    with pytest.raises(ValueError):
+        scemc.GPUTiledHamiltonian(H7)
+    d = H7.desc()
+    h = _lib.C.c_void_p()
+    assert _lib.lib().scemc_tables_create(_lib.C.byref(d), _lib.C.byref(h)) == _lib.ERR_UNSUPPORTED
+    # a corrupted table is refused, not uploaded
+    Hc, _ = build("biquadratic")
+    Hc.site_prog = Hc.site_prog.copy()
+    Hc.site_prog[0] += 1
+    with pytest.raises(_lib.ScemcArgumentError):
+        scemc.GPUTiledHamiltonian(Hc)
+
+
+def test_barrier_timeout_is_bounded(gpu):
+    """Failure detection: a grid barrier that can never complete gives up after its
+    bound and reports SCEMC_ERR_TIMEOUT; the context stays usable."""
+    assert _lib.lib().scemc_selftest_barrier_timeout(50_000_000) == _lib.ERR_TIMEOUT
+    H, _ = build("chain")
+    gH = scemc.GPUTiledHamiltonian(H)
+    gst = scemc.GPUChainState(gH, rand_cfg(H.n_sites, 1), seed=1)
+    assert scemc.gpu_metropolis_sweep(gst, gH, 1.0) >= 0
+
+
+# -- statistics -------------------------------------------------------------------------
+def langevin(x):
+    return 1.0 / math.tanh(x) - 1.0 / x
+
+
+def test_dimer_langevin_and_pt_marginals(gpu):
+    """<E> = J L(beta|J|) at every rung of an exchanging 3-rung ladder (test_gpu_pt.jl:13-42)."""
+    J = -0.02
+    gH = scemc.GPUTiledHamiltonian(models.dimer(J=J))
+    kts = abs(J) * np.array([0.3, 0.6, 1.2])
+    r = scemc.gpu_run_pt(gH, kT=kts, sweeps_therm=500, sweeps_measure=20000, measure_interval=5,
+                         exchange_interval=10, seed=31)
+    for p, kt in zip(r.points, kts):
+        exact = J * langevin(abs(J) / kt)
+        E, err = p.stats["energy"].mean[0], p.stats["energy"].err[0]
+        assert abs(E - exact) < 5 * err + 1e-3 * abs(J)
+        assert abs(E - exact) < 0.04 * abs(J)
+        np.testing.assert_array_equal(p.stats["sublattice_m"].mean[6:12], np.zeros(6))
+    assert len(r.swap_acceptance) == 2 and np.all((r.swap_acceptance > 0) & (r.swap_acceptance <= 1))
+
+
+def test_exchange_rate_limits(gpu):
+    """test_gpu_pt.jl:44-60: a degenerate ladder always swaps; a wide one rarely, and
+    the rung energies are ordered."""
+    gH = scemc.GPUTiledHamiltonian(models.dimer())
+    r = scemc.gpu_run_pt(gH, kT=[0.049999, 0.05], sweeps_therm=100, sweeps_measure=400, exchange_interval=5,
+                         seed=1)
+    assert r.swap_acceptance[0] > 0.95
+    H = scemc.TiledHamiltonian(1, models.chain_terms(-0.05), dims=(4, 4, 2))
+    gH2 = scemc.GPUTiledHamiltonian(H)
+    r2 = scemc.gpu_run_pt(gH2, kT=[0.002, 0.2], sweeps_therm=200, sweeps_measure=1000, exchange_interval=5, seed=2)
+    assert r2.swap_acceptance[0] < 0.2
+    Es = [p.stats["energy"].mean[0] for p in r2.points]
+    assert Es[0] < Es[1]
+
+
+def test_single_moment_in_a_field(gpu):
+    """<e_z> = -L(beta h) for h e_z, and a Zeeman-only moment: test_gpu.jl:458-484."""
+    c0 = 0.3
+    h = c0 * scemc.N1
+    gH = scemc.GPUTiledHamiltonian(scemc.TiledHamiltonian(1, models.single_site_terms(c0)))
+    r = scemc.gpu_run_pt(gH, kT=[h / 1.0, h / 2.0], exchange=False, sweeps_therm=500, sweeps_measure=40000,
+                         measure_interval=2, step=1.2, seed=202)
+    for p, bh in zip(r.points, (1.0, 2.0)):
+        assert p.stats["energy"].mean[0] / h == pytest.approx(-langevin(bh), abs=0.03)
+
+
+def compare_stats(a, b, names, n_sigma=3.0):
+    """Agreement within combined error bars; returns the list of z-scores."""
+    zs = []
+    for n in names:
+        ma, ea = np.asarray(a[n][0]), np.asarray(a[n][1])
+        mb, eb = np.asarray(b[n][0]), np.asarray(b[n][1])
+        z = np.abs(ma - mb) / np.sqrt(ea ** 2 + eb ** 2 + 1e-300)
+        zs += list(z)
+        assert np.all(z < n_sigma), (n, ma, mb, ea, eb)
+    return zs
+
+
+def as_tuple_stats(stats):
+    return {k: (v.mean, v.err) for k, v in stats.items()}
+
+
+def test_sc_J1J2_statistics_match_cpu_run_mc(gpu):
+    """Config-1 physics (sc 8^3 J1/J2, kT 0.5 meV): E, C, |m|, chi, U and the sublattice
+    magnetisation of the device chain agree with the oracle's run_mc within errors."""
+    w = models.config1_sc()
+    H = w.hamiltonians()[0]
+    OH = O.OracleHamiltonian(1, w.terms, (8, 8, 8))
+    kT = float(w.kts[0])
+    gH = scemc.GPUTiledHamiltonian(H)
+    r = scemc.gpu_run_pt(gH, kT=[kT], exchange=False, sweeps_therm=2000, sweeps_measure=20000, seed=1)
+    ch = O.OracleChain(OH, models.random_config(H.n_sites, 1), seed=1)
+    ost = ch.run_mc(kT, 2000, 20000)
+    names = ["energy", "specific_heat", "absm", "susceptibility", "binder", "sublattice_m"]
+    zs = compare_stats(as_tuple_stats(r.points[0].stats), ost, names, n_sigma=3.5)
+    assert sum(z > 2.0 for z in zs) <= 2
+
+
+def test_bcc_multipole_or_statistics_match_cpu(gpu):
+    """Metropolis + overrelaxation on the l<=2 + plaquette + Zeeman model (config-2
+    shape, 4^3): device vs oracle run_mc energies and magnetisation within errors."""
+    w = models.config2_bcc_l2(n=4)
+    H = w.hamiltonians()[0]
+    OH = O.OracleHamiltonian(2, w.terms, (4, 4, 4), magmoms=w.magmoms, field=w.field)
+    kT = 1.0e-3
+    gH = scemc.GPUTiledHamiltonian(H)
+    r = scemc.gpu_run_pt(gH, kT=[kT], exchange=False, sweeps_therm=1000, sweeps_measure=8000, or_per_metropolis=1,
+                         seed=2)
+    ch = O.OracleChain(OH, models.random_config(H.n_sites, 2), seed=2)
+    ost = ch.run_mc(kT, 1000, 8000, n_or=1)
+    p = r.points[0]
+    assert 0.0 < p.acceptance_or < 1.0
+    zs = compare_stats(as_tuple_stats(p.stats), ost, ["energy", "absm", "m2"], n_sigma=4.0)
+    assert sum(z > 2.0 for z in zs) <= 1
+
+
+def test_pt_energies_match_cpu_run_pt(gpu):
+    w = models.config3_bcc_pt()
+    dims = (3, 3, 3)
+    H = scemc.TiledHamiltonian(2, w.terms, dims=dims)
+    OH = O.OracleHamiltonian(2, w.terms, dims)
+    kts = np.geomspace(0.3, 3.0, 4) * 1e-3
+    gH = scemc.GPUTiledHamiltonian(H)
+    r = scemc.gpu_run_pt(gH, kT=kts, exchange_interval=1, sweeps_therm=1000, sweeps_measure=6000, seed=3)
+    chains = [O.OracleChain(OH, models.random_config(H.n_sites, 30 + i), seed=300 + i) for i in range(4)]
+    pts, swaps = O.run_pt(OH, chains, kts, 1000, 6000, exchange_interval=1)
+    zs = []
+    for p, q in zip(r.points, pts):
+        zs += compare_stats(as_tuple_stats(p.stats), q, ["energy", "absm"], n_sigma=4.0)
+    assert sum(z > 2.0 for z in zs) <= 2
+    np.testing.assert_allclose(r.swap_acceptance, swaps, atol=0.1)
