@@ -182,25 +182,29 @@ def test_energy_recompute_and_drift(gpu):
 
 
 def test_repeat_identity_lanes_and_modes(gpu):
+    """Bitwise repeatability for a fixed (seed, lanes, launch form); the launch form
+    does not change the chain; other lane counts only reorder FP32 sums, so a
+    Metropolis-only chain stays on the same trajectory (overrelaxation is a
+    chaotic deterministic map, so it is compared through the replay gates only)."""
     H, _ = build("bcc_l2_plaq_zeeman")
     gH = scemc.GPUTiledHamiltonian(H)
     cfg = rand_cfg(H.n_sites, 3)
-    outs = []
-    for lanes, mode, seed in [(4, 2, 9), (4, 2, 9), (4, 1, 9), (1, 2, 9), (32, 1, 9), (4, 2, 10)]:
+
+    def run(lanes, mode, seed, n_or):
         b = scemc.GPUBatch([gH], [1], [cfg], [seed], 0.6)
-        b.set_betas([1 / 0.05])
-        b.run(6, or_per_metropolis=1, lanes_per_site=lanes, mode=mode)
+        b.set_betas([1 / 0.002])
+        b.run(6, or_per_metropolis=n_or, lanes_per_site=lanes, mode=mode)
         st = b.download()
-        outs.append((st["configs"][0], st["energies"][0], st["counters"][0].copy()))
-    # same seed, lanes and mode: bitwise
-    assert np.array_equal(outs[0][0], outs[1][0]) and outs[0][1] == outs[1][1]
-    assert np.array_equal(outs[0][2], outs[1][2])
-    # the launch form does not change the chain (same per-item arithmetic)
-    assert np.array_equal(outs[0][0], outs[2][0]) and outs[0][1] == outs[2][1]
-    # other lane counts reorder FP32 sums only: same chain unless a tie flips a decision
-    for k in (3, 4):
-        assert np.max(np.abs(outs[0][0] - outs[k][0])) < 1e-4
-    assert not np.array_equal(outs[0][0], outs[5][0])
+        return st["configs"][0], st["energies"][0], st["counters"][0].copy()
+
+    a, b_, c = run(4, 2, 9, 1), run(4, 2, 9, 1), run(4, 1, 9, 1)
+    assert np.array_equal(a[0], b_[0]) and a[1] == b_[1] and np.array_equal(a[2], b_[2])
+    assert np.array_equal(a[0], c[0]) and a[1] == c[1]
+    m = [run(g, 2, 9, 0) for g in (4, 1, 32)]
+    for k in (1, 2):
+        assert np.max(np.abs(m[0][0] - m[k][0])) < 1e-5
+        assert np.array_equal(m[0][2], m[k][2])
+    assert not np.array_equal(run(4, 2, 10, 1)[0], a[0])
 
 
 def test_inactive_sites_frozen(gpu):
@@ -346,15 +350,19 @@ def test_single_moment_in_a_field(gpu):
         assert p.stats["energy"].mean[0] / h == pytest.approx(-langevin(bh), abs=0.03)
 
 
-def compare_stats(a, b, names, n_sigma=3.0):
+def compare_stats(a, b, names, n_sigma=3.0, comps=None):
     """Agreement within combined error bars; returns the list of z-scores."""
-    zs = []
+    zs, report = [], []
     for n in names:
         ma, ea = np.asarray(a[n][0]), np.asarray(a[n][1])
         mb, eb = np.asarray(b[n][0]), np.asarray(b[n][1])
+        if comps and n in comps:
+            ma, ea, mb, eb = ma[comps[n]], ea[comps[n]], mb[comps[n]], eb[comps[n]]
         z = np.abs(ma - mb) / np.sqrt(ea ** 2 + eb ** 2 + 1e-300)
         zs += list(z)
-        assert np.all(z < n_sigma), (n, ma, mb, ea, eb)
+        report.append((n, ma, mb, ea, eb, z))
+    for r in report:
+        assert np.all(r[5] < n_sigma), report
     return zs
 
 
@@ -363,37 +371,43 @@ def as_tuple_stats(stats):
 
 
 def test_sc_J1J2_statistics_match_cpu_run_mc(gpu):
-    """Config-1 physics (sc 8^3 J1/J2, kT 0.5 meV): E, C, |m|, chi, U and the sublattice
-    magnetisation of the device chain agree with the oracle's run_mc within errors."""
+    """Config-1 physics (sc 8^3 J1/J2, kT 0.5 meV): E, C, |m|, chi and U of the device
+    chain agree with the oracle's run_mc within their error bars. (The vector m of
+    an isotropic ferromagnet only diffuses in direction, so its components are not
+    compared here; the field-bearing model below compares sublattice vectors.)"""
     w = models.config1_sc()
     H = w.hamiltonians()[0]
     OH = O.OracleHamiltonian(1, w.terms, (8, 8, 8))
     kT = float(w.kts[0])
     gH = scemc.GPUTiledHamiltonian(H)
     r = scemc.gpu_run_pt(gH, kT=[kT], exchange=False, sweeps_therm=2000, sweeps_measure=20000, seed=1)
-    ch = O.OracleChain(OH, models.random_config(H.n_sites, 1), seed=1)
+    ch = O.OracleChain(OH, models.random_config(H.n_sites, 11), seed=11)
     ost = ch.run_mc(kT, 2000, 20000)
-    names = ["energy", "specific_heat", "absm", "susceptibility", "binder", "sublattice_m"]
-    zs = compare_stats(as_tuple_stats(r.points[0].stats), ost, names, n_sigma=3.5)
-    assert sum(z > 2.0 for z in zs) <= 2
+    names = ["energy", "specific_heat", "absm", "susceptibility", "binder"]
+    zs = compare_stats(as_tuple_stats(r.points[0].stats), ost, names, n_sigma=4.0)
+    assert sum(z > 2.0 for z in zs) <= 1, zs
+    assert abs(r.points[0].acceptance_metropolis - ost["acceptance_metropolis"]) < 0.02
 
 
 def test_bcc_multipole_or_statistics_match_cpu(gpu):
     """Metropolis + overrelaxation on the l<=2 + plaquette + Zeeman model (config-2
-    shape, 4^3): device vs oracle run_mc energies and magnetisation within errors."""
+    shape, 4^3) at kT = 4 meV, where it equilibrates quickly: energy, |m| and the
+    field-aligned sublattice magnetisation agree with the oracle's run_mc."""
     w = models.config2_bcc_l2(n=4)
     H = w.hamiltonians()[0]
     OH = O.OracleHamiltonian(2, w.terms, (4, 4, 4), magmoms=w.magmoms, field=w.field)
-    kT = 1.0e-3
+    kT = 4.0e-3
     gH = scemc.GPUTiledHamiltonian(H)
-    r = scemc.gpu_run_pt(gH, kT=[kT], exchange=False, sweeps_therm=1000, sweeps_measure=8000, or_per_metropolis=1,
+    r = scemc.gpu_run_pt(gH, kT=[kT], exchange=False, sweeps_therm=2000, sweeps_measure=20000, or_per_metropolis=1,
                          seed=2)
     ch = O.OracleChain(OH, models.random_config(H.n_sites, 2), seed=2)
-    ost = ch.run_mc(kT, 1000, 8000, n_or=1)
+    ost = ch.run_mc(kT, 2000, 20000, n_or=1)
     p = r.points[0]
     assert 0.0 < p.acceptance_or < 1.0
-    zs = compare_stats(as_tuple_stats(p.stats), ost, ["energy", "absm", "m2"], n_sigma=4.0)
-    assert sum(z > 2.0 for z in zs) <= 1
+    assert abs(p.acceptance_or - ost["acceptance_or"]) < 0.02
+    zs = compare_stats(as_tuple_stats(p.stats), ost, ["energy", "specific_heat", "absm", "m2", "sublattice_m"],
+                       n_sigma=4.0, comps={"sublattice_m": [2, 5]})
+    assert sum(z > 2.0 for z in zs) <= 1, zs
 
 
 def test_pt_energies_match_cpu_run_pt(gpu):
@@ -401,13 +415,13 @@ def test_pt_energies_match_cpu_run_pt(gpu):
     dims = (3, 3, 3)
     H = scemc.TiledHamiltonian(2, w.terms, dims=dims)
     OH = O.OracleHamiltonian(2, w.terms, dims)
-    kts = np.geomspace(0.3, 3.0, 4) * 1e-3
+    kts = np.geomspace(1.0, 6.0, 4) * 1e-3
     gH = scemc.GPUTiledHamiltonian(H)
-    r = scemc.gpu_run_pt(gH, kT=kts, exchange_interval=1, sweeps_therm=1000, sweeps_measure=6000, seed=3)
+    r = scemc.gpu_run_pt(gH, kT=kts, exchange_interval=1, sweeps_therm=2000, sweeps_measure=20000, seed=3)
     chains = [O.OracleChain(OH, models.random_config(H.n_sites, 30 + i), seed=300 + i) for i in range(4)]
-    pts, swaps = O.run_pt(OH, chains, kts, 1000, 6000, exchange_interval=1)
+    pts, swaps = O.run_pt(OH, chains, kts, 2000, 20000, exchange_interval=1)
     zs = []
     for p, q in zip(r.points, pts):
         zs += compare_stats(as_tuple_stats(p.stats), q, ["energy", "absm"], n_sigma=4.0)
-    assert sum(z > 2.0 for z in zs) <= 2
-    np.testing.assert_allclose(r.swap_acceptance, swaps, atol=0.1)
+    assert sum(z > 2.0 for z in zs) <= 2, zs
+    np.testing.assert_allclose(r.swap_acceptance, swaps, atol=0.05)
