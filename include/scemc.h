@@ -240,6 +240,28 @@ int32_t scemc_color_sites(int32_t n_sites, const int32_t* site_ptr, const int32_
  * wait gives up as designed (SCEMC_OK would mean the bound did not fire). */
 int32_t scemc_selftest_barrier_timeout(int64_t limit_ns);
 
+/* Allocation-free FP64 energy recompute (no counterpart in the reference; an
+ * addition for callers that cannot allocate device memory when they need an
+ * energy: a host whose own pool allocator owns all device memory and lends the
+ * library its buffers, or a time-critical loop that must not pay cudaMalloc's
+ * device-wide synchronisation).
+ *   spins:    caller-owned device array of float4 (x, y, z, unused), n_sites x
+ *             replicas, site-major / replica-minor (spins[site * replicas + r]);
+ *   energies: caller-owned device array of replicas doubles (output);
+ *   stream:   cudaStream_t to enqueue on (NULL = the legacy default stream).
+ * Same arithmetic as scemc_total_energy. The call enqueues two kernels and returns;
+ * the energies are ready when the stream reaches that point. It calls no
+ * allocator: its scratch is a fixed device array of 65536 doubles (512 KiB) that
+ * every GPU loading the library holds until exit, so ceil(n_instances / 1024) x
+ * replicas must not exceed 65536 (larger requests return SCEMC_ERR_ARG). The first
+ * call on each device looks up that array's device address (with the device
+ * current); make that first call before any stream capture. All calls share the
+ * array: calls whose kernels overlap on the GPU (for example on two streams) race
+ * and must be serialised by the caller. The kernels write every partial sum they
+ * read, so nothing in the array needs to start at zero. */
+int32_t scemc_total_energy_static(const scemc_tables* t, const void* spins, int32_t replicas, double* energies,
+                                  void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -38,6 +38,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1916,3 +1917,100 @@ int32_t scemc_selftest_barrier_timeout(int64_t limit_ns) {
 }
 
 }  // extern "C"
+
+// =============================================================================
+// Allocation-free FP64 energy recompute.
+//
+// Some callers cannot call cudaMalloc at the moment they need an energy: a host
+// that owns all device memory through its own pool allocator (a Julia CUDA.jl
+// program that hands the library only its arrays), or a time-critical loop that
+// must not pay cudaMalloc's device-wide synchronisation. For them this variant of
+// the FP64 recompute takes caller-owned device buffers and keeps its only scratch
+// (the per-chunk partial sums) in a fixed file-scope device array instead of the
+// buffer scemc_total_energy allocates. The array holds kStaticScratch doubles
+// (512 KiB) on every GPU that loads the library, until the process exits.
+// =============================================================================
+namespace {
+
+constexpr int kStaticScratch = 65536;  // doubles: n_chunks(1024 instances each) x replicas
+static __device__ __align__(256) double g_energy_scratch[kStaticScratch];
+
+constexpr int kMaxDevices = 64;
+double* g_scratch_ptr[kMaxDevices] = {nullptr};
+std::mutex g_scratch_mu;
+
+// Same arithmetic and chunking as k_energy_chunks, with the lattice passed by value.
+__global__ void __launch_bounds__(256) k_energy_chunks_static(DevLattice L, const float4* spins, int R,
+                                                              double* partial, int n_chunks) {
+  const int chunk = blockIdx.x, r = blockIdx.y;
+  double acc = 0.0;
+  for (int k = 0; k < kChunk / 256; ++k) {
+    const int64_t i = (int64_t)chunk * kChunk + k * 256 + threadIdx.x;
+    if (i >= L.n_inst) break;
+    const int t = L.inst_term[i];
+    const int off = L.inst_ptr[i];
+    double Ei = 0.0;
+    for (int e = L.eprog_ptr[t]; e < L.eprog_ptr[t + 1]; ++e) {
+      double p = 1.0;
+      const int f0 = L.efac_ptr[e], nf = L.efac_ptr[e + 1] - f0;
+      for (int m = 0; m < nf; ++m) {
+        const float4 v = spins[(int64_t)L.inst_sites[off + m] * R + r];
+        p *= zval_f64(L.efac_row[f0 + m], (double)v.x, (double)v.y, (double)v.z);
+      }
+      Ei += L.eent_w[e] * p;
+    }
+    acc += L.term_coef[t] * Ei;
+  }
+  __shared__ double red[256];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = 128; o >= 1; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[(size_t)r * n_chunks + chunk] = red[0];
+}
+
+__global__ void k_energy_fold_static(const double* partial, int n_chunks, int R, double* out) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= R) return;
+  double E = 0.0;
+  for (int c = 0; c < n_chunks; ++c) E += partial[(size_t)r * n_chunks + c];
+  out[r] = E;
+}
+
+}  // namespace
+
+extern "C" int32_t scemc_total_energy_static(const scemc_tables* t, const void* spins, int32_t replicas,
+                                             double* energies, void* stream) {
+  if (!t || !spins || !energies) return fail(SCEMC_ERR_ARG, "NULL argument");
+  if (replicas < 1) return fail(SCEMC_ERR_ARG, "replicas must be >= 1");
+  const int64_t n_chunks = std::max<int64_t>(1, (t->n_inst + kChunk - 1) / kChunk);
+  if (n_chunks * replicas > kStaticScratch)
+    return fail(SCEMC_ERR_ARG, "scemc_total_energy_static: ceil(n_instances/1024) x replicas = " +
+                                   std::to_string(n_chunks * replicas) + " exceeds the fixed scratch of " +
+                                   std::to_string(kStaticScratch) + " partial sums");
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return fail(SCEMC_ERR_ARG, "device index out of range");
+  double* scratch = nullptr;
+  {
+    // One-time set-up per device, with that device current: the host-side name of
+    // g_energy_scratch is not a device address, so its address is looked up here.
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    if (!g_scratch_ptr[dev]) {
+      void* p = nullptr;
+      CUDA_TRY(cudaGetSymbolAddress(&p, g_energy_scratch));
+      g_scratch_ptr[dev] = static_cast<double*>(p);
+    }
+    scratch = g_scratch_ptr[dev];
+  }
+  DevLattice L = t->dl;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  k_energy_chunks_static<<<dim3((unsigned)n_chunks, (unsigned)replicas), 256, 0, st>>>(
+      L, static_cast<const float4*>(spins), replicas, scratch, (int)n_chunks);
+  CUDA_TRY(cudaGetLastError());
+  k_energy_fold_static<<<(replicas + 127) / 128, 128, 0, st>>>(scratch, (int)n_chunks, replicas, energies);
+  CUDA_TRY(cudaGetLastError());
+  return SCEMC_OK;
+}
