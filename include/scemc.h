@@ -182,6 +182,8 @@ typedef struct scemc_run_params {
    * (phase_total; 0 means phase_done + nsweeps). */
   int64_t phase_done;
   int64_t phase_total;
+  int32_t kernel;     /* 0 = auto, 1 = generic record walk, 2 = row-parallel fast kernel */
+  int32_t proposals;  /* 0 = auto, 1 = precompute a pass's Metropolis proposals, 2 = inline */
 } scemc_run_params;
 
 /* Inverse temperatures per rung (n_slots values, table-major like the slots). */

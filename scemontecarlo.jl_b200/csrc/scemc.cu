@@ -37,6 +37,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <array>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -111,6 +113,15 @@ struct DevLattice {
   const int32_t* efac_ptr;  // 0-based
   const int8_t* efac_row;   // 0-based
   const double* term_coef;
+  // row-parallel fast tables (lmax 1 or 2, every program of a fast kind); fast == 0 otherwise
+  int32_t fast, dmax;            // dmax: largest number of distinct neighbours of a site
+  int32_t rmax, pad2;            // rmax: largest number of fast records of a site
+  const int32_t* nb_ptr;         // n_sites+1: distinct neighbours of site s
+  const int32_t* nb_list;        // 0-based site ids
+  const int32_t* fr_ptr;         // n_sites+1: fast records of site s
+  const uint32_t* fr_cnt;        // per site: n_pair | n_trip << 8 | n_quad << 16 | n_one << 24
+  const uint2* frec;             // {kind<<26 | tensor offset, local neighbour indices (8 bits each)}
+  const float* ftensor;          // dense blocks, rows padded to the kernel's row count
 };
 
 // Grid barrier state (one per ensemble).
@@ -152,6 +163,11 @@ struct SweepArgs {
   double* rec_u;
   float* rec_dE;
   uint8_t* rec_acc;
+  // fast kernel: precomputed Metropolis proposals (null = computed inline)
+  const int32_t* item_base;  // max_colors+1: first global item of each colour
+  float4* prop;
+  double* propu;
+  int32_t dmax, rmax;
 };
 
 __device__ __forceinline__ unsigned long long globaltimer() {
@@ -513,6 +529,292 @@ __global__ void k_barrier_selftest(GridSync* gs, long long limit_ns) {
   grid_barrier(gs, gridDim.x + 1, limit_ns);
 }
 
+// ---------------------------------------------------------------------------
+// Row-parallel fast sweep (lmax 1 or 2; every program a dense l in {1,2} kind).
+// A group of G lanes owns one (site, replica) item; lane t owns coefficient row
+// t+1 (rows 1..NR; the l = 0 row never changes dE). Phase A gathers the site's
+// distinct neighbours once and writes their Z rows to shared memory; phase B walks
+// the site's records with every lane on the same record (per-neighbour merged
+// NR x NR pair blocks, l = 1 triplets and quads, one merged body-1 vector); phase C
+// reduces dE = sum_t c_t (znew_t - zold_t) with a fixed butterfly, so the result
+// does not depend on the launch shape.
+// ---------------------------------------------------------------------------
+constexpr int F_PAIR = 1, F_TRIP = 2, F_QUAD = 3, F_ONE = 4;
+
+template <int NR>
+__device__ __forceinline__ void zrow_nr(float x, float y, float z, float* o) {
+  zrow_l1(x, y, z, o);
+  if (NR > 3) zrow_l2(x, y, z, o + 3);
+}
+
+// Shared-memory floats one warp of the fast kernel uses (host and device agree):
+// rmax records (uint2) then dmax Z rows of NR floats, each region a multiple of 16 bytes.
+__host__ __device__ __forceinline__ size_t fast_rec_floats(int rmax) { return (2 * (size_t)rmax + 3) & ~(size_t)3; }
+__host__ __device__ __forceinline__ size_t fast_group_floats(int dmax, int rmax, int NR) {
+  return fast_rec_floats(rmax) + (((size_t)dmax * NR + 3) & ~(size_t)3);
+}
+
+template <int N>
+__device__ __forceinline__ float pick(const float* v, int k) {
+  float r = 0.0f;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+    if (i == k) r = v[i];
+  return r;
+}
+
+__device__ __forceinline__ int find_colour(const int32_t* base, int n, int idx) {
+  int lo = 0, hi = n;  // base[lo] <= idx < base[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (base[mid] <= idx) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Metropolis proposals of every item of the pass (they depend only on the item's
+// own spin, which no earlier colour changes).
+template <bool PERSIST>
+__device__ void make_proposals(const SweepArgs& a) {
+  const int total = a.item_base[a.max_colors];
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    const int col = find_colour(a.item_base, a.max_colors, idx);
+    const int item = idx - a.item_base[col];
+    const int32_t* seg_c = a.seg + (size_t)col * (a.n_lat + 1);
+    const int li = find_lattice(seg_c, a.n_lat, item);
+    const DevLattice& L = a.lat[li];
+    const int local = item - seg_c[li];
+    const int q = local / L.R, r = local - (local / L.R) * L.R;
+    const int s = L.color_sites[L.color_ptr[col] + q];
+    const int rung = a.rung_of_slot[L.slot0 + r];
+    const float4 e = load_spin<PERSIST>(a.spins + L.spin_off + (int64_t)s * L.R + r);
+    float px, py, pz;
+    const double u = keyed_proposal(a.seed[rung], (uint32_t)(s + 1), a.sweep, e.x, e.y, e.z, a.step[rung], px, py, pz);
+    a.prop[idx] = make_float4(px, py, pz, 0.0f);
+    a.propu[idx] = u;
+  }
+}
+
+template <int LMAX, bool PERSIST>
+__device__ void fast_colour(const SweepArgs& a, int col, unsigned long long* s_dE, unsigned int* s_cnt,
+                            float* zsm) {
+  // One warp per (site, replica) item: lane = slice * G + row. The G row lanes own
+  // coefficient rows 1..NR; the S = 32 / G slices split the site's records
+  // (record j goes to slice j % S) and are summed with a fixed butterfly.
+  constexpr int NR = (LMAX + 1) * (LMAX + 1) - 1;
+  constexpr int G = NR <= 4 ? 4 : 8;
+  constexpr int S = 32 / G;
+  const int32_t* seg_c = a.seg + (size_t)col * (a.n_lat + 1);
+  const int n_items = seg_c[a.n_lat];
+  const int lane = threadIdx.x & 31;
+  const int row = lane % G, slice = lane / G;
+  const int wib = threadIdx.x >> 5;
+  const int warps_per_block = blockDim.x >> 5;
+  const int warp = blockIdx.x * warps_per_block + wib;
+  const int n_warps = gridDim.x * warps_per_block;
+  const size_t per_warp = fast_group_floats(a.dmax, a.rmax, NR);
+  uint2* rb = reinterpret_cast<uint2*>(zsm + (size_t)wib * per_warp);
+  float* zb = zsm + (size_t)wib * per_warp + fast_rec_floats(a.rmax);
+  const bool do_or = a.pass >= 0;
+  for (int item = warp; item < n_items; item += n_warps) {  // warp-uniform
+    const int li = find_lattice(seg_c, a.n_lat, item);
+    const DevLattice& L = a.lat[li];
+    const int local = item - seg_c[li];
+    const int R = L.R;
+    const int q = local / R;
+    const int r = local - q * R;
+    const int s = L.color_sites[L.color_ptr[col] + q];
+    const int slot = L.slot0 + r;
+    const float4* __restrict__ sp = a.spins + L.spin_off;
+    if (do_or && !L.has_l1[s]) continue;  // warp-uniform
+    const int n0 = L.nb_ptr[s], nd = L.nb_ptr[s + 1] - n0;
+    const int j0 = L.fr_ptr[s], nrec = L.fr_ptr[s + 1] - j0;
+    // every record and neighbour spin of the site is requested before any is used
+    for (int k = lane; k < nrec; k += 32) rb[k] = __ldg(L.frec + j0 + k);
+    for (int k = lane; k < nd; k += 32) {
+      const int nb = __ldg(L.nb_list + n0 + k);
+      const float4 v = load_spin<PERSIST>(sp + (int64_t)nb * R + r);
+      zrow_nr<NR>(v.x, v.y, v.z, zb + k * NR);
+    }
+    __syncwarp();
+    const uint32_t cnt = L.fr_cnt[s];
+    const int n_pair = (int)(cnt & 0xffu), n_trip = (int)((cnt >> 8) & 0xffu), n_quad = (int)((cnt >> 16) & 0xffu);
+    const int n_one = (int)(cnt >> 24);
+    float acc = 0.0f, acc2 = 0.0f;
+    // pairs: each row lane dots its W row with the neighbour's Z row
+    if (row < NR) {
+#pragma unroll 4
+      for (int j = slice; j < n_pair; j += S) {
+        const uint2 fr = rb[j];
+        const float* z = zb + (fr.y & 0xffu) * NR;
+        const float* w = L.ftensor + (fr.x & kOffMask) + row * NR;
+        if (NR == 8) {
+          const float4 w0 = __ldg(reinterpret_cast<const float4*>(w));
+          const float4 w1 = __ldg(reinterpret_cast<const float4*>(w) + 1);
+          const float4 z0 = *reinterpret_cast<const float4*>(z);
+          const float4 z1 = *reinterpret_cast<const float4*>(z + 4);
+          acc = fmaf(w0.x, z0.x, acc);
+          acc2 = fmaf(w0.y, z0.y, acc2);
+          acc = fmaf(w0.z, z0.z, acc);
+          acc2 = fmaf(w0.w, z0.w, acc2);
+          acc = fmaf(w1.x, z1.x, acc);
+          acc2 = fmaf(w1.y, z1.y, acc2);
+          acc = fmaf(w1.z, z1.z, acc);
+          acc2 = fmaf(w1.w, z1.w, acc2);
+        } else {
+#pragma unroll
+          for (int m = 0; m < NR; ++m) acc = fmaf(__ldg(w + m), z[m], acc);
+        }
+      }
+    }
+    // l = 1 triplets and quads: rows 1..3 only
+    if (row < 3) {
+      for (int j = n_pair + slice; j < n_pair + n_trip; j += S) {
+        const uint2 fr = rb[j];
+        const float* z1 = zb + (fr.y & 0xffu) * NR;
+        const float* z2 = zb + ((fr.y >> 8) & 0xffu) * NR;
+        const float4* w4 = reinterpret_cast<const float4*>(L.ftensor + (fr.x & kOffMask) + row * 12);
+        const float4 a0 = __ldg(w4), a1 = __ldg(w4 + 1), a2 = __ldg(w4 + 2);
+        const float w[9] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a2.x};
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {
+          const float t = fmaf(w[p * 3 + 0], z2[0], fmaf(w[p * 3 + 1], z2[1], w[p * 3 + 2] * z2[2]));
+          acc = fmaf(z1[p], t, acc);
+        }
+      }
+      for (int j = n_pair + n_trip + slice; j < n_pair + n_trip + n_quad; j += S) {
+        const uint2 fr = rb[j];
+        const float* z1 = zb + (fr.y & 0xffu) * NR;
+        const float* z2 = zb + ((fr.y >> 8) & 0xffu) * NR;
+        const float* z3 = zb + ((fr.y >> 16) & 0xffu) * NR;
+        const float4* w4 = reinterpret_cast<const float4*>(L.ftensor + (fr.x & kOffMask) + row * 28);
+        float w[28];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+          const float4 v = __ldg(w4 + k);
+          w[4 * k] = v.x, w[4 * k + 1] = v.y, w[4 * k + 2] = v.z, w[4 * k + 3] = v.w;
+        }
+        const float z3a = z3[0], z3b = z3[1], z3c = z3[2];
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {
+          float t2 = 0.0f;
+#pragma unroll
+          for (int qq = 0; qq < 3; ++qq) {
+            const int o = (p * 3 + qq) * 3;
+            const float t3 = fmaf(w[o], z3a, fmaf(w[o + 1], z3b, w[o + 2] * z3c));
+            t2 = fmaf(z2[qq], t3, t2);
+          }
+          acc = fmaf(z1[p], t2, acc);
+        }
+      }
+    }
+    if (n_one && slice == 0 && row < NR) {
+      const uint2 fr = rb[n_pair + n_trip + n_quad];
+      acc += __ldg(L.ftensor + (fr.x & kOffMask) + row);
+    }
+    acc += acc2;
+#pragma unroll
+    for (int o = G; o < 32; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    __syncwarp();  // rb / zb are rewritten for the next item
+    const int rung = a.rung_of_slot[slot];
+    const double beta = a.beta[rung];
+    const float4 e = load_spin<PERSIST>(sp + (int64_t)s * R + r);
+    float px, py, pz;
+    double u;
+    bool attempted = true;
+    if (!do_or) {
+      if (a.prop != nullptr) {
+        const int idx = a.item_base[col] + item;
+        const float4 p4 = a.prop[idx];
+        px = p4.x, py = p4.y, pz = p4.z;
+        u = a.propu[idx];
+      } else {
+        u = keyed_proposal(a.seed[rung], (uint32_t)(s + 1), a.sweep, e.x, e.y, e.z, a.step[rung], px, py, pz);
+      }
+    } else {
+      // reflection about h = (c4, c2, c3): rows 3, 1, 2 live in lanes 2, 0, 1
+      const double h0 = __shfl_sync(0xffffffffu, acc, 2);
+      const double h1 = __shfl_sync(0xffffffffu, acc, 0);
+      const double h2 = __shfl_sync(0xffffffffu, acc, 1);
+      const double hn = sqrt((h0 * h0 + h1 * h1) + h2 * h2);
+      if (hn < 1e-12) {
+        attempted = false;
+        px = e.x, py = e.y, pz = e.z;
+      } else {
+        const double a0 = h0 / hn, a1 = h1 / hn, a2 = h2 / hn;
+        const double d2 = 2.0 * (((double)e.x * a0 + (double)e.y * a1) + (double)e.z * a2);
+        const double r0 = d2 * a0 - e.x, r1 = d2 * a1 - e.y, r2 = d2 * a2 - e.z;
+        const double rn = sqrt((r0 * r0 + r1 * r1) + r2 * r2);
+        px = (float)(r0 / rn);
+        py = (float)(r1 / rn);
+        pz = (float)(r2 / rn);
+      }
+      const Blk bk = philox_block(a.seed[rung], (uint32_t)(s + 1), a.sweep, (uint32_t)a.pass, kTagOR);
+      u = philox_uniform(bk.w0, bk.w1);
+    }
+    float zo[NR], zn[NR];
+    zrow_nr<NR>(e.x, e.y, e.z, zo);
+    zrow_nr<NR>(px, py, pz, zn);
+    float term = 0.0f;
+    if (row < NR && acc != 0.0f) term = acc * (pick<NR>(zn, row) - pick<NR>(zo, row));
+#pragma unroll
+    for (int o = G / 2; o >= 1; o >>= 1) term += __shfl_xor_sync(0xffffffffu, term, o);
+    const float dE = attempted ? term : 0.0f;
+    const bool acc_ok = attempted && (dE <= 0.0f || u < exp(-beta * (double)dE));
+    if (lane != 0) continue;
+    if (acc_ok) {
+      a.spins[L.spin_off + (int64_t)s * R + r] = make_float4(px, py, pz, 0.0f);
+      atomicAdd(s_dE + slot, (unsigned long long)llrint((double)dE * kFixScale));
+    }
+    if (do_or) {
+      if (attempted) atomicAdd(s_cnt + 3 * slot + 2, 1u);
+      if (acc_ok) atomicAdd(s_cnt + 3 * slot + 1, 1u);
+    } else if (acc_ok) {
+      atomicAdd(s_cnt + 3 * slot + 0, 1u);
+    }
+    if (a.rec_prop != nullptr && li == 0 && r == 0 && a.pass + 1 < kRecPasses) {
+      const int64_t qq = (int64_t)(a.pass + 1) * L.n_sites + s;
+      a.rec_prop[3 * qq + 0] = px;
+      a.rec_prop[3 * qq + 1] = py;
+      a.rec_prop[3 * qq + 2] = pz;
+      a.rec_u[qq] = u;
+      a.rec_dE[qq] = dE;
+      a.rec_acc[qq] = (uint8_t)(acc_ok ? 1 : (attempted ? 0 : 2));
+    }
+  }
+}
+
+template <int LMAX>
+__global__ void __launch_bounds__(256) k_fast_colour(SweepArgs a) {
+  extern __shared__ __align__(16) float zsm[];
+  __shared__ unsigned long long s_dE[kMaxSlots];
+  __shared__ unsigned int s_cnt[3 * kMaxSlots];
+  zero_block(a.n_slots, s_dE, s_cnt);
+  fast_colour<LMAX, false>(a, a.colour, s_dE, s_cnt, zsm);
+  flush_block(a, s_dE, s_cnt);
+}
+
+template <int LMAX>
+__global__ void __launch_bounds__(256) k_fast_persistent(SweepArgs a) {
+  extern __shared__ __align__(16) float zsm[];
+  __shared__ unsigned long long s_dE[kMaxSlots];
+  __shared__ unsigned int s_cnt[3 * kMaxSlots];
+  zero_block(a.n_slots, s_dE, s_cnt);
+  bool ok = true;
+  if (a.pass < 0 && a.prop != nullptr) {
+    make_proposals<true>(a);
+    ok = grid_barrier(a.gs, gridDim.x, a.barrier_limit_ns);
+  }
+  for (int col = 0; ok && col < a.max_colors; ++col) {
+    fast_colour<LMAX, true>(a, col, s_dE, s_cnt, zsm);
+    if (col + 1 < a.max_colors) ok = grid_barrier(a.gs, gridDim.x, a.barrier_limit_ns);
+  }
+  flush_block(a, s_dE, s_cnt);
+}
+
+__global__ void __launch_bounds__(256) k_proposals(SweepArgs a) { make_proposals<false>(a); }
+
 struct TailArgs {
   int32_t n_slots, n_rungs, n_lat;
   const DevLattice* lat;
@@ -753,6 +1055,8 @@ struct scemc_tables {
   int64_t n_inst = 0;
   double d_mean = 0, a_mean = 0;
   int64_t bytes = 0;
+  bool has_generic = true;
+  int64_t fast_records = 0;
   ~scemc_tables() {
     for (void* p : allocs) cudaFree(p);
   }
@@ -807,6 +1111,14 @@ struct scemc_ensemble {
   int coop_blocks = 0;  // cached co-resident grid size for the persistent form
   int coop_G = -1;
   float4* h_stage = nullptr;  // pinned host staging of the spins (n_spins float4)
+  // row-parallel fast kernel
+  bool fast = false;
+  int32_t dmax = 0, rmax = 0;
+  std::vector<int32_t> item_base;  // max_colors+1
+  int32_t* d_item_base = nullptr;
+  float4* d_prop = nullptr;
+  double* d_propu = nullptr;
+  int coop_key[4] = {-1, -1, -1, -1};
   // live timing of the sweep kernels: one event pair per pass
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -820,6 +1132,9 @@ struct scemc_ensemble {
       ev_pool.push_back(pr.second);
     }
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
+    void* qs[] = {d_item_base, d_prop, d_propu};
+    for (void* p : qs)
+      if (p) cudaFree(p);
     void* ps[] = {d_lat,   d_spins, d_seg,  d_energy,       d_dEfix,        d_cnt,       d_win,    d_swaps,
                   d_beta,  d_step,  d_seed, d_slot_of_rung, d_rung_of_slot, d_max_drift, d_drift,  d_eout,
                   d_gs,    d_st,    d_partial, d_meas,      d_rprop,        d_ru,        d_rdE,    d_racc};
@@ -839,6 +1154,159 @@ int32_t check_ptr(const int32_t* p, int64_t n, int64_t first, int64_t last, cons
     if (p[i + 1] < p[i]) return fail(SCEMC_ERR_ARG, std::string(name) + " is not monotone");
   if (p[n] != last) return fail(SCEMC_ERR_ARG, std::string(name) + " does not end at its array length + 1");
   return SCEMC_OK;
+}
+
+// Row-parallel fast tables: per site the distinct neighbours (first-appearance
+// order) and records referencing them by local index. All pair programs of a site
+// that share a neighbour merge into one NR x NR block (rows/columns 1..NR of the
+// tesseral row); body-1 programs merge into one NR vector; l = 1 triplets and quads
+// keep one record each. Blocks are deduplicated by the list of merged program ids.
+struct FastBuild {
+  std::vector<int32_t> nb_ptr, nb_list, fr_ptr;
+  std::vector<uint32_t> fr_cnt;
+  std::vector<uint2> frec;
+  std::vector<float> ft;
+  int32_t dmax = 0, rmax = 0;
+};
+
+bool build_fast(const scemc_tables_desc* d, const std::vector<int32_t>& prog_kind,
+                const std::vector<int32_t>& prog_toff, const std::vector<float>& tensor,
+                const std::vector<int32_t>& pbase, FastBuild& F) {
+  if (d->lmax != 1 && d->lmax != 2) return false;
+  const int NR = d->nlm - 1;
+  for (int32_t k : prog_kind)
+    if (k == K_GEN) return false;
+  auto place = [&](const std::vector<float>& v) {
+    while (F.ft.size() % 4) F.ft.push_back(0.0f);
+    const int32_t off = (int32_t)F.ft.size();
+    F.ft.insert(F.ft.end(), v.begin(), v.end());
+    return off;
+  };
+  std::map<std::vector<int32_t>, int32_t> pair_cache, one_cache;
+  std::vector<int32_t> single_off(prog_kind.size(), -1);
+  // program id -> (template, slot) for the l placement of pair blocks
+  const int ns = d->n_sites;
+  F.nb_ptr.assign(ns + 1, 0);
+  F.fr_ptr.assign(ns + 1, 0);
+  F.fr_cnt.assign(ns, 0u);
+  std::vector<int32_t> nbs;
+  std::vector<std::pair<int32_t, std::vector<int32_t>>> pairs;  // (local, pids)
+  std::vector<int32_t> ones;
+  std::vector<std::array<int32_t, 5>> multi;  // (kind, pid, l0, l1, l2)
+  for (int32_t s = 0; s < ns; ++s) {
+    nbs.clear();
+    pairs.clear();
+    ones.clear();
+    multi.clear();
+    auto local = [&](int32_t site) {
+      for (size_t i = 0; i < nbs.size(); ++i)
+        if (nbs[i] == site) return (int32_t)i;
+      nbs.push_back(site);
+      return (int32_t)nbs.size() - 1;
+    };
+    for (int64_t j = d->site_ptr[s] - 1; j < d->site_ptr[s + 1] - 1; ++j) {
+      const int32_t inst = d->site_inst[j] - 1;
+      const int32_t pid = d->site_prog[j] - 1;
+      const int own = d->site_slot[j];
+      const int32_t k = d->inst_term[inst] - 1;
+      const int D = d->term_body[k];
+      int32_t loc[3] = {0, 0, 0}, q = 0;
+      for (int sl = 1; sl <= D; ++sl)
+        if (sl != own) loc[q++] = local(d->inst_sites[d->inst_ptr[inst] - 1 + sl - 1] - 1);
+      const int kind = prog_kind[pid];
+      if (kind == K_B1_L1 || kind == K_B1_L2) {
+        ones.push_back(pid);
+      } else if (kind >= K_B2_11 && kind <= K_B2_22) {
+        bool found = false;
+        for (auto& pr : pairs)
+          if (pr.first == loc[0]) {
+            pr.second.push_back(pid);
+            found = true;
+            break;
+          }
+        if (!found) pairs.push_back({loc[0], {pid}});
+      } else {
+        multi.push_back({kind, pid, loc[0], loc[1], loc[2]});
+      }
+    }
+    if (nbs.size() > 255) return false;
+    F.dmax = std::max<int32_t>(F.dmax, (int32_t)nbs.size());
+    F.nb_ptr[s] = (int32_t)F.nb_list.size();
+    F.nb_list.insert(F.nb_list.end(), nbs.begin(), nbs.end());
+    F.fr_ptr[s] = (int32_t)F.frec.size();
+    for (auto& pr : pairs) {
+      std::vector<int32_t> key = pr.second;
+      std::sort(key.begin(), key.end());
+      auto it = pair_cache.find(key);
+      int32_t off;
+      if (it != pair_cache.end()) {
+        off = it->second;
+      } else {
+        std::vector<float> W((size_t)NR * NR, 0.0f);
+        for (int32_t pid : key) {
+          const int kind = prog_kind[pid];
+          const int lt = (kind == K_B2_11 || kind == K_B2_12) ? 1 : 2;
+          const int lf = (kind == K_B2_11 || kind == K_B2_21) ? 1 : 2;
+          const int rt = lt == 1 ? 0 : 3, rf = lf == 1 ? 0 : 3;
+          for (int mt = 0; mt < 2 * lt + 1; ++mt)
+            for (int mf = 0; mf < 2 * lf + 1; ++mf)
+              W[(size_t)(rt + mt) * NR + rf + mf] += tensor[prog_toff[pid] + mt * (2 * lf + 1) + mf];
+        }
+        off = place(W);
+        pair_cache[key] = off;
+      }
+      if (off > kOffMask) return false;
+      F.frec.push_back(make_uint2(((uint32_t)F_PAIR << kKindShift) | (uint32_t)off, (uint32_t)pr.first));
+    }
+    std::stable_sort(multi.begin(), multi.end(),
+                     [](const std::array<int32_t, 5>& x, const std::array<int32_t, 5>& y) { return x[0] < y[0]; });
+    int n_trip = 0, n_quad = 0;
+    for (auto& m : multi) {
+      const int32_t pid = m[1];
+      if (single_off[pid] < 0) {
+        // three target rows, each padded to a multiple of 4 floats (16-byte loads)
+        const int row = m[0] == K_B3_111 ? 9 : 27, stride = m[0] == K_B3_111 ? 12 : 28;
+        std::vector<float> v((size_t)3 * stride, 0.0f);
+        for (int t = 0; t < 3; ++t)
+          for (int k = 0; k < row; ++k) v[(size_t)t * stride + k] = tensor[prog_toff[pid] + t * row + k];
+        single_off[pid] = place(v);
+      }
+      if (m[0] == K_B3_111) ++n_trip;
+      else ++n_quad;
+      const uint32_t kind = m[0] == K_B3_111 ? F_TRIP : F_QUAD;
+      if (single_off[pid] > kOffMask) return false;
+      F.frec.push_back(make_uint2((kind << kKindShift) | (uint32_t)single_off[pid],
+                                  (uint32_t)m[2] | ((uint32_t)m[3] << 8) | ((uint32_t)m[4] << 16)));
+    }
+    if (!ones.empty()) {
+      std::vector<int32_t> key = ones;  // merged body-1 vector
+      std::sort(key.begin(), key.end());
+      auto it = one_cache.find(key);
+      int32_t off;
+      if (it != one_cache.end()) {
+        off = it->second;
+      } else {
+        std::vector<float> w(NR, 0.0f);
+        for (int32_t pid : key) {
+          const int lt = prog_kind[pid] == K_B1_L1 ? 1 : 2;
+          const int rt = lt == 1 ? 0 : 3;
+          for (int mt = 0; mt < 2 * lt + 1; ++mt) w[rt + mt] += tensor[prog_toff[pid] + mt];
+        }
+        off = place(w);
+        one_cache[key] = off;
+      }
+      if (off > kOffMask) return false;
+      F.frec.push_back(make_uint2(((uint32_t)F_ONE << kKindShift) | (uint32_t)off, 0u));
+    }
+    if (pairs.size() > 255 || n_trip > 255 || n_quad > 255) return false;
+    F.fr_cnt[s] = (uint32_t)pairs.size() | ((uint32_t)n_trip << 8) | ((uint32_t)n_quad << 16) |
+                  ((uint32_t)(ones.empty() ? 0 : 1) << 24);
+  }
+  F.nb_ptr[ns] = (int32_t)F.nb_list.size();
+  F.fr_ptr[ns] = (int32_t)F.frec.size();
+  for (int32_t s = 0; s < ns; ++s) F.rmax = std::max(F.rmax, F.fr_ptr[s + 1] - F.fr_ptr[s]);
+  (void)pbase;
+  return true;
 }
 
 int32_t compile_tables(const scemc_tables_desc* d, scemc_tables* T) {
@@ -1017,7 +1485,14 @@ int32_t compile_tables(const scemc_tables_desc* d, scemc_tables* T) {
     sfac_slot[f] = d->sfac_slot[f];
   }
   for (int64_t f = 0; f < d->n_efac; ++f) efac_row[f] = (int8_t)(d->efac_row[f] - 1);
-  std::vector<int4> rec_v = rec;
+  FastBuild F;
+  const bool fast = build_fast(d, prog_kind, prog_toff, tensor, pbase, F);
+  // the generic records are kept for every model that needs them, and for small
+  // fast ones (so the generic form can still be selected); huge fast models skip them
+  const bool keep_generic = !fast || d->n_adj <= (int64_t)(1 << 24);
+  std::vector<int4> rec_v;
+  if (keep_generic) rec_v = std::move(rec);
+  std::vector<int4>().swap(rec);
   std::vector<uint8_t> has_l1(d->site_has_l1, d->site_has_l1 + ns), active(d->site_active, d->site_active + ns);
   std::vector<double> eent_w(d->eent_w, d->eent_w + d->n_eent), term_coef(d->term_coef, d->term_coef + d->n_terms);
   DevLattice& L = T->dl;
@@ -1051,6 +1526,19 @@ int32_t compile_tables(const scemc_tables_desc* d, scemc_tables* T) {
   if ((r = upload(T->allocs, rebase(d->efac_ptr, d->n_eent + 1), &L.efac_ptr))) return r;
   if ((r = upload(T->allocs, efac_row, &L.efac_row))) return r;
   if ((r = upload(T->allocs, term_coef, &L.term_coef))) return r;
+  L.fast = fast ? 1 : 0;
+  L.dmax = F.dmax;
+  L.rmax = F.rmax;
+  if (fast) {
+    if ((r = upload(T->allocs, F.nb_ptr, &L.nb_ptr))) return r;
+    if ((r = upload(T->allocs, F.nb_list, &L.nb_list))) return r;
+    if ((r = upload(T->allocs, F.fr_ptr, &L.fr_ptr))) return r;
+    if ((r = upload(T->allocs, F.fr_cnt, &L.fr_cnt))) return r;
+    if ((r = upload(T->allocs, F.frec, &L.frec))) return r;
+    if ((r = upload(T->allocs, F.ft, &L.ftensor))) return r;
+  }
+  T->has_generic = keep_generic;
+  T->fast_records = (int64_t)F.frec.size();
   T->color_ptr = cp;
   T->active = active;
   T->n_sites = ns;
@@ -1063,7 +1551,8 @@ int32_t compile_tables(const scemc_tables_desc* d, scemc_tables* T) {
   T->d_mean = d->n_active ? (double)d_sum / d->n_active : 0.0;
   T->a_mean = d->n_active ? (double)a_sum / d->n_active : 0.0;
   T->bytes = (int64_t)(rec_v.size() * 16 + adj_ptr.size() * 4 + tensor.size() * 4 + sent_w.size() * 6 +
-                       d->n_inst_sites * 4 + d->n_inst * 8);
+                       d->n_inst_sites * 4 + d->n_inst * 8 + F.frec.size() * 8 + F.nb_list.size() * 4 +
+                       F.ft.size() * 4 + (F.nb_ptr.size() + F.fr_ptr.size()) * 4);
   return SCEMC_OK;
 }
 
@@ -1178,6 +1667,20 @@ int32_t create_ensemble(int32_t n_tables, const scemc_tables* const* tables, con
   }
   if ((rc = dalloc(&E->d_seg, E->seg.size()))) return rc;
   CUDA_TRY(cudaMemcpy(E->d_seg, E->seg.data(), E->seg.size() * 4, cudaMemcpyHostToDevice));
+  E->item_base.assign(E->max_colors + 1, 0);
+  for (int c = 0; c < E->max_colors; ++c) {
+    const int64_t nb = (int64_t)E->item_base[c] + E->seg[(size_t)c * (n_tables + 1) + n_tables];
+    if (nb > 0x7fffffffll) return fail(SCEMC_ERR_UNSUPPORTED, "more than 2^31 items in one pass");
+    E->item_base[c + 1] = (int32_t)nb;
+  }
+  if ((rc = dalloc(&E->d_item_base, E->item_base.size()))) return rc;
+  CUDA_TRY(cudaMemcpy(E->d_item_base, E->item_base.data(), E->item_base.size() * 4, cudaMemcpyHostToDevice));
+  E->fast = true;
+  for (int i = 0; i < n_tables; ++i) {
+    E->fast = E->fast && tables[i]->dl.fast && tables[i]->lmax == E->lmax;
+    E->dmax = std::max(E->dmax, tables[i]->dl.dmax);
+    E->rmax = std::max(E->rmax, tables[i]->dl.rmax);
+  }
   if ((rc = dalloc(&E->d_energy, slots)) || (rc = dalloc(&E->d_dEfix, slots)) || (rc = dalloc(&E->d_cnt, 4 * slots)) ||
       (rc = dalloc(&E->d_win, 2 * slots)) || (rc = dalloc(&E->d_swaps, 2 * slots)) ||
       (rc = dalloc(&E->d_beta, slots)) || (rc = dalloc(&E->d_step, slots)) || (rc = dalloc(&E->d_seed, slots)) ||
@@ -1307,36 +1810,129 @@ void harvest_events(scemc_ensemble* E) {
   E->ev_pending.clear();
 }
 
-int32_t run_pass_impl(scemc_ensemble* E, int pass, int G, int mode);
+// Resolved launch configuration of a sweep pass.
+struct Launch {
+  int G = 1;          // lanes per item (generic kernel); the fast kernel fixes its own
+  int mode = 2;       // 1 = one launch per colour, 2 = persistent cooperative kernel
+  bool fast = false;  // row-parallel fast kernel
+  bool precompute = false;  // Metropolis proposals computed before the colour loop
+};
+
+using FastFn = void (*)(SweepArgs);
+
+FastFn fast_kernel(int lmax, bool persist) {
+  if (lmax == 1) return persist ? k_fast_persistent<1> : k_fast_colour<1>;
+  return persist ? k_fast_persistent<2> : k_fast_colour<2>;
+}
+
+int fast_rows(int lmax) { return lmax == 1 ? 3 : 8; }
+int fast_group(int lmax) { return lmax == 1 ? 4 : 8; }
+
+// Threads per block and dynamic shared memory (neighbour Z rows) of the fast kernel.
+void fast_shape(const scemc_ensemble* E, int* threads, size_t* smem) {
+  const int NR = fast_rows(E->lmax);
+  const size_t per_warp = fast_group_floats(std::max(E->dmax, 1), std::max(E->rmax, 1), NR) * sizeof(float);
+  int t = 256;
+  size_t m = (size_t)(t / 32) * per_warp;
+  while (m > 160 * 1024 && t > 32) {
+    t /= 2;
+    m = (size_t)(t / 32) * per_warp;
+  }
+  *threads = t;
+  *smem = m;
+}
+
+int32_t ensure_props(scemc_ensemble* E) {
+  if (E->d_prop) return SCEMC_OK;
+  const int64_t n = std::max<int32_t>(E->item_base.back(), 1);
+  int32_t rc;
+  if ((rc = dalloc(&E->d_prop, n)) || (rc = dalloc(&E->d_propu, n))) return rc;
+  return SCEMC_OK;
+}
+
+int32_t run_pass_impl(scemc_ensemble* E, int pass, const Launch& Lc);
 
 // One pass (Metropolis or OR pass k) over every colour, optionally timed.
-int32_t run_pass(scemc_ensemble* E, int pass, int G, int mode) {
-  if (!E->profiling) return run_pass_impl(E, pass, G, mode);
+int32_t run_pass(scemc_ensemble* E, int pass, const Launch& Lc) {
+  if (!E->profiling) return run_pass_impl(E, pass, Lc);
   cudaEvent_t a = take_event(E), b = take_event(E);
   CUDA_TRY(cudaEventRecord(a, E->stream));
-  const int32_t rc = run_pass_impl(E, pass, G, mode);
+  const int32_t rc = run_pass_impl(E, pass, Lc);
   CUDA_TRY(cudaEventRecord(b, E->stream));
   E->ev_pending.emplace_back(a, b);
   return rc;
 }
 
-int32_t run_pass_impl(scemc_ensemble* E, int pass, int G, int mode) {
+int max_colour_items(const scemc_ensemble* E) {
+  int m = 1;
+  for (int c = 0; c < E->max_colors; ++c) m = std::max(m, E->seg[(size_t)c * (E->tabs.size() + 1) + E->tabs.size()]);
+  return m;
+}
+
+int32_t run_pass_impl(scemc_ensemble* E, int pass, const Launch& Lc) {
   const int lmax = E->lmax;
-  const int threads = 256;
   SweepArgs a = make_args(E, pass);
-  if (mode == 2) {
+  const int max_items = max_colour_items(E);
+  if (Lc.fast) {
+    int threads;
+    size_t smem;
+    fast_shape(E, &threads, &smem);
+    const int G = 32;  // one warp per item
+    a.dmax = std::max(E->dmax, 1);
+    a.rmax = std::max(E->rmax, 1);
+    a.item_base = E->d_item_base;
+    if (Lc.precompute && pass < 0) {
+      int32_t rc;
+      if ((rc = ensure_props(E))) return rc;
+      a.prop = E->d_prop;
+      a.propu = E->d_propu;
+    }
+    FastFn fn = fast_kernel(lmax, Lc.mode == 2);
+    CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (Lc.mode == 2) {
+      const int key[4] = {2, lmax, threads, (int)smem};
+      if (!std::equal(key, key + 4, E->coop_key)) {
+        int per_sm = 0;
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, threads, smem));
+        if (per_sm < 1) return fail(SCEMC_ERR_CUDA, "persistent fast sweep kernel cannot be resident");
+        E->coop_blocks = per_sm * sm_count(E->device);
+        std::copy(key, key + 4, E->coop_key);
+      }
+      int64_t need = ((int64_t)max_items * G + threads - 1) / threads;
+      if (a.prop) need = std::max<int64_t>(need, ((int64_t)E->item_base.back() + threads - 1) / threads);
+      const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(E->coop_blocks, need));
+      void* params[] = {&a};
+      CUDA_TRY(cudaLaunchCooperativeKernel((const void*)fn, dim3(blocks), dim3(threads), params, smem, E->stream));
+      return SCEMC_OK;
+    }
+    const int cap = sm_count(E->device) * 16;
+    if (a.prop) {
+      const int blocks = (int)std::min<int64_t>(cap, ((int64_t)E->item_base.back() + 255) / 256);
+      k_proposals<<<std::max(blocks, 1), 256, 0, E->stream>>>(a);
+      CUDA_TRY(cudaGetLastError());
+    }
+    for (int c = 0; c < E->max_colors; ++c) {
+      const int n = E->seg[(size_t)c * (E->tabs.size() + 1) + E->tabs.size()];
+      if (n == 0) continue;
+      a.colour = c;
+      const int blocks = (int)std::min<int64_t>(cap, ((int64_t)n * G + threads - 1) / threads);
+      fn<<<std::max(blocks, 1), threads, smem, E->stream>>>(a);
+      CUDA_TRY(cudaGetLastError());
+    }
+    return SCEMC_OK;
+  }
+  const int threads = 256;
+  const int G = Lc.G;
+  if (Lc.mode == 2) {
     KFn fn = kernel_for(lmax, G, true);
-    if (E->coop_G != G) {
+    const int key[4] = {1, lmax, G, 0};
+    if (!std::equal(key, key + 4, E->coop_key)) {
       int per_sm = 0;
       CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, threads, 0));
       if (per_sm < 1) return fail(SCEMC_ERR_CUDA, "persistent sweep kernel cannot be resident");
       E->coop_blocks = per_sm * sm_count(E->device);
-      E->coop_G = G;
+      std::copy(key, key + 4, E->coop_key);
     }
-    // no more blocks than there are item groups in the widest colour
-    int max_items = 1;
-    for (int c = 0; c < E->max_colors; ++c)
-      max_items = std::max(max_items, E->seg[(size_t)c * (E->tabs.size() + 1) + E->tabs.size()]);
     const int want = (int)std::min<int64_t>(E->coop_blocks, ((int64_t)max_items * G + threads - 1) / threads);
     const int blocks = std::max(1, want);
     void* params[] = {&a};
@@ -1476,13 +2072,36 @@ int auto_lanes(const scemc_ensemble* E) {
   return G;
 }
 
-int32_t sweep_once(scemc_ensemble* E, int n_or, int G, int mode) {
+// kernel: 0 auto, 1 generic, 2 fast; proposals: 0 auto, 1 precompute, 2 inline.
+int32_t resolve_launch(const scemc_ensemble* E, int lanes, int mode, int kernel, int proposals, Launch* out) {
+  Launch L;
+  L.mode = mode == 0 ? 2 : mode;
+  if (L.mode != 1 && L.mode != 2) return fail(SCEMC_ERR_ARG, "mode must be 0, 1 or 2");
+  if (kernel < 0 || kernel > 2 || proposals < 0 || proposals > 2)
+    return fail(SCEMC_ERR_ARG, "kernel and proposals must be 0, 1 or 2");
+  bool generic_ok = true;
+  for (const scemc_tables* T : E->tabs) generic_ok = generic_ok && T->has_generic;
+  if (kernel == 2 && !E->fast)
+    return fail(SCEMC_ERR_ARG, "the fast kernel needs lmax 1 or 2 and dense l in {1,2} programs of body <= 4 "
+                               "(l = 1 only for bodies 3 and 4), equal lmax across the batch");
+  if (kernel == 1 && !generic_ok) return fail(SCEMC_ERR_ARG, "generic records were not kept for these tables");
+  L.fast = kernel == 2 || (kernel == 0 && E->fast);
+  L.G = lanes ? norm_lanes(lanes) : auto_lanes(E);
+  if (L.fast) {
+    const int64_t groups = (int64_t)max_colour_items(E) * 32;
+    L.precompute = proposals == 1 || (proposals == 0 && groups < (int64_t)sm_count(E->device) * 2048);
+  }
+  *out = L;
+  return SCEMC_OK;
+}
+
+int32_t sweep_once(scemc_ensemble* E, int n_or, const Launch& L) {
   if (E->sweep_index >= 0x7ffffffell - 1)
     return fail(SCEMC_ERR_EXHAUSTED, "sweep_index exhausted the 32-bit RNG counter word");
   int32_t rc;
-  if ((rc = run_pass(E, -1, G, mode))) return rc;
+  if ((rc = run_pass(E, -1, L))) return rc;
   for (int k = 0; k < n_or; ++k)
-    if ((rc = run_pass(E, k, G, mode))) return rc;
+    if ((rc = run_pass(E, k, L))) return rc;
   return SCEMC_OK;
 }
 
@@ -1579,7 +2198,9 @@ int32_t scemc_metropolis_sweep(scemc_chain* c, const scemc_tables* t, double bet
   unsigned long long before = 0;
   CUDA_TRY(cudaMemcpyAsync(&before, c->d_cnt, 8, cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(cudaStreamSynchronize(c->stream));
-  if ((rc = sweep_once(c, 0, norm_lanes(lanes_per_site), 1))) return rc;
+  Launch L;
+  if ((rc = resolve_launch(c, lanes_per_site, 1, 0, 0, &L))) return rc;
+  if ((rc = sweep_once(c, 0, L))) return rc;
   if ((rc = launch_tail(c, true, false, 0.5, false))) return rc;
   unsigned long long after = 0;
   CUDA_TRY(cudaMemcpyAsync(&after, c->d_cnt, 8, cudaMemcpyDeviceToHost, c->stream));
@@ -1601,7 +2222,9 @@ int32_t scemc_overrelaxation_sweep(scemc_chain* c, const scemc_tables* t, double
   CUDA_TRY(cudaMemcpyAsync(before, c->d_cnt, 32, cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   // a stand-alone OR sweep uses pass 0 of the next sweep counter word
-  if ((rc = run_pass(c, 0, norm_lanes(lanes_per_site), 1))) return rc;
+  Launch L;
+  if ((rc = resolve_launch(c, lanes_per_site, 1, 0, 0, &L))) return rc;
+  if ((rc = run_pass(c, 0, L))) return rc;
   if ((rc = launch_tail(c, false, false, 0.5, false))) return rc;
   CUDA_TRY(cudaMemcpyAsync(after, c->d_cnt, 32, cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -1617,9 +2240,10 @@ int32_t scemc_run_sweeps(scemc_chain* c, const scemc_tables* t, double beta, int
   if ((rc = check_single(c, t)) || (rc = check_lanes(lanes_per_site))) return rc;
   if (!std::isfinite(beta) || nsweeps < 0) return fail(SCEMC_ERR_ARG, "bad beta or nsweeps");
   CUDA_TRY(cudaMemcpyAsync(c->d_beta, &beta, 8, cudaMemcpyHostToDevice, c->stream));
-  const int G = norm_lanes(lanes_per_site);
+  Launch L;
+  if ((rc = resolve_launch(c, lanes_per_site, 1, 0, 0, &L))) return rc;
   for (int64_t i = 1; i <= nsweeps; ++i) {
-    if ((rc = sweep_once(c, 0, G, 1))) return rc;
+    if ((rc = sweep_once(c, 0, L))) return rc;
     if ((rc = launch_tail(c, true, false, 0.5, false))) return rc;
     c->sweep_index += 1;
     if (renorm_interval > 0 && i % renorm_interval == 0)
@@ -1722,14 +2346,14 @@ int32_t scemc_batch_run_async(scemc_batch* b, const scemc_run_params* p) {
     int32_t rc = check_lanes(p->lanes_per_site);
     if (rc) return rc;
   }
-  const int G = p->lanes_per_site ? norm_lanes(p->lanes_per_site) : auto_lanes(b);
-  const int mode = p->mode == 0 ? 2 : p->mode;
   if (p->phase_done < 0 || p->phase_total < 0) return fail(SCEMC_ERR_ARG, "bad phase bookkeeping");
   const int64_t total = p->phase_total > 0 ? p->phase_total : p->phase_done + p->nsweeps;
   int32_t rc;
+  Launch L;
+  if ((rc = resolve_launch(b, p->lanes_per_site, p->mode, p->kernel, p->proposals, &L))) return rc;
   for (int64_t k = 1; k <= p->nsweeps; ++k) {
     const int64_t i = p->phase_done + k;
-    if ((rc = sweep_once(b, p->or_per_metropolis, G, mode))) return rc;
+    if ((rc = sweep_once(b, p->or_per_metropolis, L))) return rc;
     b->sweep_index += 1;
     const bool adapt = p->adapt_interval > 0 && i % p->adapt_interval == 0;
     if ((rc = launch_tail(b, true, adapt, p->adapt_target, false))) return rc;

@@ -115,14 +115,24 @@ def check_pass(OH, cfg, rec, beta, kind, seed=None, sweep=None, step=None, orpas
     return int(tie[mism].sum()), int(att.sum()), n_sites
 
 
-REPLAY_CASES = [(m, 4, 2) for m in MODELS] + [
-    ("biquadratic", 1, 1), ("biquadratic", 32, 1), ("bcc_l2_plaq_zeeman", 1, 2), ("bcc_l2_plaq_zeeman", 32, 1),
-    ("high_l", 1, 1), ("fourbody", 32, 2), ("sc_J1J2", 8, 1), ("fcc_l2_tri_zeeman", 16, 2),
+NOT_FAST = {"mixed", "high_l"}  # programs outside the fast kinds (l = 0 / l >= 3 members)
+FAST = [m for m in MODELS if m not in NOT_FAST]
+
+# (model, lanes, mode, kernel, proposals): kernel 1 = generic record walk, 0 = auto
+# (the row-parallel fast kernel wherever the model allows it); proposals 1 =
+# precomputed before the colour loop, 2 = inline.
+REPLAY_CASES = [(m, 4, 2, 1, 0) for m in MODELS] + [(m, 0, 2, 0, 1) for m in FAST] + [
+    ("biquadratic", 1, 1, 1, 0), ("biquadratic", 32, 1, 1, 0), ("bcc_l2_plaq_zeeman", 1, 2, 1, 0),
+    ("bcc_l2_plaq_zeeman", 32, 1, 1, 0), ("high_l", 1, 1, 0, 0), ("mixed", 32, 2, 0, 0),
+    ("fourbody", 32, 2, 1, 0), ("sc_J1J2", 8, 1, 1, 0), ("fcc_l2_tri_zeeman", 16, 2, 1, 0),
+    ("bcc_l2_plaq_zeeman", 0, 1, 0, 2), ("bcc_l2_plaq_zeeman", 0, 1, 0, 1), ("bcc_l2_plaq_zeeman", 0, 2, 0, 2),
+    ("fcc_l2_tri_zeeman", 0, 1, 0, 2), ("threebody", 0, 1, 0, 1), ("chain", 0, 2, 0, 2),
 ]
 
 
-@pytest.mark.parametrize("name,lanes,mode", REPLAY_CASES, ids=[f"{m}-G{g}-mode{d}" for m, g, d in REPLAY_CASES])
-def test_sweep_replay(gpu, name, lanes, mode):
+@pytest.mark.parametrize("name,lanes,mode,kernel,proposals", REPLAY_CASES,
+                         ids=[f"{m}-G{g}-mode{d}-k{k}-p{q}" for m, g, d, k, q in REPLAY_CASES])
+def test_sweep_replay(gpu, name, lanes, mode, kernel, proposals):
     H, OH = build(name)
     gH = scemc.GPUTiledHamiltonian(H)
     seed, step, beta = 0xC0FFEE + lanes, 0.6, 1 / 0.05
@@ -133,7 +143,7 @@ def test_sweep_replay(gpu, name, lanes, mode):
     for sw in range(1, 5):
         cfg = b.download()["configs"][0].copy()
         b.record(True)
-        b.run(1, or_per_metropolis=n_or, lanes_per_site=lanes, mode=mode)
+        b.run(1, or_per_metropolis=n_or, lanes_per_site=lanes, mode=mode, kernel=kernel, proposals=proposals)
         t, a, _ = check_pass(OH, cfg, b.fetch_record(-1), beta, "metro", seed=seed, sweep=sw, step=step)
         ties, att = ties + t, att + a
         for k in range(n_or):
@@ -148,6 +158,34 @@ def test_sweep_replay(gpu, name, lanes, mode):
         # the running (FP32 dE, fixed-point summed) energy tracks the recompute
         assert abs(post["energies"][0] - E_or) <= 1e-5 * max(1.0, abs(E_or))
     assert ties <= max(1, att // 100)
+
+
+def test_fast_kernel_is_launch_shape_independent(gpu):
+    """The fast kernel fixes its lane count by lmax and reduces dE with a fixed
+    butterfly: per-colour vs persistent launches and precomputed vs inline proposals
+    give bitwise-identical chains, overrelaxation included."""
+    H, _ = build("bcc_l2_plaq_zeeman")
+    gH = scemc.GPUTiledHamiltonian(H)
+    cfg = rand_cfg(H.n_sites, 3)
+    outs = []
+    for mode, prop in [(1, 1), (1, 2), (2, 1), (2, 2)]:
+        b = scemc.GPUBatch([gH], [2], [cfg, cfg], [9, 10], 0.6)
+        b.set_betas([1 / 0.002, 1 / 0.01])
+        b.run(6, or_per_metropolis=1, mode=mode, proposals=prop, kernel=2)
+        st = b.download()
+        outs.append((np.stack(st["configs"]), st["energies"].copy(), st["counters"].copy()))
+    for o in outs[1:]:
+        assert np.array_equal(o[0], outs[0][0]) and np.array_equal(o[1], outs[0][1])
+        assert np.array_equal(o[2], outs[0][2])
+
+
+def test_fast_kernel_refused_where_it_does_not_apply(gpu):
+    H, _ = build("mixed")
+    gH = scemc.GPUTiledHamiltonian(H)
+    b = scemc.GPUBatch([gH], [1], [rand_cfg(H.n_sites, 1)], [1], 0.6)
+    with pytest.raises(_lib.ScemcArgumentError):
+        b.run(1, kernel=2)
+    b.run(1, kernel=0)  # auto falls back to the generic record walk
 
 
 def test_proposal_stream_is_the_reference_stream(gpu):
@@ -193,7 +231,7 @@ def test_repeat_identity_lanes_and_modes(gpu):
     def run(lanes, mode, seed, n_or):
         b = scemc.GPUBatch([gH], [1], [cfg], [seed], 0.6)
         b.set_betas([1 / 0.002])
-        b.run(6, or_per_metropolis=n_or, lanes_per_site=lanes, mode=mode)
+        b.run(6, or_per_metropolis=n_or, lanes_per_site=lanes, mode=mode, kernel=1)
         st = b.download()
         return st["configs"][0], st["energies"][0], st["counters"][0].copy()
 
