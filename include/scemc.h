@@ -175,7 +175,9 @@ typedef struct scemc_run_params {
   int64_t renorm_interval;   /* > 0: renormalise + FP64 recompute every renorm_interval sweeps */
   int64_t measure_interval;  /* > 0: record observables every measure_interval sweeps */
   int32_t lanes_per_site;    /* 0 = autotuned */
-  int32_t mode;              /* 0 = auto, 1 = one launch per colour, 2 = persistent grid kernel */
+  int32_t mode;              /* 0 = auto (autotuned if scemc_batch_autotune ran, else 2), 1 = one launch per
+                                colour, 2 = persistent grid kernel per pass, 3 = per-colour launches of a
+                                compound sweep captured once in a CUDA graph and replayed */
   /* Phase bookkeeping (the reference's lane.phase_sweeps): sweep i of this call is
    * sweep phase_done + i of its phase; adaptation, renormalisation, measurement and
    * exchange fire on that count, and no exchange follows the phase's last sweep
@@ -203,6 +205,12 @@ int32_t scemc_batch_upload(scemc_batch* b, const double* configs, const double* 
  * CUDA event pair on the batch stream; scemc_batch_kernel_time returns the summed
  * device time (ms) and the number of passes since profiling was switched on. */
 int32_t scemc_batch_profile(scemc_batch* b, int32_t on);
+/* Times the launch forms (modes 2 and 3; proposal precompute on/off for the fast
+ * kernel, lanes per site for the generic one) for sweeps_per_trial compound sweeps
+ * each and keeps the fastest for runs with mode = 0. The trial sweeps are real
+ * sweeps of the batch (its chains advance). Outputs may be NULL. */
+int32_t scemc_batch_autotune(scemc_batch* b, int32_t or_per_metropolis, int32_t sweeps_per_trial, int32_t* mode,
+                             int32_t* proposals, int32_t* lanes, double* ms_per_sweep);
 int32_t scemc_batch_kernel_time(const scemc_batch* b, double* ms, int64_t* passes);
 /* State readback. configs: 3 x n_sites per SLOT (payload order); energies per slot;
  * slot_of_rung per rung; counters 4 per rung {acc_metro, att_metro, acc_or, att_or};

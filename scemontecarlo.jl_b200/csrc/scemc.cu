@@ -120,14 +120,15 @@ struct DevLattice {
   const int32_t* nb_list;        // 0-based site ids
   const int32_t* fr_ptr;         // n_sites+1: fast records of site s
   const uint32_t* fr_cnt;        // per site: n_pair | n_trip << 8 | n_quad << 16 | n_one << 24
+  const int4* idesc;             // per colour position: {site | has_l1 << 30 | n_one << 31, nb offset,
+                                 //   record offset, n_pair | n_trip << 8 | n_quad << 16 | n_nb << 24}
   const uint2* frec;             // {kind<<26 | tensor offset, local neighbour indices (8 bits each)}
   const float* ftensor;          // dense blocks, rows padded to the kernel's row count
 };
 
 // Grid barrier state (one per ensemble).
 struct GridSync {
-  unsigned int count;
-  unsigned int gen;
+  unsigned long long arrived;  // monotonically increasing arrival count (never reset)
   int error;
   int pad;
 };
@@ -137,7 +138,7 @@ struct EnsState {
   int32_t exchange_parity;
   int32_t exchange_count;
   int32_t error;
-  int32_t pad;
+  uint32_t sweep;  // completed sweeps (the keyed stream's counter word is sweep + 1)
 };
 
 struct SweepArgs {
@@ -158,6 +159,8 @@ struct SweepArgs {
   unsigned long long* cnt;         // per rung: [acc_metro, att_metro, acc_or, att_or]
   GridSync* gs;
   long long barrier_limit_ns;
+  unsigned long long bar_base;  // arrival count at launch (persistent form)
+  const EnsState* st;           // device sweep counter (read by every launch, so graphs stay valid)
   // replay recording (slot 0 of lattice 0), may be null
   float* rec_prop;
   double* rec_u;
@@ -176,27 +179,35 @@ __device__ __forceinline__ unsigned long long globaltimer() {
   return t;
 }
 
-// Sense-free generation barrier across all blocks of a cooperative launch. The
-// wait is bounded: after limit_ns it records an error and returns false; every
-// other block sees the flag and leaves too.
-__device__ __forceinline__ bool grid_barrier(GridSync* gs, unsigned int nblocks, long long limit_ns) {
+__device__ __forceinline__ void red_add_release(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Barrier across all blocks of a cooperative launch on a monotonically increasing
+// arrival counter: barrier k of a launch whose counter started at `base` completes
+// when the counter reaches base + (k + 1) * nblocks. One fire-and-forget release
+// add per block and acquire polling; the wait is bounded by limit_ns, after which
+// the error word is set, every block leaves, and every later barrier fails at once.
+__device__ __forceinline__ bool grid_barrier(GridSync* gs, unsigned long long base, int k, unsigned int nblocks,
+                                             long long limit_ns) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned int* vgen = &gs->gen;
     volatile int* verr = &gs->error;
-    int ok = *verr ? 0 : 1;  // a failed barrier poisons every later one
+    int ok = *verr ? 0 : 1;
     if (ok) {
-      const unsigned int g = *vgen;
       __threadfence();
-      const unsigned int arrived = atomicAdd(&gs->count, 1u);
-      if (arrived == nblocks - 1) {
-        atomicExch(&gs->count, 0u);
-        __threadfence();
-        atomicAdd(&gs->gen, 1u);
-      } else {
-        const unsigned long long t0 = globaltimer();
-        while (*vgen == g) {
+      red_add_release(&gs->arrived, 1ull);
+      const unsigned long long target = base + (unsigned long long)(k + 1) * nblocks;
+      const unsigned long long t0 = globaltimer();
+      for (unsigned int it = 0;; ++it) {
+        if (ld_acquire(&gs->arrived) >= target) break;
+        if ((it & 31u) == 31u) {
           if (*verr) {
             ok = 0;
             break;
@@ -206,10 +217,9 @@ __device__ __forceinline__ bool grid_barrier(GridSync* gs, unsigned int nblocks,
             ok = 0;
             break;
           }
-          __nanosleep(64);
         }
+        if (it > 64) __nanosleep(32);
       }
-      __threadfence();
     }
     s_ok = ok;
   }
@@ -424,7 +434,7 @@ __device__ void sweep_colour(const SweepArgs& a, int col, unsigned long long* s_
     double u;
     bool attempted = true;
     if (!do_or) {
-      u = keyed_proposal(a.seed[rung], (uint32_t)(s + 1), a.sweep, e.x, e.y, e.z, a.step[rung], px, py, pz);
+      u = keyed_proposal(a.seed[rung], (uint32_t)(s + 1), a.st->sweep + 1u, e.x, e.y, e.z, a.step[rung], px, py, pz);
     } else {
       // Reflection about the l = 1 field axis h = (c4, c2, c3) (updates.jl:66-87).
       const double h0 = LMAX >= 1 ? c[NLM > 3 ? 3 : 0] : 0.0, h1 = LMAX >= 1 ? c[NLM > 1 ? 1 : 0] : 0.0,
@@ -442,7 +452,7 @@ __device__ void sweep_colour(const SweepArgs& a, int col, unsigned long long* s_
         py = (float)(r1 / rn);
         pz = (float)(r2 / rn);
       }
-      const Blk b = philox_block(a.seed[rung], (uint32_t)(s + 1), a.sweep, (uint32_t)a.pass, kTagOR);
+      const Blk b = philox_block(a.seed[rung], (uint32_t)(s + 1), a.st->sweep + 1u, (uint32_t)a.pass, kTagOR);
       u = philox_uniform(b.w0, b.w1);
     }
     float dE = 0.0f;
@@ -519,14 +529,14 @@ __global__ void __launch_bounds__(256) k_sweep_persistent(SweepArgs a) {
   for (int col = 0; col < a.max_colors; ++col) {
     sweep_colour<LMAX, G, true>(a, col, s_dE, s_cnt);
     if (col + 1 < a.max_colors)
-      if (!grid_barrier(a.gs, gridDim.x, a.barrier_limit_ns)) break;
+      if (!grid_barrier(a.gs, a.bar_base, col, gridDim.x, a.barrier_limit_ns)) break;
   }
   flush_block(a, s_dE, s_cnt);
 }
 
 // Barrier self-test: nblocks_expected = gridDim.x + 1 can never be reached.
 __global__ void k_barrier_selftest(GridSync* gs, long long limit_ns) {
-  grid_barrier(gs, gridDim.x + 1, limit_ns);
+  grid_barrier(gs, 0ull, 0, gridDim.x + 1, limit_ns);
 }
 
 // ---------------------------------------------------------------------------
@@ -545,6 +555,23 @@ template <int NR>
 __device__ __forceinline__ void zrow_nr(float x, float y, float z, float* o) {
   zrow_l1(x, y, z, o);
   if (NR > 3) zrow_l2(x, y, z, o + 3);
+}
+
+// Per-slot run parameters (beta, step, key) staged at the start of the fast kernel's
+// dynamic shared memory: 3 x 8 bytes per slot, rounded to 16 bytes.
+__host__ __device__ __forceinline__ size_t fast_param_floats(int n_slots) { return ((size_t)6 * n_slots + 3) & ~(size_t)3; }
+
+__device__ __forceinline__ void stage_params(const SweepArgs& a, float* zsm) {
+  double* b = reinterpret_cast<double*>(zsm);
+  double* st = b + a.n_slots;
+  unsigned long long* sd = reinterpret_cast<unsigned long long*>(st + a.n_slots);
+  for (int i = threadIdx.x; i < a.n_slots; i += blockDim.x) {
+    const int rung = a.rung_of_slot[i];
+    b[i] = a.beta[rung];
+    st[i] = a.step[rung];
+    sd[i] = a.seed[rung];
+  }
+  __syncthreads();
 }
 
 // Shared-memory floats one warp of the fast kernel uses (host and device agree):
@@ -590,7 +617,8 @@ __device__ void make_proposals(const SweepArgs& a) {
     const int rung = a.rung_of_slot[L.slot0 + r];
     const float4 e = load_spin<PERSIST>(a.spins + L.spin_off + (int64_t)s * L.R + r);
     float px, py, pz;
-    const double u = keyed_proposal(a.seed[rung], (uint32_t)(s + 1), a.sweep, e.x, e.y, e.z, a.step[rung], px, py, pz);
+    const double u =
+        keyed_proposal(a.seed[rung], (uint32_t)(s + 1), a.st->sweep + 1u, e.x, e.y, e.z, a.step[rung], px, py, pz);
     a.prop[idx] = make_float4(px, py, pz, 0.0f);
     a.propu[idx] = u;
   }
@@ -614,8 +642,11 @@ __device__ void fast_colour(const SweepArgs& a, int col, unsigned long long* s_d
   const int warp = blockIdx.x * warps_per_block + wib;
   const int n_warps = gridDim.x * warps_per_block;
   const size_t per_warp = fast_group_floats(a.dmax, a.rmax, NR);
-  uint2* rb = reinterpret_cast<uint2*>(zsm + (size_t)wib * per_warp);
-  float* zb = zsm + (size_t)wib * per_warp + fast_rec_floats(a.rmax);
+  uint2* rb = reinterpret_cast<uint2*>(zsm + fast_param_floats(a.n_slots) + (size_t)wib * per_warp);
+  float* zb = zsm + fast_param_floats(a.n_slots) + (size_t)wib * per_warp + fast_rec_floats(a.rmax);
+  const double* p_beta = reinterpret_cast<const double*>(zsm);
+  const double* p_step = p_beta + a.n_slots;
+  const unsigned long long* p_seed = reinterpret_cast<const unsigned long long*>(p_step + a.n_slots);
   const bool do_or = a.pass >= 0;
   for (int item = warp; item < n_items; item += n_warps) {  // warp-uniform
     const int li = find_lattice(seg_c, a.n_lat, item);
@@ -624,12 +655,26 @@ __device__ void fast_colour(const SweepArgs& a, int col, unsigned long long* s_d
     const int R = L.R;
     const int q = local / R;
     const int r = local - q * R;
-    const int s = L.color_sites[L.color_ptr[col] + q];
+    const int4 dsc = __ldg(L.idesc + __ldg(L.color_ptr + col) + q);
+    const int s = dsc.x & 0x3fffffff;
+    if (do_or && !(dsc.x & (1 << 30))) continue;  // warp-uniform: no l = 1 channel
     const int slot = L.slot0 + r;
     const float4* __restrict__ sp = a.spins + L.spin_off;
-    if (do_or && !L.has_l1[s]) continue;  // warp-uniform
-    const int n0 = L.nb_ptr[s], nd = L.nb_ptr[s + 1] - n0;
-    const int j0 = L.fr_ptr[s], nrec = L.fr_ptr[s + 1] - j0;
+    // independent loads of the item, issued before the table walk
+    const float4 e = load_spin<PERSIST>(sp + (int64_t)s * R + r);
+    float4 p4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    double u_pre = 0.0;
+    if (!do_or && a.prop != nullptr) {
+      const int idx = a.item_base[col] + item;
+      p4 = a.prop[idx];
+      u_pre = a.propu[idx];
+    }
+    const int n0 = dsc.y, j0 = dsc.z;
+    const uint32_t cnt = (uint32_t)dsc.w;
+    const int nd = (int)(cnt >> 24);
+    const int n_pair = (int)(cnt & 0xffu), n_trip = (int)((cnt >> 8) & 0xffu), n_quad = (int)((cnt >> 16) & 0xffu);
+    const int n_one = (dsc.x >> 31) & 1;
+    const int nrec = n_pair + n_trip + n_quad + n_one;
     // every record and neighbour spin of the site is requested before any is used
     for (int k = lane; k < nrec; k += 32) rb[k] = __ldg(L.frec + j0 + k);
     for (int k = lane; k < nd; k += 32) {
@@ -638,9 +683,6 @@ __device__ void fast_colour(const SweepArgs& a, int col, unsigned long long* s_d
       zrow_nr<NR>(v.x, v.y, v.z, zb + k * NR);
     }
     __syncwarp();
-    const uint32_t cnt = L.fr_cnt[s];
-    const int n_pair = (int)(cnt & 0xffu), n_trip = (int)((cnt >> 8) & 0xffu), n_quad = (int)((cnt >> 16) & 0xffu);
-    const int n_one = (int)(cnt >> 24);
     float acc = 0.0f, acc2 = 0.0f;
     // pairs: each row lane dots its W row with the neighbour's Z row
     if (row < NR) {
@@ -717,20 +759,16 @@ __device__ void fast_colour(const SweepArgs& a, int col, unsigned long long* s_d
 #pragma unroll
     for (int o = G; o < 32; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     __syncwarp();  // rb / zb are rewritten for the next item
-    const int rung = a.rung_of_slot[slot];
-    const double beta = a.beta[rung];
-    const float4 e = load_spin<PERSIST>(sp + (int64_t)s * R + r);
+    const double beta = p_beta[slot];
     float px, py, pz;
     double u;
     bool attempted = true;
     if (!do_or) {
       if (a.prop != nullptr) {
-        const int idx = a.item_base[col] + item;
-        const float4 p4 = a.prop[idx];
         px = p4.x, py = p4.y, pz = p4.z;
-        u = a.propu[idx];
+        u = u_pre;
       } else {
-        u = keyed_proposal(a.seed[rung], (uint32_t)(s + 1), a.sweep, e.x, e.y, e.z, a.step[rung], px, py, pz);
+        u = keyed_proposal(p_seed[slot], (uint32_t)(s + 1), a.st->sweep + 1u, e.x, e.y, e.z, p_step[slot], px, py, pz);
       }
     } else {
       // reflection about h = (c4, c2, c3): rows 3, 1, 2 live in lanes 2, 0, 1
@@ -750,7 +788,7 @@ __device__ void fast_colour(const SweepArgs& a, int col, unsigned long long* s_d
         py = (float)(r1 / rn);
         pz = (float)(r2 / rn);
       }
-      const Blk bk = philox_block(a.seed[rung], (uint32_t)(s + 1), a.sweep, (uint32_t)a.pass, kTagOR);
+      const Blk bk = philox_block(p_seed[slot], (uint32_t)(s + 1), a.st->sweep + 1u, (uint32_t)a.pass, kTagOR);
       u = philox_uniform(bk.w0, bk.w1);
     }
     float zo[NR], zn[NR];
@@ -791,6 +829,7 @@ __global__ void __launch_bounds__(256) k_fast_colour(SweepArgs a) {
   __shared__ unsigned long long s_dE[kMaxSlots];
   __shared__ unsigned int s_cnt[3 * kMaxSlots];
   zero_block(a.n_slots, s_dE, s_cnt);
+  stage_params(a, zsm);
   fast_colour<LMAX, false>(a, a.colour, s_dE, s_cnt, zsm);
   flush_block(a, s_dE, s_cnt);
 }
@@ -801,14 +840,16 @@ __global__ void __launch_bounds__(256) k_fast_persistent(SweepArgs a) {
   __shared__ unsigned long long s_dE[kMaxSlots];
   __shared__ unsigned int s_cnt[3 * kMaxSlots];
   zero_block(a.n_slots, s_dE, s_cnt);
+  stage_params(a, zsm);
   bool ok = true;
+  int k = 0;
   if (a.pass < 0 && a.prop != nullptr) {
     make_proposals<true>(a);
-    ok = grid_barrier(a.gs, gridDim.x, a.barrier_limit_ns);
+    ok = grid_barrier(a.gs, a.bar_base, k++, gridDim.x, a.barrier_limit_ns);
   }
   for (int col = 0; ok && col < a.max_colors; ++col) {
     fast_colour<LMAX, true>(a, col, s_dE, s_cnt, zsm);
-    if (col + 1 < a.max_colors) ok = grid_barrier(a.gs, gridDim.x, a.barrier_limit_ns);
+    if (col + 1 < a.max_colors) ok = grid_barrier(a.gs, a.bar_base, k++, gridDim.x, a.barrier_limit_ns);
   }
   flush_block(a, s_dE, s_cnt);
 }
@@ -833,6 +874,7 @@ struct TailArgs {
   unsigned long long* swaps;    // per rung x2 {att, acc}
   uint64_t exchange_seed;
   EnsState* st;
+  int bump;  // one sweep completed: advance the device sweep counter
 };
 
 // Energy fold, counters, adaptation and replica exchange (one block).
@@ -845,6 +887,7 @@ __global__ void k_tail(TailArgs t) {
   }
   __syncthreads();
   if (threadIdx.x != 0) return;
+  if (t.bump) t.st->sweep += 1u;
   for (int li = 0; li < t.n_lat; ++li) {
     const DevLattice& L = t.lat[li];
     for (int k = 0; k < L.R; ++k) {
@@ -1119,6 +1162,17 @@ struct scemc_ensemble {
   float4* d_prop = nullptr;
   double* d_propu = nullptr;
   int coop_key[4] = {-1, -1, -1, -1};
+  unsigned long long bar_base = 0;  // host mirror of GridSync::arrived after the enqueued launches
+  int graph_passes_per_launch = 0;
+  // autotuned launch form (used when mode, proposals, lanes are 0)
+  bool tuned = false;
+  int tuned_mode = 2, tuned_proposals = 0, tuned_lanes = 0;
+  // captured compound-sweep graphs keyed by {n_or, fast, precompute, G, recording}
+  struct GraphEntry {
+    int key[5];
+    cudaGraphExec_t exec;
+  };
+  std::vector<GraphEntry> graphs;
   // live timing of the sweep kernels: one event pair per pass
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -1132,6 +1186,7 @@ struct scemc_ensemble {
       ev_pool.push_back(pr.second);
     }
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
+    for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
     void* qs[] = {d_item_base, d_prop, d_propu};
     for (void* p : qs)
       if (p) cudaFree(p);
@@ -1534,6 +1589,15 @@ int32_t compile_tables(const scemc_tables_desc* d, scemc_tables* T) {
     if ((r = upload(T->allocs, F.nb_list, &L.nb_list))) return r;
     if ((r = upload(T->allocs, F.fr_ptr, &L.fr_ptr))) return r;
     if ((r = upload(T->allocs, F.fr_cnt, &L.fr_cnt))) return r;
+    std::vector<int4> idesc(d->n_active);
+    for (int64_t qpos = 0; qpos < d->n_active; ++qpos) {
+      const int32_t site = d->color_sites[qpos] - 1;
+      const uint32_t c = F.fr_cnt[site];
+      const int32_t nd = F.nb_ptr[site + 1] - F.nb_ptr[site];
+      idesc[qpos] = make_int4(site | (d->site_has_l1[site] ? (1 << 30) : 0) | ((c >> 24) ? (int)(1u << 31) : 0),
+                              F.nb_ptr[site], F.fr_ptr[site], (int32_t)((c & 0xffffffu) | ((uint32_t)nd << 24)));
+    }
+    if ((r = upload(T->allocs, idesc, &L.idesc))) return r;
     if ((r = upload(T->allocs, F.frec, &L.frec))) return r;
     if ((r = upload(T->allocs, F.ft, &L.ftensor))) return r;
   }
@@ -1762,6 +1826,7 @@ SweepArgs make_args(scemc_ensemble* E, int pass) {
   a.max_colors = E->max_colors;
   a.pass = pass;
   a.sweep = (uint32_t)(E->sweep_index + 1);
+  a.st = E->d_st;
   a.rung_of_slot = E->d_rung_of_slot;
   a.beta = E->d_beta;
   a.step = E->d_step;
@@ -1802,18 +1867,20 @@ void harvest_events(scemc_ensemble* E) {
     float ms = 0.0f;
     if (cudaEventElapsedTime(&ms, pr.first, pr.second) == cudaSuccess) {
       E->prof_ms += ms;
-      E->prof_passes += 1;
+      E->prof_passes += E->graph_passes_per_launch > 0 ? E->graph_passes_per_launch : 1;
     }
     E->ev_pool.push_back(pr.first);
     E->ev_pool.push_back(pr.second);
   }
   E->ev_pending.clear();
+  E->graph_passes_per_launch = 0;
 }
 
 // Resolved launch configuration of a sweep pass.
 struct Launch {
   int G = 1;          // lanes per item (generic kernel); the fast kernel fixes its own
   int mode = 2;       // 1 = one launch per colour, 2 = persistent cooperative kernel
+  bool graph = false; // per-colour launches of a compound sweep captured in a CUDA graph
   bool fast = false;  // row-parallel fast kernel
   bool precompute = false;  // Metropolis proposals computed before the colour loop
 };
@@ -1832,11 +1899,12 @@ int fast_group(int lmax) { return lmax == 1 ? 4 : 8; }
 void fast_shape(const scemc_ensemble* E, int* threads, size_t* smem) {
   const int NR = fast_rows(E->lmax);
   const size_t per_warp = fast_group_floats(std::max(E->dmax, 1), std::max(E->rmax, 1), NR) * sizeof(float);
+  const size_t params = fast_param_floats(E->n_slots) * sizeof(float);
   int t = 256;
-  size_t m = (size_t)(t / 32) * per_warp;
+  size_t m = params + (size_t)(t / 32) * per_warp;
   while (m > 160 * 1024 && t > 32) {
     t /= 2;
-    m = (size_t)(t / 32) * per_warp;
+    m = params + (size_t)(t / 32) * per_warp;
   }
   *threads = t;
   *smem = m;
@@ -1901,8 +1969,10 @@ int32_t run_pass_impl(scemc_ensemble* E, int pass, const Launch& Lc) {
       int64_t need = ((int64_t)max_items * G + threads - 1) / threads;
       if (a.prop) need = std::max<int64_t>(need, ((int64_t)E->item_base.back() + threads - 1) / threads);
       const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(E->coop_blocks, need));
+      a.bar_base = E->bar_base;
       void* params[] = {&a};
       CUDA_TRY(cudaLaunchCooperativeKernel((const void*)fn, dim3(blocks), dim3(threads), params, smem, E->stream));
+      E->bar_base += (unsigned long long)blocks * ((a.prop ? 1 : 0) + std::max(E->max_colors - 1, 0));
       return SCEMC_OK;
     }
     const int cap = sm_count(E->device) * 16;
@@ -1935,8 +2005,10 @@ int32_t run_pass_impl(scemc_ensemble* E, int pass, const Launch& Lc) {
     }
     const int want = (int)std::min<int64_t>(E->coop_blocks, ((int64_t)max_items * G + threads - 1) / threads);
     const int blocks = std::max(1, want);
+    a.bar_base = E->bar_base;
     void* params[] = {&a};
     CUDA_TRY(cudaLaunchCooperativeKernel((const void*)fn, dim3(blocks), dim3(threads), params, 0, E->stream));
+    E->bar_base += (unsigned long long)blocks * std::max(E->max_colors - 1, 0);
     return SCEMC_OK;
   }
   KFn fn = kernel_for(lmax, G, false);
@@ -1952,8 +2024,9 @@ int32_t run_pass_impl(scemc_ensemble* E, int pass, const Launch& Lc) {
   return SCEMC_OK;
 }
 
-int32_t launch_tail(scemc_ensemble* E, bool add_att, bool adapt, double target, bool exchange) {
+int32_t launch_tail(scemc_ensemble* E, bool add_att, bool adapt, double target, bool exchange, bool bump) {
   TailArgs t{};
+  t.bump = bump;
   t.n_slots = E->n_slots;
   t.n_rungs = E->n_slots;
   t.n_lat = (int32_t)E->tabs.size();
@@ -2055,6 +2128,7 @@ int32_t check_error(scemc_ensemble* E) {
   if (gs.error) {
     GridSync z{};
     cudaMemcpy(E->d_gs, &z, sizeof(z), cudaMemcpyHostToDevice);
+    E->bar_base = 0;
     return fail(SCEMC_ERR_TIMEOUT, "grid barrier wait gave up (bounded spin); state of this sweep is torn");
   }
   return SCEMC_OK;
@@ -2075,8 +2149,17 @@ int auto_lanes(const scemc_ensemble* E) {
 // kernel: 0 auto, 1 generic, 2 fast; proposals: 0 auto, 1 precompute, 2 inline.
 int32_t resolve_launch(const scemc_ensemble* E, int lanes, int mode, int kernel, int proposals, Launch* out) {
   Launch L;
+  if (mode == 0 && E->tuned) {
+    mode = E->tuned_mode;
+    if (proposals == 0) proposals = E->tuned_proposals;
+    if (lanes == 0) lanes = E->tuned_lanes;
+  }
   L.mode = mode == 0 ? 2 : mode;
-  if (L.mode != 1 && L.mode != 2) return fail(SCEMC_ERR_ARG, "mode must be 0, 1 or 2");
+  if (L.mode < 1 || L.mode > 3) return fail(SCEMC_ERR_ARG, "mode must be 0..3");
+  if (L.mode == 3) {
+    L.graph = true;
+    L.mode = 1;
+  }
   if (kernel < 0 || kernel > 2 || proposals < 0 || proposals > 2)
     return fail(SCEMC_ERR_ARG, "kernel and proposals must be 0, 1 or 2");
   bool generic_ok = true;
@@ -2102,6 +2185,51 @@ int32_t sweep_once(scemc_ensemble* E, int n_or, const Launch& L) {
   if ((rc = run_pass(E, -1, L))) return rc;
   for (int k = 0; k < n_or; ++k)
     if ((rc = run_pass(E, k, L))) return rc;
+  return SCEMC_OK;
+}
+
+// The passes and tail of one compound sweep as a CUDA graph (captured once per
+// configuration, replayed every sweep). Every launch reads the sweep counter from
+// device memory and the tail advances it, so one capture serves all sweeps.
+int32_t sweep_graph(scemc_ensemble* E, int n_or, const Launch& L, cudaGraphExec_t* out) {
+  const int key[5] = {n_or, L.fast ? 1 : 0, L.precompute ? 1 : 0, L.fast ? 0 : L.G, E->recording ? 1 : 0};
+  for (auto& g : E->graphs)
+    if (std::equal(key, key + 5, g.key)) {
+      *out = g.exec;
+      return SCEMC_OK;
+    }
+  int32_t rc;
+  if (L.fast && L.precompute)
+    if ((rc = ensure_props(E))) return rc;
+  if (L.fast) {  // attributes are set outside the capture
+    int threads;
+    size_t smem;
+    fast_shape(E, &threads, &smem);
+    CUDA_TRY(cudaFuncSetAttribute((const void*)fast_kernel(E->lmax, false),
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  }
+  const bool prof = E->profiling;
+  E->profiling = false;  // graph launches are timed as a whole
+  CUDA_TRY(cudaStreamBeginCapture(E->stream, cudaStreamCaptureModeThreadLocal));
+  rc = sweep_once(E, n_or, L);
+  if (!rc) rc = launch_tail(E, true, false, 0.5, false, true);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(E->stream, &graph);
+  E->profiling = prof;
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (ce != cudaSuccess) return fail(SCEMC_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(ce));
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ie != cudaSuccess) return fail(SCEMC_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+  scemc_ensemble::GraphEntry g;
+  std::copy(key, key + 5, g.key);
+  g.exec = exec;
+  E->graphs.push_back(g);
+  *out = exec;
   return SCEMC_OK;
 }
 
@@ -2201,7 +2329,7 @@ int32_t scemc_metropolis_sweep(scemc_chain* c, const scemc_tables* t, double bet
   Launch L;
   if ((rc = resolve_launch(c, lanes_per_site, 1, 0, 0, &L))) return rc;
   if ((rc = sweep_once(c, 0, L))) return rc;
-  if ((rc = launch_tail(c, true, false, 0.5, false))) return rc;
+  if ((rc = launch_tail(c, true, false, 0.5, false, true))) return rc;
   unsigned long long after = 0;
   CUDA_TRY(cudaMemcpyAsync(&after, c->d_cnt, 8, cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -2225,7 +2353,7 @@ int32_t scemc_overrelaxation_sweep(scemc_chain* c, const scemc_tables* t, double
   Launch L;
   if ((rc = resolve_launch(c, lanes_per_site, 1, 0, 0, &L))) return rc;
   if ((rc = run_pass(c, 0, L))) return rc;
-  if ((rc = launch_tail(c, false, false, 0.5, false))) return rc;
+  if ((rc = launch_tail(c, false, false, 0.5, false, true))) return rc;
   CUDA_TRY(cudaMemcpyAsync(after, c->d_cnt, 32, cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   c->sweep_index += 1;
@@ -2244,7 +2372,7 @@ int32_t scemc_run_sweeps(scemc_chain* c, const scemc_tables* t, double beta, int
   if ((rc = resolve_launch(c, lanes_per_site, 1, 0, 0, &L))) return rc;
   for (int64_t i = 1; i <= nsweeps; ++i) {
     if ((rc = sweep_once(c, 0, L))) return rc;
-    if ((rc = launch_tail(c, true, false, 0.5, false))) return rc;
+    if ((rc = launch_tail(c, true, false, 0.5, false, true))) return rc;
     c->sweep_index += 1;
     if (renorm_interval > 0 && i % renorm_interval == 0)
       if ((rc = recompute(c, 1))) return rc;
@@ -2347,23 +2475,107 @@ int32_t scemc_batch_run_async(scemc_batch* b, const scemc_run_params* p) {
     if (rc) return rc;
   }
   if (p->phase_done < 0 || p->phase_total < 0) return fail(SCEMC_ERR_ARG, "bad phase bookkeeping");
+  if (p->mode < 0 || p->mode > 3) return fail(SCEMC_ERR_ARG, "mode must be 0..3");
   const int64_t total = p->phase_total > 0 ? p->phase_total : p->phase_done + p->nsweeps;
   int32_t rc;
   Launch L;
   if ((rc = resolve_launch(b, p->lanes_per_site, p->mode, p->kernel, p->proposals, &L))) return rc;
+  if (b->sweep_index + p->nsweeps >= 0x7ffffffell - 1)
+    return fail(SCEMC_ERR_EXHAUSTED, "sweep_index would exhaust the 32-bit RNG counter word");
+  cudaGraphExec_t exec = nullptr;
+  if (L.graph) {
+    if ((rc = sweep_graph(b, p->or_per_metropolis, L, &exec))) return rc;
+  }
   for (int64_t k = 1; k <= p->nsweeps; ++k) {
     const int64_t i = p->phase_done + k;
-    if ((rc = sweep_once(b, p->or_per_metropolis, L))) return rc;
-    b->sweep_index += 1;
     const bool adapt = p->adapt_interval > 0 && i % p->adapt_interval == 0;
-    if ((rc = launch_tail(b, true, adapt, p->adapt_target, false))) return rc;
+    if (exec) {
+      // passes + tail (fold, att, sweep counter) replayed as one graph
+      cudaEvent_t e0 = nullptr, e1 = nullptr;
+      if (b->profiling) {
+        e0 = take_event(b);
+        e1 = take_event(b);
+        CUDA_TRY(cudaEventRecord(e0, b->stream));
+      }
+      CUDA_TRY(cudaGraphLaunch(exec, b->stream));
+      if (b->profiling) {
+        CUDA_TRY(cudaEventRecord(e1, b->stream));
+        b->ev_pending.emplace_back(e0, e1);
+        b->graph_passes_per_launch = 1 + p->or_per_metropolis;
+      }
+      if (adapt)
+        if ((rc = launch_tail(b, false, true, p->adapt_target, false, false))) return rc;
+    } else {
+      if ((rc = sweep_once(b, p->or_per_metropolis, L))) return rc;
+      if ((rc = launch_tail(b, true, adapt, p->adapt_target, false, true))) return rc;
+    }
+    b->sweep_index += 1;
     if (p->renorm_interval > 0 && i % p->renorm_interval == 0)
       if ((rc = recompute(b, 1))) return rc;
     if (p->measure_interval > 0 && i % p->measure_interval == 0)
       if ((rc = measure(b))) return rc;
     if (p->exchange && i % p->exchange_interval == 0 && i < total)
-      if ((rc = launch_tail(b, false, false, 0.5, true))) return rc;
+      if ((rc = launch_tail(b, false, false, 0.5, true, false))) return rc;
   }
+  return SCEMC_OK;
+}
+
+int32_t scemc_batch_autotune(scemc_batch* b, int32_t or_per_metropolis, int32_t sweeps_per_trial, int32_t* mode,
+                             int32_t* proposals, int32_t* lanes, double* ms_per_sweep) {
+  if (!b || or_per_metropolis < 0 || sweeps_per_trial < 1) return fail(SCEMC_ERR_ARG, "bad autotune arguments");
+  struct Cand {
+    int mode, proposals, lanes;
+  };
+  std::vector<Cand> cands;
+  if (b->fast) {
+    for (int m : {2, 3})
+      for (int q : {1, 2}) cands.push_back({m, q, 0});
+  } else {
+    for (int m : {2, 3})
+      for (int g : {1, 4, 8, 32}) cands.push_back({m, 0, g});
+  }
+  const bool prof = b->profiling;
+  b->profiling = false;
+  b->tuned = false;
+  double best = 1e300;
+  Cand bc = cands[0];
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+  int32_t rc = SCEMC_OK;
+  for (const Cand& c : cands) {
+    scemc_run_params p{};
+    p.nsweeps = 1;
+    p.or_per_metropolis = or_per_metropolis;
+    p.mode = c.mode;
+    p.proposals = c.proposals;
+    p.lanes_per_site = c.lanes;
+    if ((rc = scemc_batch_run(b, &p))) break;  // warm-up (builds graphs, sets attributes)
+    p.nsweeps = sweeps_per_trial;
+    cudaEventRecord(e0, b->stream);
+    if ((rc = scemc_batch_run_async(b, &p))) break;
+    cudaEventRecord(e1, b->stream);
+    if ((rc = scemc_batch_sync(b))) break;
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    const double per = ms / sweeps_per_trial;
+    if (per < best) {
+      best = per;
+      bc = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->profiling = prof;
+  if (rc) return rc;
+  b->tuned = true;
+  b->tuned_mode = bc.mode;
+  b->tuned_proposals = bc.proposals;
+  b->tuned_lanes = bc.lanes;
+  if (mode) *mode = bc.mode;
+  if (proposals) *proposals = bc.proposals;
+  if (lanes) *lanes = bc.lanes;
+  if (ms_per_sweep) *ms_per_sweep = best;
   return SCEMC_OK;
 }
 
@@ -2471,6 +2683,8 @@ int32_t scemc_batch_fetch_measurements(scemc_batch* b, double* rec, int64_t capa
 int32_t scemc_batch_record(scemc_batch* b, int32_t on) {
   if (!b) return fail(SCEMC_ERR_ARG, "batch is NULL");
   b->recording = on != 0;
+  for (auto& g : b->graphs) cudaGraphExecDestroy(g.exec);
+  b->graphs.clear();
   const size_t n = (size_t)b->tabs[0]->n_sites * kRecPasses;
   if (b->recording && !b->d_rprop) {
     int32_t rc;

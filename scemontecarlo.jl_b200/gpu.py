@@ -267,6 +267,14 @@ class GPUBatch:
     def profile(self, on: bool):
         check(_lib.lib().scemc_batch_profile(self.h, int(bool(on))))
 
+    def autotune(self, or_per_metropolis: int = 0, sweeps_per_trial: int = 5):
+        """Times the launch forms on this batch (its chains advance) and keeps the
+        fastest for runs with mode=0; returns (mode, proposals, lanes, ms/sweep)."""
+        m, q, g, ms = C.c_int32(), C.c_int32(), C.c_int32(), C.c_double()
+        check(_lib.lib().scemc_batch_autotune(self.h, int(or_per_metropolis), int(sweeps_per_trial), C.byref(m),
+                                              C.byref(q), C.byref(g), C.byref(ms)))
+        return m.value, q.value, g.value, ms.value
+
     def kernel_time(self):
         """(summed device ms of the sweep passes, number of passes) since profile(True)."""
         ms, n = C.c_double(), C.c_int64()

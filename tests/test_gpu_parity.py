@@ -127,6 +127,8 @@ REPLAY_CASES = [(m, 4, 2, 1, 0) for m in MODELS] + [(m, 0, 2, 0, 1) for m in FAS
     ("fourbody", 32, 2, 1, 0), ("sc_J1J2", 8, 1, 1, 0), ("fcc_l2_tri_zeeman", 16, 2, 1, 0),
     ("bcc_l2_plaq_zeeman", 0, 1, 0, 2), ("bcc_l2_plaq_zeeman", 0, 1, 0, 1), ("bcc_l2_plaq_zeeman", 0, 2, 0, 2),
     ("fcc_l2_tri_zeeman", 0, 1, 0, 2), ("threebody", 0, 1, 0, 1), ("chain", 0, 2, 0, 2),
+    ("bcc_l2_plaq_zeeman", 0, 3, 0, 1), ("fcc_l2_tri_zeeman", 0, 3, 0, 2), ("biquadratic", 4, 3, 1, 0),
+    ("mixed", 8, 3, 0, 0),
 ]
 
 
@@ -168,7 +170,7 @@ def test_fast_kernel_is_launch_shape_independent(gpu):
     gH = scemc.GPUTiledHamiltonian(H)
     cfg = rand_cfg(H.n_sites, 3)
     outs = []
-    for mode, prop in [(1, 1), (1, 2), (2, 1), (2, 2)]:
+    for mode, prop in [(1, 1), (1, 2), (2, 1), (2, 2), (3, 1), (3, 2)]:
         b = scemc.GPUBatch([gH], [2], [cfg, cfg], [9, 10], 0.6)
         b.set_betas([1 / 0.002, 1 / 0.01])
         b.run(6, or_per_metropolis=1, mode=mode, proposals=prop, kernel=2)
@@ -177,6 +179,22 @@ def test_fast_kernel_is_launch_shape_independent(gpu):
     for o in outs[1:]:
         assert np.array_equal(o[0], outs[0][0]) and np.array_equal(o[1], outs[0][1])
         assert np.array_equal(o[2], outs[0][2])
+
+
+def test_autotune_keeps_a_valid_launch_form(gpu):
+    H, _ = build("bcc_l2_plaq_zeeman")
+    gH = scemc.GPUTiledHamiltonian(H)
+    b = scemc.GPUBatch([gH], [3], [rand_cfg(H.n_sites, i) for i in range(3)], [1, 2, 3], 0.6)
+    b.set_betas([1 / 0.002, 1 / 0.004, 1 / 0.008])
+    mode, prop, lanes, ms = b.autotune(or_per_metropolis=1, sweeps_per_trial=3)
+    assert mode in (2, 3) and prop in (1, 2) and ms > 0
+    before = b.download()["counters"].copy()
+    b.run(4, or_per_metropolis=1)  # mode 0 now uses the tuned form
+    after = b.download()["counters"]
+    assert np.all(after[:, 1] - before[:, 1] == 4 * H.n_active)
+    for r in range(3):
+        st = b.download()
+        assert abs(st["energies"][r] - b.total_energy(r)) <= 1e-5 * max(1.0, abs(st["energies"][r]))
 
 
 def test_fast_kernel_refused_where_it_does_not_apply(gpu):
