@@ -184,7 +184,9 @@ typedef struct scemc_run_params {
    * (phase_total; 0 means phase_done + nsweeps). */
   int64_t phase_done;
   int64_t phase_total;
-  int32_t kernel;     /* 0 = auto, 1 = generic record walk, 2 = row-parallel fast kernel */
+  int32_t kernel;     /* 0 = auto, 1 = generic record walk, 2 = row-parallel fast kernel (one warp per
+                         item), 3 = replica-parallel kernel (one thread per item; per-colour launches,
+                         mode 1 or 3) */
   int32_t proposals;  /* 0 = auto, 1 = precompute a pass's Metropolis proposals, 2 = inline */
 } scemc_run_params;
 
@@ -205,13 +207,18 @@ int32_t scemc_batch_upload(scemc_batch* b, const double* configs, const double* 
  * CUDA event pair on the batch stream; scemc_batch_kernel_time returns the summed
  * device time (ms) and the number of passes since profiling was switched on. */
 int32_t scemc_batch_profile(scemc_batch* b, int32_t on);
-/* Times the launch forms (modes 2 and 3; proposal precompute on/off for the fast
- * kernel, lanes per site for the generic one) for sweeps_per_trial compound sweeps
- * each and keeps the fastest for runs with mode = 0. The trial sweeps are real
- * sweeps of the batch (its chains advance). Outputs may be NULL. */
+/* Times the launch forms (modes 2 and 3; for fast tables the row- and
+ * replica-parallel kernels with proposal precompute on/off, for the generic kernel
+ * the lanes per site) for sweeps_per_trial compound sweeps each and keeps the
+ * fastest for runs with mode = 0 and kernel = 0. The trial sweeps are real sweeps of
+ * the batch (its chains advance). Outputs may be NULL. */
 int32_t scemc_batch_autotune(scemc_batch* b, int32_t or_per_metropolis, int32_t sweeps_per_trial, int32_t* mode,
-                             int32_t* proposals, int32_t* lanes, double* ms_per_sweep);
+                             int32_t* proposals, int32_t* lanes, int32_t* kernel, double* ms_per_sweep);
 int32_t scemc_batch_kernel_time(const scemc_batch* b, double* ms, int64_t* passes);
+/* Number of kernels the batch has enqueued on its stream since creation: sweep
+ * passes, proposal precompute, tails, recomputes and measurements; a replayed
+ * sweep graph adds its kernel nodes. */
+int32_t scemc_batch_launches(const scemc_batch* b, int64_t* launches);
 /* State readback. configs: 3 x n_sites per SLOT (payload order); energies per slot;
  * slot_of_rung per rung; counters 4 per rung {acc_metro, att_metro, acc_or, att_or};
  * swap counters 2 per rung pair {attempted, accepted} (pair r = rungs r, r+1 of one

@@ -94,7 +94,8 @@ SIGNATURES = [
     ("scemc_batch_upload", C.c_int32, [C.c_void_p, F64P, F64P]),
     ("scemc_batch_profile", C.c_int32, [C.c_void_p, C.c_int32]),
     ("scemc_batch_kernel_time", C.c_int32, [C.c_void_p, F64P, I64P]),
-    ("scemc_batch_autotune", C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, I32P, I32P, I32P, F64P]),
+    ("scemc_batch_launches", C.c_int32, [C.c_void_p, I64P]),
+    ("scemc_batch_autotune", C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, I32P, I32P, I32P, I32P, F64P]),
     ("scemc_batch_download", C.c_int32, [C.c_void_p, F64P, F64P, I32P, I64P, I64P, F64P, F64P]),
     ("scemc_batch_reset_counters", C.c_int32, [C.c_void_p]),
     ("scemc_batch_fetch_measurements", C.c_int32, [C.c_void_p, F64P, C.c_int64, I64P, I32P]),

@@ -856,6 +856,217 @@ __global__ void __launch_bounds__(256) k_fast_persistent(SweepArgs a) {
 
 __global__ void __launch_bounds__(256) k_proposals(SweepArgs a) { make_proposals<false>(a); }
 
+// ---------------------------------------------------------------------------
+// Replica-parallel sweep (same tables as the row-parallel kernel). One thread per
+// (site, replica) item; items run replica-fastest, so when a lattice carries 32 or
+// more replicas a warp holds consecutive replicas of one site: every table word
+// (descriptor, record, W block) is a warp-uniform broadcast and each neighbour
+// gather spins[nb * R + r] is one coalesced transaction. Each thread keeps the
+// site's NR coefficients in registers, c_t = sum_j W_j[t, :] . z_j, and forms
+// dE = sum_t c_t (znew_t - zold_t) itself, so no shuffles or shared-memory rows are
+// needed. Built for large replica counts (many PT rungs of one Hamiltonian).
+// ---------------------------------------------------------------------------
+template <int LMAX>
+__device__ void rep_colour(const SweepArgs& a, int col, unsigned long long* s_dE, unsigned int* s_cnt,
+                           const float* zsm) {
+  constexpr int NR = (LMAX + 1) * (LMAX + 1) - 1;
+  const int32_t* seg_c = a.seg + (size_t)col * (a.n_lat + 1);
+  const int n_items = seg_c[a.n_lat];
+  const double* p_beta = reinterpret_cast<const double*>(zsm);
+  const double* p_step = p_beta + a.n_slots;
+  const unsigned long long* p_seed = reinterpret_cast<const unsigned long long*>(p_step + a.n_slots);
+  const bool do_or = a.pass >= 0;
+  const int stride = gridDim.x * blockDim.x;
+  for (int item = blockIdx.x * blockDim.x + threadIdx.x; item < n_items; item += stride) {
+    const int li = find_lattice(seg_c, a.n_lat, item);
+    const DevLattice& L = a.lat[li];
+    const int local = item - seg_c[li];
+    const int R = L.R;
+    const int q = local / R;
+    const int r = local - q * R;
+    const int4 dsc = __ldg(L.idesc + __ldg(L.color_ptr + col) + q);
+    const int s = dsc.x & 0x3fffffff;
+    if (do_or && !(dsc.x & (1 << 30))) continue;  // no l = 1 channel
+    const int slot = L.slot0 + r;
+    const float4* __restrict__ sp = a.spins + L.spin_off;
+    const float4 e = __ldg(sp + (int64_t)s * R + r);
+    const int n0 = dsc.y, j0 = dsc.z;
+    const uint32_t cnt = (uint32_t)dsc.w;
+    const int n_pair = (int)(cnt & 0xffu), n_trip = (int)((cnt >> 8) & 0xffu), n_quad = (int)((cnt >> 16) & 0xffu);
+    const int n_one = (dsc.x >> 31) & 1;
+    const uint2* __restrict__ fr = L.frec + j0;
+    const int32_t* __restrict__ nbl = L.nb_list + n0;
+    const float* __restrict__ ft = L.ftensor;
+    float c[NR];
+#pragma unroll
+    for (int t = 0; t < NR; ++t) c[t] = 0.0f;
+    // merged per-neighbour pair blocks: c += W z_nb
+#pragma unroll 2
+    for (int j = 0; j < n_pair; ++j) {
+      const uint2 rec = __ldg(fr + j);
+      const float4 v = __ldcg(sp + (int64_t)__ldg(nbl + (rec.y & 0xffu)) * R + r);
+      float z[NR];
+      zrow_nr<NR>(v.x, v.y, v.z, z);
+      const float4* w4 = reinterpret_cast<const float4*>(ft + (rec.x & kOffMask));
+      if constexpr (NR == 8) {
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+          const float4 a0 = __ldg(w4 + 2 * t), a1 = __ldg(w4 + 2 * t + 1);
+          float x = c[t];
+          x = fmaf(a0.x, z[0], x);
+          x = fmaf(a0.y, z[1], x);
+          x = fmaf(a0.z, z[2], x);
+          x = fmaf(a0.w, z[3], x);
+          x = fmaf(a1.x, z[4], x);
+          x = fmaf(a1.y, z[5], x);
+          x = fmaf(a1.z, z[6], x);
+          x = fmaf(a1.w, z[7], x);
+          c[t] = x;
+        }
+      } else {
+        const float4 a0 = __ldg(w4), a1 = __ldg(w4 + 1);
+        const float a8 = __ldg(ft + (rec.x & kOffMask) + 8);
+        const float w[9] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a8};
+#pragma unroll
+        for (int t = 0; t < 3; ++t)
+          c[t] = fmaf(w[3 * t], z[0], fmaf(w[3 * t + 1], z[1], fmaf(w[3 * t + 2], z[2], c[t])));
+      }
+    }
+    // l = 1 triplets: c_t += sum_p z1_p sum_q W[t][3p + q] z2_q (rows padded to 12)
+    for (int j = n_pair; j < n_pair + n_trip; ++j) {
+      const uint2 rec = __ldg(fr + j);
+      const float4 v1 = __ldcg(sp + (int64_t)__ldg(nbl + (rec.y & 0xffu)) * R + r);
+      const float4 v2 = __ldcg(sp + (int64_t)__ldg(nbl + ((rec.y >> 8) & 0xffu)) * R + r);
+      float z1[3], z2[3];
+      zrow_l1(v1.x, v1.y, v1.z, z1);
+      zrow_l1(v2.x, v2.y, v2.z, z2);
+      const float4* w4 = reinterpret_cast<const float4*>(ft + (rec.x & kOffMask));
+#pragma unroll
+      for (int t = 0; t < 3; ++t) {
+        const float4 a0 = __ldg(w4 + 3 * t), a1 = __ldg(w4 + 3 * t + 1), a2 = __ldg(w4 + 3 * t + 2);
+        const float w[9] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a2.x};
+        float x = c[t];
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {
+          const float u = fmaf(w[p * 3 + 0], z2[0], fmaf(w[p * 3 + 1], z2[1], w[p * 3 + 2] * z2[2]));
+          x = fmaf(z1[p], u, x);
+        }
+        c[t] = x;
+      }
+    }
+    // l = 1 quads (rows padded to 28)
+    for (int j = n_pair + n_trip; j < n_pair + n_trip + n_quad; ++j) {
+      const uint2 rec = __ldg(fr + j);
+      const float4 v1 = __ldcg(sp + (int64_t)__ldg(nbl + (rec.y & 0xffu)) * R + r);
+      const float4 v2 = __ldcg(sp + (int64_t)__ldg(nbl + ((rec.y >> 8) & 0xffu)) * R + r);
+      const float4 v3 = __ldcg(sp + (int64_t)__ldg(nbl + ((rec.y >> 16) & 0xffu)) * R + r);
+      float z1[3], z2[3], z3[3];
+      zrow_l1(v1.x, v1.y, v1.z, z1);
+      zrow_l1(v2.x, v2.y, v2.z, z2);
+      zrow_l1(v3.x, v3.y, v3.z, z3);
+      const float4* w4 = reinterpret_cast<const float4*>(ft + (rec.x & kOffMask));
+#pragma unroll
+      for (int t = 0; t < 3; ++t) {
+        float w[28];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+          const float4 v = __ldg(w4 + 7 * t + k);
+          w[4 * k] = v.x, w[4 * k + 1] = v.y, w[4 * k + 2] = v.z, w[4 * k + 3] = v.w;
+        }
+        float x = c[t];
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {
+          float t2 = 0.0f;
+#pragma unroll
+          for (int qq = 0; qq < 3; ++qq) {
+            const int o = (p * 3 + qq) * 3;
+            const float t3 = fmaf(w[o], z3[0], fmaf(w[o + 1], z3[1], w[o + 2] * z3[2]));
+            t2 = fmaf(z2[qq], t3, t2);
+          }
+          x = fmaf(z1[p], t2, x);
+        }
+        c[t] = x;
+      }
+    }
+    if (n_one) {
+      const float* w = ft + (__ldg(fr + n_pair + n_trip + n_quad).x & kOffMask);
+#pragma unroll
+      for (int t = 0; t < NR; ++t) c[t] += __ldg(w + t);
+    }
+    const double beta = p_beta[slot];
+    float px, py, pz;
+    double u;
+    bool attempted = true;
+    if (!do_or) {
+      if (a.prop != nullptr) {
+        const int idx = a.item_base[col] + item;
+        const float4 p4 = a.prop[idx];
+        px = p4.x, py = p4.y, pz = p4.z;
+        u = a.propu[idx];
+      } else {
+        u = keyed_proposal(p_seed[slot], (uint32_t)(s + 1), a.st->sweep + 1u, e.x, e.y, e.z, p_step[slot], px, py, pz);
+      }
+    } else {
+      // reflection about h = (c4, c2, c3) = rows (3, 1, 2)
+      const double h0 = c[2], h1 = c[0], h2 = c[1];
+      const double hn = sqrt((h0 * h0 + h1 * h1) + h2 * h2);
+      if (hn < 1e-12) {
+        attempted = false;
+        px = e.x, py = e.y, pz = e.z;
+      } else {
+        const double a0 = h0 / hn, a1 = h1 / hn, a2 = h2 / hn;
+        const double d2 = 2.0 * (((double)e.x * a0 + (double)e.y * a1) + (double)e.z * a2);
+        const double r0 = d2 * a0 - e.x, r1 = d2 * a1 - e.y, r2 = d2 * a2 - e.z;
+        const double rn = sqrt((r0 * r0 + r1 * r1) + r2 * r2);
+        px = (float)(r0 / rn);
+        py = (float)(r1 / rn);
+        pz = (float)(r2 / rn);
+      }
+      const Blk bk = philox_block(p_seed[slot], (uint32_t)(s + 1), a.st->sweep + 1u, (uint32_t)a.pass, kTagOR);
+      u = philox_uniform(bk.w0, bk.w1);
+    }
+    float zo[NR], zn[NR];
+    zrow_nr<NR>(e.x, e.y, e.z, zo);
+    zrow_nr<NR>(px, py, pz, zn);
+    float term = 0.0f;
+#pragma unroll
+    for (int t = 0; t < NR; ++t) term = fmaf(c[t], zn[t] - zo[t], term);
+    const float dE = attempted ? term : 0.0f;
+    const bool acc_ok = attempted && (dE <= 0.0f || u < exp(-beta * (double)dE));
+    if (acc_ok) {
+      a.spins[L.spin_off + (int64_t)s * R + r] = make_float4(px, py, pz, 0.0f);
+      atomicAdd(s_dE + slot, (unsigned long long)llrint((double)dE * kFixScale));
+    }
+    if (do_or) {
+      if (attempted) atomicAdd(s_cnt + 3 * slot + 2, 1u);
+      if (acc_ok) atomicAdd(s_cnt + 3 * slot + 1, 1u);
+    } else if (acc_ok) {
+      atomicAdd(s_cnt + 3 * slot + 0, 1u);
+    }
+    if (a.rec_prop != nullptr && li == 0 && r == 0 && a.pass + 1 < kRecPasses) {
+      const int64_t qq = (int64_t)(a.pass + 1) * L.n_sites + s;
+      a.rec_prop[3 * qq + 0] = px;
+      a.rec_prop[3 * qq + 1] = py;
+      a.rec_prop[3 * qq + 2] = pz;
+      a.rec_u[qq] = u;
+      a.rec_dE[qq] = dE;
+      a.rec_acc[qq] = (uint8_t)(acc_ok ? 1 : (attempted ? 0 : 2));
+    }
+  }
+}
+
+template <int LMAX>
+__global__ void __launch_bounds__(256) k_rep_colour(SweepArgs a) {
+  extern __shared__ __align__(16) float zsm[];
+  __shared__ unsigned long long s_dE[kMaxSlots];
+  __shared__ unsigned int s_cnt[3 * kMaxSlots];
+  zero_block(a.n_slots, s_dE, s_cnt);
+  stage_params(a, zsm);
+  rep_colour<LMAX>(a, a.colour, s_dE, s_cnt, zsm);
+  flush_block(a, s_dE, s_cnt);
+}
+
+
 struct TailArgs {
   int32_t n_slots, n_rungs, n_lat;
   const DevLattice* lat;
@@ -1166,12 +1377,14 @@ struct scemc_ensemble {
   int graph_passes_per_launch = 0;
   // autotuned launch form (used when mode, proposals, lanes are 0)
   bool tuned = false;
-  int tuned_mode = 2, tuned_proposals = 0, tuned_lanes = 0;
+  int tuned_mode = 2, tuned_proposals = 0, tuned_lanes = 0, tuned_kernel = 0;
   // captured compound-sweep graphs keyed by {n_or, fast, precompute, G, recording}
   struct GraphEntry {
     int key[5];
     cudaGraphExec_t exec;
+    int64_t launches;  // kernel nodes in the graph
   };
+  int64_t launches = 0;  // kernels enqueued on the stream (a graph replay adds its kernel nodes)
   std::vector<GraphEntry> graphs;
   // live timing of the sweep kernels: one event pair per pass
   bool profiling = false;
@@ -1881,7 +2094,8 @@ struct Launch {
   int G = 1;          // lanes per item (generic kernel); the fast kernel fixes its own
   int mode = 2;       // 1 = one launch per colour, 2 = persistent cooperative kernel
   bool graph = false; // per-colour launches of a compound sweep captured in a CUDA graph
-  bool fast = false;  // row-parallel fast kernel
+  bool fast = false;  // row-parallel fast kernel (one warp per item)
+  bool rep = false;   // replica-parallel kernel (one thread per item, per-colour launches)
   bool precompute = false;  // Metropolis proposals computed before the colour loop
 };
 
@@ -1941,6 +2155,33 @@ int32_t run_pass_impl(scemc_ensemble* E, int pass, const Launch& Lc) {
   const int lmax = E->lmax;
   SweepArgs a = make_args(E, pass);
   const int max_items = max_colour_items(E);
+  if (Lc.rep) {
+    const int threads = 256;
+    const size_t smem = fast_param_floats(E->n_slots) * sizeof(float);
+    a.item_base = E->d_item_base;
+    const int cap = sm_count(E->device) * 64;
+    if (Lc.precompute && pass < 0) {
+      int32_t rc;
+      if ((rc = ensure_props(E))) return rc;
+      a.prop = E->d_prop;
+      a.propu = E->d_propu;
+      const int blocks = (int)std::min<int64_t>(cap, ((int64_t)E->item_base.back() + 255) / 256);
+      ++E->launches;
+      k_proposals<<<std::max(blocks, 1), 256, 0, E->stream>>>(a);
+      CUDA_TRY(cudaGetLastError());
+    }
+    FastFn fn = lmax == 1 ? k_rep_colour<1> : k_rep_colour<2>;
+    for (int c = 0; c < E->max_colors; ++c) {
+      const int n = E->seg[(size_t)c * (E->tabs.size() + 1) + E->tabs.size()];
+      if (n == 0) continue;
+      a.colour = c;
+      const int blocks = (int)std::min<int64_t>(cap, ((int64_t)n + threads - 1) / threads);
+      ++E->launches;
+      fn<<<std::max(blocks, 1), threads, smem, E->stream>>>(a);
+      CUDA_TRY(cudaGetLastError());
+    }
+    return SCEMC_OK;
+  }
   if (Lc.fast) {
     int threads;
     size_t smem;
@@ -1971,6 +2212,7 @@ int32_t run_pass_impl(scemc_ensemble* E, int pass, const Launch& Lc) {
       const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(E->coop_blocks, need));
       a.bar_base = E->bar_base;
       void* params[] = {&a};
+      ++E->launches;
       CUDA_TRY(cudaLaunchCooperativeKernel((const void*)fn, dim3(blocks), dim3(threads), params, smem, E->stream));
       E->bar_base += (unsigned long long)blocks * ((a.prop ? 1 : 0) + std::max(E->max_colors - 1, 0));
       return SCEMC_OK;
@@ -1978,6 +2220,7 @@ int32_t run_pass_impl(scemc_ensemble* E, int pass, const Launch& Lc) {
     const int cap = sm_count(E->device) * 16;
     if (a.prop) {
       const int blocks = (int)std::min<int64_t>(cap, ((int64_t)E->item_base.back() + 255) / 256);
+      ++E->launches;
       k_proposals<<<std::max(blocks, 1), 256, 0, E->stream>>>(a);
       CUDA_TRY(cudaGetLastError());
     }
@@ -1986,6 +2229,7 @@ int32_t run_pass_impl(scemc_ensemble* E, int pass, const Launch& Lc) {
       if (n == 0) continue;
       a.colour = c;
       const int blocks = (int)std::min<int64_t>(cap, ((int64_t)n * G + threads - 1) / threads);
+      ++E->launches;
       fn<<<std::max(blocks, 1), threads, smem, E->stream>>>(a);
       CUDA_TRY(cudaGetLastError());
     }
@@ -2007,6 +2251,7 @@ int32_t run_pass_impl(scemc_ensemble* E, int pass, const Launch& Lc) {
     const int blocks = std::max(1, want);
     a.bar_base = E->bar_base;
     void* params[] = {&a};
+    ++E->launches;
     CUDA_TRY(cudaLaunchCooperativeKernel((const void*)fn, dim3(blocks), dim3(threads), params, 0, E->stream));
     E->bar_base += (unsigned long long)blocks * std::max(E->max_colors - 1, 0);
     return SCEMC_OK;
@@ -2018,6 +2263,7 @@ int32_t run_pass_impl(scemc_ensemble* E, int pass, const Launch& Lc) {
     if (n == 0) continue;
     a.colour = c;
     const int blocks = (int)std::min<int64_t>(cap, ((int64_t)n * G + threads - 1) / threads);
+    ++E->launches;
     fn<<<std::max(blocks, 1), threads, 0, E->stream>>>(a);
     CUDA_TRY(cudaGetLastError());
   }
@@ -2046,6 +2292,7 @@ int32_t launch_tail(scemc_ensemble* E, bool add_att, bool adapt, double target, 
   t.swaps = E->d_swaps;
   t.exchange_seed = E->exchange_seed;
   t.st = E->d_st;
+  ++E->launches;
   k_tail<<<1, 128, 0, E->stream>>>(t);
   CUDA_TRY(cudaGetLastError());
   return SCEMC_OK;
@@ -2069,14 +2316,17 @@ int32_t recompute(scemc_ensemble* E, int mode) {
     if (mode == 1) {
       const int64_t n = (int64_t)T->n_sites * R;
       const int blocks = (int)std::min<int64_t>(sm_count(E->device) * 4, (n + 255) / 256);
+      ++E->launches;
       k_normalize<<<std::max(blocks, 1), 256, 0, E->stream>>>(E->d_lat, (int)li, E->d_spins);
       CUDA_TRY(cudaGetLastError());
     }
     const int n_chunks = (int)std::max<int64_t>(1, (T->n_inst + kChunk - 1) / kChunk);
     int32_t rc;
     if ((rc = ensure_partial(E, (size_t)n_chunks * R))) return rc;
+    ++E->launches;
     k_energy_chunks<<<dim3(n_chunks, R), 256, 0, E->stream>>>(E->d_lat, (int)li, E->d_spins, E->d_partial, n_chunks);
     CUDA_TRY(cudaGetLastError());
+    ++E->launches;
     k_energy_fold<<<1, 512, 0, E->stream>>>(E->d_lat, (int)li, E->d_partial, n_chunks, E->d_energy, E->d_eout,
                                             E->d_drift, E->d_max_drift, E->d_rung_of_slot, mode);
     CUDA_TRY(cudaGetLastError());
@@ -2110,9 +2360,11 @@ int32_t measure(scemc_ensemble* E) {
     const int n_chunks = (T->n_sites + kChunk - 1) / kChunk;
     const int rlen = 3 + 3 * T->n_cell_atoms;
     if ((rc = ensure_partial(E, (size_t)n_chunks * R * rlen))) return rc;
+    ++E->launches;
     k_measure_chunks<<<dim3(n_chunks, R), 256, 0, E->stream>>>(E->d_lat, (int)li, E->d_spins, E->d_partial, n_chunks,
                                                                rlen);
     CUDA_TRY(cudaGetLastError());
+    ++E->launches;
     k_measure_fold<<<R, 128, 0, E->stream>>>(E->d_lat, (int)li, E->d_partial, n_chunks, rlen, E->d_energy,
                                              E->d_rung_of_slot, row, E->rec_len);
     CUDA_TRY(cudaGetLastError());
@@ -2146,33 +2398,46 @@ int auto_lanes(const scemc_ensemble* E) {
   return G;
 }
 
-// kernel: 0 auto, 1 generic, 2 fast; proposals: 0 auto, 1 precompute, 2 inline.
+// kernel: 0 auto, 1 generic, 2 row-parallel fast, 3 replica-parallel; proposals: 0 auto,
+// 1 precompute, 2 inline.
 int32_t resolve_launch(const scemc_ensemble* E, int lanes, int mode, int kernel, int proposals, Launch* out) {
   Launch L;
-  if (mode == 0 && E->tuned) {
+  if (mode == 0 && kernel == 0 && E->tuned) {
     mode = E->tuned_mode;
+    kernel = E->tuned_kernel;
     if (proposals == 0) proposals = E->tuned_proposals;
     if (lanes == 0) lanes = E->tuned_lanes;
   }
-  L.mode = mode == 0 ? 2 : mode;
-  if (L.mode < 1 || L.mode > 3) return fail(SCEMC_ERR_ARG, "mode must be 0..3");
+  if (mode < 0 || mode > 3) return fail(SCEMC_ERR_ARG, "mode must be 0..3");
+  if (kernel < 0 || kernel > 3 || proposals < 0 || proposals > 2)
+    return fail(SCEMC_ERR_ARG, "kernel must be 0..3 and proposals 0, 1 or 2");
+  bool generic_ok = true;
+  for (const scemc_tables* T : E->tabs) generic_ok = generic_ok && T->has_generic;
+  if ((kernel == 2 || kernel == 3) && !E->fast)
+    return fail(SCEMC_ERR_ARG, "the fast and replica-parallel kernels need lmax 1 or 2 and dense l in {1,2} "
+                               "programs of body <= 4 (l = 1 only for bodies 3 and 4), equal lmax across the batch");
+  if (kernel == 1 && !generic_ok) return fail(SCEMC_ERR_ARG, "generic records were not kept for these tables");
+  if (kernel == 3 && mode == 2)
+    return fail(SCEMC_ERR_ARG, "the replica-parallel kernel runs per-colour launches (mode 1 or 3)");
+  // untuned auto choice: one thread per item once a colour's items fill every SM
+  // and warps hold (mostly) one site's replicas
+  int min_r = 1 << 30;
+  for (int r : E->R) min_r = std::min(min_r, r);
+  const bool rep_auto = E->fast && mode != 2 && min_r >= 16 &&
+                        (int64_t)max_colour_items(E) >= (int64_t)sm_count(E->device) * 2048;
+  L.rep = kernel == 3 || (kernel == 0 && rep_auto);
+  L.fast = !L.rep && (kernel == 2 || (kernel == 0 && E->fast));
+  L.mode = mode == 0 ? (L.rep ? 1 : 2) : mode;
   if (L.mode == 3) {
     L.graph = true;
     L.mode = 1;
   }
-  if (kernel < 0 || kernel > 2 || proposals < 0 || proposals > 2)
-    return fail(SCEMC_ERR_ARG, "kernel and proposals must be 0, 1 or 2");
-  bool generic_ok = true;
-  for (const scemc_tables* T : E->tabs) generic_ok = generic_ok && T->has_generic;
-  if (kernel == 2 && !E->fast)
-    return fail(SCEMC_ERR_ARG, "the fast kernel needs lmax 1 or 2 and dense l in {1,2} programs of body <= 4 "
-                               "(l = 1 only for bodies 3 and 4), equal lmax across the batch");
-  if (kernel == 1 && !generic_ok) return fail(SCEMC_ERR_ARG, "generic records were not kept for these tables");
-  L.fast = kernel == 2 || (kernel == 0 && E->fast);
   L.G = lanes ? norm_lanes(lanes) : auto_lanes(E);
   if (L.fast) {
     const int64_t groups = (int64_t)max_colour_items(E) * 32;
     L.precompute = proposals == 1 || (proposals == 0 && groups < (int64_t)sm_count(E->device) * 2048);
+  } else if (L.rep) {
+    L.precompute = proposals == 1;
   }
   *out = L;
   return SCEMC_OK;
@@ -2191,15 +2456,17 @@ int32_t sweep_once(scemc_ensemble* E, int n_or, const Launch& L) {
 // The passes and tail of one compound sweep as a CUDA graph (captured once per
 // configuration, replayed every sweep). Every launch reads the sweep counter from
 // device memory and the tail advances it, so one capture serves all sweeps.
-int32_t sweep_graph(scemc_ensemble* E, int n_or, const Launch& L, cudaGraphExec_t* out) {
-  const int key[5] = {n_or, L.fast ? 1 : 0, L.precompute ? 1 : 0, L.fast ? 0 : L.G, E->recording ? 1 : 0};
+int32_t sweep_graph(scemc_ensemble* E, int n_or, const Launch& L, cudaGraphExec_t* out, int64_t* n_launch) {
+  const int key[5] = {n_or, L.rep ? 2 : (L.fast ? 1 : 0), L.precompute ? 1 : 0, (L.fast || L.rep) ? 0 : L.G,
+                      E->recording ? 1 : 0};
   for (auto& g : E->graphs)
     if (std::equal(key, key + 5, g.key)) {
       *out = g.exec;
+      *n_launch = g.launches;
       return SCEMC_OK;
     }
   int32_t rc;
-  if (L.fast && L.precompute)
+  if ((L.fast || L.rep) && L.precompute)
     if ((rc = ensure_props(E))) return rc;
   if (L.fast) {  // attributes are set outside the capture
     int threads;
@@ -2210,12 +2477,15 @@ int32_t sweep_graph(scemc_ensemble* E, int n_or, const Launch& L, cudaGraphExec_
   }
   const bool prof = E->profiling;
   E->profiling = false;  // graph launches are timed as a whole
+  const int64_t launches0 = E->launches;
   CUDA_TRY(cudaStreamBeginCapture(E->stream, cudaStreamCaptureModeThreadLocal));
   rc = sweep_once(E, n_or, L);
   if (!rc) rc = launch_tail(E, true, false, 0.5, false, true);
   cudaGraph_t graph = nullptr;
   const cudaError_t ce = cudaStreamEndCapture(E->stream, &graph);
   E->profiling = prof;
+  const int64_t captured = E->launches - launches0;
+  E->launches = launches0;  // captured, not yet run
   if (rc) {
     if (graph) cudaGraphDestroy(graph);
     return rc;
@@ -2228,8 +2498,10 @@ int32_t sweep_graph(scemc_ensemble* E, int n_or, const Launch& L, cudaGraphExec_
   scemc_ensemble::GraphEntry g;
   std::copy(key, key + 5, g.key);
   g.exec = exec;
+  g.launches = captured;
   E->graphs.push_back(g);
   *out = exec;
+  *n_launch = captured;
   return SCEMC_OK;
 }
 
@@ -2483,8 +2755,9 @@ int32_t scemc_batch_run_async(scemc_batch* b, const scemc_run_params* p) {
   if (b->sweep_index + p->nsweeps >= 0x7ffffffell - 1)
     return fail(SCEMC_ERR_EXHAUSTED, "sweep_index would exhaust the 32-bit RNG counter word");
   cudaGraphExec_t exec = nullptr;
+  int64_t graph_launches = 0;
   if (L.graph) {
-    if ((rc = sweep_graph(b, p->or_per_metropolis, L, &exec))) return rc;
+    if ((rc = sweep_graph(b, p->or_per_metropolis, L, &exec, &graph_launches))) return rc;
   }
   for (int64_t k = 1; k <= p->nsweeps; ++k) {
     const int64_t i = p->phase_done + k;
@@ -2498,6 +2771,7 @@ int32_t scemc_batch_run_async(scemc_batch* b, const scemc_run_params* p) {
         CUDA_TRY(cudaEventRecord(e0, b->stream));
       }
       CUDA_TRY(cudaGraphLaunch(exec, b->stream));
+      b->launches += graph_launches;
       if (b->profiling) {
         CUDA_TRY(cudaEventRecord(e1, b->stream));
         b->ev_pending.emplace_back(e0, e1);
@@ -2521,18 +2795,19 @@ int32_t scemc_batch_run_async(scemc_batch* b, const scemc_run_params* p) {
 }
 
 int32_t scemc_batch_autotune(scemc_batch* b, int32_t or_per_metropolis, int32_t sweeps_per_trial, int32_t* mode,
-                             int32_t* proposals, int32_t* lanes, double* ms_per_sweep) {
+                             int32_t* proposals, int32_t* lanes, int32_t* kernel, double* ms_per_sweep) {
   if (!b || or_per_metropolis < 0 || sweeps_per_trial < 1) return fail(SCEMC_ERR_ARG, "bad autotune arguments");
   struct Cand {
-    int mode, proposals, lanes;
+    int mode, proposals, lanes, kernel;
   };
   std::vector<Cand> cands;
   if (b->fast) {
     for (int m : {2, 3})
-      for (int q : {1, 2}) cands.push_back({m, q, 0});
+      for (int q : {1, 2}) cands.push_back({m, q, 0, 2});
+    for (int q : {1, 2}) cands.push_back({3, q, 0, 3});
   } else {
     for (int m : {2, 3})
-      for (int g : {1, 4, 8, 32}) cands.push_back({m, 0, g});
+      for (int g : {1, 4, 8, 32}) cands.push_back({m, 0, g, 1});
   }
   const bool prof = b->profiling;
   b->profiling = false;
@@ -2550,6 +2825,7 @@ int32_t scemc_batch_autotune(scemc_batch* b, int32_t or_per_metropolis, int32_t 
     p.mode = c.mode;
     p.proposals = c.proposals;
     p.lanes_per_site = c.lanes;
+    p.kernel = c.kernel;
     if ((rc = scemc_batch_run(b, &p))) break;  // warm-up (builds graphs, sets attributes)
     p.nsweeps = sweeps_per_trial;
     cudaEventRecord(e0, b->stream);
@@ -2572,7 +2848,9 @@ int32_t scemc_batch_autotune(scemc_batch* b, int32_t or_per_metropolis, int32_t 
   b->tuned_mode = bc.mode;
   b->tuned_proposals = bc.proposals;
   b->tuned_lanes = bc.lanes;
+  b->tuned_kernel = bc.kernel;
   if (mode) *mode = bc.mode;
+  if (kernel) *kernel = bc.kernel;
   if (proposals) *proposals = bc.proposals;
   if (lanes) *lanes = bc.lanes;
   if (ms_per_sweep) *ms_per_sweep = best;
@@ -2630,6 +2908,12 @@ int32_t scemc_batch_kernel_time(const scemc_batch* b, double* ms, int64_t* passe
   if (!b) return fail(SCEMC_ERR_ARG, "batch is NULL");
   if (ms) *ms = b->prof_ms;
   if (passes) *passes = b->prof_passes;
+  return SCEMC_OK;
+}
+
+int32_t scemc_batch_launches(const scemc_batch* b, int64_t* launches) {
+  if (!b || !launches) return fail(SCEMC_ERR_ARG, "NULL argument");
+  *launches = b->launches;
   return SCEMC_OK;
 }
 

@@ -269,11 +269,18 @@ class GPUBatch:
 
     def autotune(self, or_per_metropolis: int = 0, sweeps_per_trial: int = 5):
         """Times the launch forms on this batch (its chains advance) and keeps the
-        fastest for runs with mode=0; returns (mode, proposals, lanes, ms/sweep)."""
-        m, q, g, ms = C.c_int32(), C.c_int32(), C.c_int32(), C.c_double()
+        fastest for runs with mode=0 and kernel=0; returns a dict with the chosen mode,
+        proposals, lanes, kernel and its ms/sweep."""
+        m, q, g, k, ms = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32(), C.c_double()
         check(_lib.lib().scemc_batch_autotune(self.h, int(or_per_metropolis), int(sweeps_per_trial), C.byref(m),
-                                              C.byref(q), C.byref(g), C.byref(ms)))
-        return m.value, q.value, g.value, ms.value
+                                              C.byref(q), C.byref(g), C.byref(k), C.byref(ms)))
+        return {"mode": m.value, "proposals": q.value, "lanes": g.value, "kernel": k.value, "ms_per_sweep": ms.value}
+
+    def launches(self) -> int:
+        """Kernels this batch has enqueued (graph replays count their kernel nodes)."""
+        n = C.c_int64()
+        check(_lib.lib().scemc_batch_launches(self.h, C.byref(n)))
+        return n.value
 
     def kernel_time(self):
         """(summed device ms of the sweep passes, number of passes) since profile(True)."""

@@ -119,8 +119,8 @@ NOT_FAST = {"mixed", "high_l"}  # programs outside the fast kinds (l = 0 / l >= 
 FAST = [m for m in MODELS if m not in NOT_FAST]
 
 # (model, lanes, mode, kernel, proposals): kernel 1 = generic record walk, 0 = auto
-# (the row-parallel fast kernel wherever the model allows it); proposals 1 =
-# precomputed before the colour loop, 2 = inline.
+# (the row-parallel fast kernel wherever the model allows it), 3 = replica-parallel
+# kernel; proposals 1 = precomputed before the colour loop, 2 = inline.
 REPLAY_CASES = [(m, 4, 2, 1, 0) for m in MODELS] + [(m, 0, 2, 0, 1) for m in FAST] + [
     ("biquadratic", 1, 1, 1, 0), ("biquadratic", 32, 1, 1, 0), ("bcc_l2_plaq_zeeman", 1, 2, 1, 0),
     ("bcc_l2_plaq_zeeman", 32, 1, 1, 0), ("high_l", 1, 1, 0, 0), ("mixed", 32, 2, 0, 0),
@@ -129,7 +129,7 @@ REPLAY_CASES = [(m, 4, 2, 1, 0) for m in MODELS] + [(m, 0, 2, 0, 1) for m in FAS
     ("fcc_l2_tri_zeeman", 0, 1, 0, 2), ("threebody", 0, 1, 0, 1), ("chain", 0, 2, 0, 2),
     ("bcc_l2_plaq_zeeman", 0, 3, 0, 1), ("fcc_l2_tri_zeeman", 0, 3, 0, 2), ("biquadratic", 4, 3, 1, 0),
     ("mixed", 8, 3, 0, 0),
-]
+] + [(m, 0, 1, 3, 2) for m in FAST] + [("bcc_l2_plaq_zeeman", 0, 3, 3, 1), ("fcc_l2_tri_zeeman", 0, 3, 3, 2)]
 
 
 @pytest.mark.parametrize("name,lanes,mode,kernel,proposals", REPLAY_CASES,
@@ -169,16 +169,17 @@ def test_fast_kernel_is_launch_shape_independent(gpu):
     H, _ = build("bcc_l2_plaq_zeeman")
     gH = scemc.GPUTiledHamiltonian(H)
     cfg = rand_cfg(H.n_sites, 3)
-    outs = []
-    for mode, prop in [(1, 1), (1, 2), (2, 1), (2, 2), (3, 1), (3, 2)]:
-        b = scemc.GPUBatch([gH], [2], [cfg, cfg], [9, 10], 0.6)
-        b.set_betas([1 / 0.002, 1 / 0.01])
-        b.run(6, or_per_metropolis=1, mode=mode, proposals=prop, kernel=2)
-        st = b.download()
-        outs.append((np.stack(st["configs"]), st["energies"].copy(), st["counters"].copy()))
-    for o in outs[1:]:
-        assert np.array_equal(o[0], outs[0][0]) and np.array_equal(o[1], outs[0][1])
-        assert np.array_equal(o[2], outs[0][2])
+    for kernel, forms in [(2, [(1, 1), (1, 2), (2, 1), (2, 2), (3, 1), (3, 2)]), (3, [(1, 1), (1, 2), (3, 1), (3, 2)])]:
+        outs = []
+        for mode, prop in forms:
+            b = scemc.GPUBatch([gH], [2], [cfg, cfg], [9, 10], 0.6)
+            b.set_betas([1 / 0.002, 1 / 0.01])
+            b.run(6, or_per_metropolis=1, mode=mode, proposals=prop, kernel=kernel)
+            st = b.download()
+            outs.append((np.stack(st["configs"]), st["energies"].copy(), st["counters"].copy()))
+        for o in outs[1:]:
+            assert np.array_equal(o[0], outs[0][0]) and np.array_equal(o[1], outs[0][1])
+            assert np.array_equal(o[2], outs[0][2])
 
 
 def test_autotune_keeps_a_valid_launch_form(gpu):
@@ -186,8 +187,10 @@ def test_autotune_keeps_a_valid_launch_form(gpu):
     gH = scemc.GPUTiledHamiltonian(H)
     b = scemc.GPUBatch([gH], [3], [rand_cfg(H.n_sites, i) for i in range(3)], [1, 2, 3], 0.6)
     b.set_betas([1 / 0.002, 1 / 0.004, 1 / 0.008])
-    mode, prop, lanes, ms = b.autotune(or_per_metropolis=1, sweeps_per_trial=3)
-    assert mode in (2, 3) and prop in (1, 2) and ms > 0
+    t = b.autotune(or_per_metropolis=1, sweeps_per_trial=3)
+    assert t["mode"] in (2, 3) and t["proposals"] in (1, 2) and t["kernel"] in (2, 3) and t["ms_per_sweep"] > 0
+    if t["kernel"] == 3:
+        assert t["mode"] == 3
     before = b.download()["counters"].copy()
     b.run(4, or_per_metropolis=1)  # mode 0 now uses the tuned form
     after = b.download()["counters"]
@@ -203,7 +206,13 @@ def test_fast_kernel_refused_where_it_does_not_apply(gpu):
     b = scemc.GPUBatch([gH], [1], [rand_cfg(H.n_sites, 1)], [1], 0.6)
     with pytest.raises(_lib.ScemcArgumentError):
         b.run(1, kernel=2)
+    with pytest.raises(_lib.ScemcArgumentError):
+        b.run(1, kernel=3)
     b.run(1, kernel=0)  # auto falls back to the generic record walk
+    H2, _ = build("bcc_l2_plaq_zeeman")
+    b2 = scemc.GPUBatch([scemc.GPUTiledHamiltonian(H2)], [1], [rand_cfg(H2.n_sites, 1)], [1], 0.6)
+    with pytest.raises(_lib.ScemcArgumentError):
+        b2.run(1, kernel=3, mode=2)  # the replica-parallel kernel has no persistent form
 
 
 def test_proposal_stream_is_the_reference_stream(gpu):
@@ -481,3 +490,21 @@ def test_pt_energies_match_cpu_run_pt(gpu):
         zs += compare_stats(as_tuple_stats(p.stats), q, ["energy", "absm"], n_sigma=4.0)
     assert sum(z > 2.0 for z in zs) <= 2, zs
     np.testing.assert_allclose(r.swap_acceptance, swaps, atol=0.05)
+
+
+def test_launch_count_matches_the_launch_form(gpu):
+    """scemc_batch_launches counts every kernel the batch enqueues: per compound sweep
+    of per-colour launches, one precompute launch plus one launch per colour and pass
+    plus the tail; a replayed graph adds the same kernel nodes."""
+    H, _ = build("bcc_l2_plaq_zeeman")
+    gH = scemc.GPUTiledHamiltonian(H)
+    b = scemc.GPUBatch([gH], [2], [rand_cfg(H.n_sites, 1), rand_cfg(H.n_sites, 2)], [1, 2], 0.6)
+    per_sweep = 1 + 2 * H.n_colors + 1
+    for kernel, mode in [(2, 1), (2, 3), (3, 1), (3, 3)]:
+        b.run(1, or_per_metropolis=1, mode=mode, kernel=kernel, proposals=1)  # graph capture, if any
+        n0 = b.launches()
+        b.run(3, or_per_metropolis=1, mode=mode, kernel=kernel, proposals=1)
+        assert b.launches() - n0 == 3 * per_sweep, (kernel, mode)
+    n0 = b.launches()
+    b.run(2, or_per_metropolis=1, mode=2, kernel=2, proposals=2)  # one persistent launch per pass + tail
+    assert b.launches() - n0 == 2 * 3
