@@ -1,19 +1,27 @@
 #!/usr/bin/env python
-"""Spin-updates/s of the B200 sweep on the bcc 16^3 multipole workload.
+"""Spin-updates/s of the B200 colour-class sweep.
 
-Workload (the second benchmark configuration): bcc, 2 sublattices, 16^3 cells
-(8192 spins); l = 1 and l = 2 pair products to the 3rd shell (shell means
--1.0/-0.3/-0.1 meV, sigma 0.1 meV per (l m, l' m') entry), l = 1 body-4
-plaquettes N(0, 0.05 meV), Zeeman 2 muB in 1 T || z; 5 temperatures uniform in
-[0.2, 2.0] meV; colour-class Metropolis + 1 overrelaxation pass per sweep, FP32
-dE with FP64 running energies; seed 2. Synthetic, seeded (no fitted model).
+Default workload (the second benchmark configuration, --workload bcc16): bcc,
+2 sublattices, 16^3 cells (8192 spins); l = 1 and l = 2 pair products to the 3rd
+shell (shell means -1.0/-0.3/-0.1 meV, sigma 0.1 meV per (l m, l' m') entry),
+l = 1 body-4 plaquettes N(0, 0.05 meV), Zeeman 2 muB in 1 T || z; 5 temperatures
+uniform in [0.2, 2.0] meV; colour-class Metropolis + 1 overrelaxation pass per
+sweep, FP32 dE with FP64 running energies; seed 2. One step = one compound sweep
+(1 Metropolis + 1 overrelaxation pass) of all 5 chains. The working set (~16 MB)
+fits in L2, so L2 is flushed (a 256 MiB write) before every timed step.
 
-One step = one compound sweep (1 Metropolis + 1 overrelaxation pass) of all 5
-chains. The metric counts attempts on active sites (Metropolis + overrelaxation)
-per second, summed over chains and GPUs. The working set (~16 MB) fits in L2, so
-L2 is flushed (a 256 MiB write) before every timed step.
+--workload fcc (the large frustrated configuration): fcc 4-site cell, n^3 cells
+(--fcc-n, default 64: 1,048,576 spins); l <= 2 pairs to shell 4 (N(0, 1 meV),
++0.5 meV isotropic mean on shell 1), NN triangles N(0, 0.1 meV), Zeeman 2 muB in
+0.5 T || [111]; 32 parallel-tempering rungs with kT geometric in [0.05, 2.0] meV.
+One step = one compound sweep (Metropolis + 1 overrelaxation pass) of all 32
+rungs followed by an on-device replica-exchange attempt. The spins alone
+(32 x 1 M x 16 B = 512 MiB) exceed L2, so no flush is needed.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl scemc|reference]
+The metric counts attempts on active sites (Metropolis + overrelaxation) per
+second, summed over chains and GPUs. Synthetic, seeded inputs (no fitted model).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl scemc|reference] [--workload bcc16|fcc]
 
 --impl reference times the FP64 CPU restatement of the reference's
 metropolis_sweep!/overrelaxation_sweep! (oracle/, colour-parallel over all host
@@ -35,7 +43,10 @@ import numpy as np
 ROOT = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-WORKLOAD = "bcc16_l2_plaquette_zeeman_5T_metropolis+OR"
+WORKLOADS = {
+    "bcc16": "bcc16_l2_plaquette_zeeman_5T_metropolis+OR",
+    "fcc": "fcc{n}_l2_tri_zeeman_32rungs_metropolis+OR+exchange",
+}
 
 
 def peaks():
@@ -46,10 +57,14 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def workload():
+def workload(args):
+    """(workload name, Workload, TiledHamiltonian, exchange after every sweep)."""
     from scemc import models
+    if args.workload == "fcc":
+        w = models.config5_fcc(n=args.fcc_n, replicas=32)
+        return WORKLOADS["fcc"].format(n=args.fcc_n), w, w.hamiltonians()[0], True
     w = models.config2_bcc_l2(16)
-    return w, w.hamiltonians()[0]
+    return WORKLOADS["bcc16"], w, w.hamiltonians()[0], False
 
 
 def cpu_model() -> str:
@@ -62,19 +77,21 @@ def cpu_model() -> str:
     return "unknown"
 
 
-def run_cpu_reference(w, H, steps: int, warmup: int, budget_s: float):
-    """Times the oracle's compound sweep (Metropolis + 1 OR) of the 5 chains on all
+def run_cpu_reference(w, H, steps: int, warmup: int, budget_s: float, max_chains: int = 0):
+    """Times the oracle's compound sweep (Metropolis + 1 OR) of the workload's chains
+    (the first max_chains of them when > 0, a bounded sample of a large batch) on all
     host threads; returns (attempts/s, threads, sample description, per-step ms)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
-    OH = O.OracleHamiltonian(2, w.terms, (16, 16, 16), magmoms=w.magmoms, field=w.field)
+    OH = O.OracleHamiltonian(w.n_cell_atoms, w.terms, tuple(w.dims_list[0]), magmoms=w.magmoms, field=w.field)
     threads = max(1, os.cpu_count() or 1)
+    kts = w.kts[:max_chains] if max_chains > 0 else w.kts
     chains = [O.OracleChain(OH, __import__("scemc").models.random_config(H.n_sites, 100 + i), seed=1000 + i)
-              for i in range(len(w.kts))]
+              for i in range(len(kts))]
 
     def step():
         att = 0
-        for ch, kt in zip(chains, w.kts):
+        for ch, kt in zip(chains, kts):
             c0 = ch.get()[3]
             ch.sweeps(1.0 / kt, 1, n_or=w.or_per_metropolis, threads=threads)
             c1 = ch.get()[3]
@@ -91,8 +108,8 @@ def run_cpu_reference(w, H, steps: int, warmup: int, budget_s: float):
         n += 1
         if tot_t > budget_s:
             break
-    sample = (f"{n} compound sweeps (Metropolis + {w.or_per_metropolis} OR) of {len(w.kts)} chains x {H.n_sites} "
-              f"spins, FP64 oracle, {threads} threads, {cpu_model()}")
+    sample = (f"{n} compound sweeps (Metropolis + {w.or_per_metropolis} OR) of {len(kts)} of {len(w.kts)} chains x "
+              f"{H.n_sites} spins, FP64 oracle, {threads} threads, {cpu_model()}")
     return tot_att / tot_t, threads, sample, 1e3 * tot_t / n
 
 
@@ -146,15 +163,21 @@ class ClockSampler:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--steps", type=int, default=None, help="timed steps (default 2000 bcc16, 20 fcc)")
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="scemc", choices=["scemc", "reference"])
-    ap.add_argument("--mode", type=int, default=0, help="0 auto, 1 per-colour launches, 2 persistent")
+    ap.add_argument("--workload", default="bcc16", choices=sorted(WORKLOADS))
+    ap.add_argument("--fcc-n", type=int, default=64, help="cells per edge of the fcc workload")
+    ap.add_argument("--mode", type=int, default=0, help="0 auto, 1 per-colour launches, 2 persistent, 3 graph")
+    ap.add_argument("--kernel", type=int, default=0, help="0 auto, 1 generic, 2 row-parallel, 3 replica-parallel")
     ap.add_argument("--lanes", type=int, default=0, help="lanes per site (0 = autotuned)")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    big = args.workload == "fcc"
+    if args.steps is None:
+        args.steps = 20 if big else 2000
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -163,13 +186,14 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        w, H = workload()
-        steps = max(1, args.steps if args.steps <= 50 else 50)
-        v, threads, sample, ms = run_cpu_reference(w, H, steps, min(args.warmup, 3), args.cpu_budget)
+        name, w, H, _ = workload(args)
+        steps = max(1, min(args.steps, 50))
+        v, threads, sample, ms = run_cpu_reference(w, H, steps, min(args.warmup, 3) if not big else 1,
+                                                   args.cpu_budget, max_chains=1 if big else 0)
         line = {"metric": "spin-updates/s", "value": v, "unit": "attempts/s", "n_gpus": args.gpus,
                 "steps": steps, "warmup": min(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "sites_per_chain": H.n_sites, "chains": len(w.kts)},
+                "config": {"workload": name, "sites_per_chain": H.n_sites, "chains": len(w.kts)},
                 "impl": "reference",
                 "cpu_baseline": {"value": v, "unit": "attempts/s", "cores": threads, "kind": "port",
                                  "sample": sample},
@@ -188,7 +212,7 @@ def main():
         dist_.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = dist_
 
-    w, H = workload()
+    name, w, H, exchange = workload(args)
     gH = scemc.GPUTiledHamiltonian(H)
     d_mean, a_mean, table_bytes = gH.stats()
     R = len(w.kts)
@@ -197,19 +221,23 @@ def main():
     seeds = [int(x) for x in rng.integers(0, 2 ** 63, size=R)]
     batch = scemc.GPUBatch([gH], [R], configs, seeds, 0.6)
     batch.set_betas(1.0 / w.kts)
-    p = scemc.GPUBatch.params(1, or_per_metropolis=w.or_per_metropolis, lanes_per_site=args.lanes, mode=args.mode)
+    n_or = w.or_per_metropolis
+    form = dict(lanes_per_site=args.lanes, mode=args.mode, kernel=args.kernel)
+    # exchange after every sweep: phase_total far ahead so that no sweep is a phase's last
+    xkw = dict(exchange=True, exchange_interval=1, phase_total=1 << 62) if exchange else {}
+    p = scemc.GPUBatch.params(1, or_per_metropolis=n_or, **form, **xkw)
     stream = torch.cuda.ExternalStream(batch.stream())
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    flush = None if big else torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     def one_step():
         batch.run_async(p)
         batch.sync()
 
     tuned = None
-    if args.mode == 0 and args.lanes == 0:  # pick the launch form by timing them on this batch
-        tuned = batch.autotune(or_per_metropolis=w.or_per_metropolis, sweeps_per_trial=10)
+    if args.mode == 0 and args.lanes == 0 and args.kernel == 0:  # pick the launch form by timing them
+        tuned = batch.autotune(or_per_metropolis=n_or, sweeps_per_trial=2 if big else 10)
     # thermalise a little so acceptance rates are representative, then warm up
-    batch.run(200, or_per_metropolis=w.or_per_metropolis, lanes_per_site=args.lanes, mode=args.mode)
+    batch.run(10 if big else 200, or_per_metropolis=n_or, **form)
     for _ in range(args.warmup):
         one_step()
 
@@ -225,7 +253,8 @@ def main():
     torch.cuda.nvtx.range_push("timed_steps")  # lets a profiler select the timed launches
     for _ in range(args.steps):
         with torch.cuda.stream(stream):
-            flush.zero_()
+            if flush is not None:
+                flush.zero_()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
@@ -240,7 +269,8 @@ def main():
         dist.barrier()
     kern_ms, passes = batch.kernel_time()
     batch.profile(False)
-    cnt1 = batch.download()["counters"]
+    st1 = batch.download()
+    cnt1 = st1["counters"]
     launches = batch.launches() - launches0
     att = cnt1 - cnt0
     attempts = int(att[:, 1].sum() + att[:, 3].sum())
@@ -260,30 +290,32 @@ def main():
     hbm, peak_kind = peaks()
     achieved = attempts * B / (kern_ms * 1e-3) / 1e9 if kern_ms > 0 else None
 
-    # end-to-end through the C ABI with host buffers: upload the 5 chains, one
-    # compound sweep, download the 5 chains + energies
-    host_cfg = np.concatenate([c.reshape(-1) for c in batch.download()["configs"]])
-    host_en = batch.download()["energies"].copy()
-    e2e_steps = max(10, min(args.steps, 100))
+    # end-to-end through the C ABI with host buffers: upload every chain's spins and
+    # energy, one step (compound sweep, plus the exchange where the workload has one),
+    # download the full state
+    host_cfg = np.concatenate([c.reshape(-1) for c in st1["configs"]])
+    host_en = st1["energies"].copy()
+    e2e_steps = 3 if big else max(10, min(args.steps, 100))
+    e2e_kw = dict(or_per_metropolis=n_or, **form, **xkw)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    e2e_att = 0
+    d2h = 0
     for _ in range(e2e_steps):
         batch.upload(host_cfg, host_en)
-        batch.run(1, or_per_metropolis=w.or_per_metropolis, lanes_per_site=args.lanes, mode=args.mode)
+        batch.run(1, **e2e_kw)
         st = batch.download()
         host_cfg = np.concatenate([c.reshape(-1) for c in st["configs"]])
         host_en = st["energies"].copy()
+        d2h = sum(np.asarray(v).nbytes for k, v in st.items() if k != "configs") + host_cfg.nbytes
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     per_step_att = attempts / args.steps
     e2e_value = per_step_att * e2e_steps * world / e2e_s
     h2d = host_cfg.nbytes + host_en.nbytes
-    d2h = host_cfg.nbytes + host_en.nbytes + 8 * 4 * R + 8 * 2 * R + 8 * 3 * R + 4 * R
 
     cpu = None
     if rank == 0 and world == 1:
-        v, threads, sample, _ = run_cpu_reference(w, H, 50, 1, args.cpu_budget)
+        v, threads, sample, _ = run_cpu_reference(w, H, 50, 1, args.cpu_budget, max_chains=1 if big else 0)
         cpu = {"value": v, "unit": "attempts/s", "cores": threads, "kind": "port", "sample": sample}
 
     if rank == 0:
@@ -292,10 +324,12 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sites_per_chain": H.n_sites, "chains_per_gpu": R,
-                       "compound_sweep": f"1 Metropolis + {w.or_per_metropolis} OR", "l2": "flushed (256 MiB) before every step",
+            "config": {"workload": name, "sites_per_chain": H.n_sites, "chains_per_gpu": R,
+                       "compound_sweep": f"1 Metropolis + {n_or} OR" + (" + exchange" if exchange else ""),
+                       "l2": ("inputs larger than L2 (spins alone %.0f MiB)" % (R * H.n_sites * 16 / 2 ** 20)) if big
+                       else "flushed (256 MiB) before every step",
                        "lanes_per_site": args.lanes or "auto", "mode": args.mode or "auto",
-                       "autotuned": tuned,
+                       "kernel": args.kernel or "auto", "autotuned": tuned,
                        "d_mean": d_mean, "A_mean": a_mean, "table_bytes": table_bytes,
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",

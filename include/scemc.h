@@ -187,7 +187,8 @@ typedef struct scemc_run_params {
   int32_t kernel;     /* 0 = auto, 1 = generic record walk, 2 = row-parallel fast kernel (one warp per
                          item), 3 = replica-parallel kernel (one thread per item; per-colour launches,
                          mode 1 or 3) */
-  int32_t proposals;  /* 0 = auto, 1 = precompute a pass's Metropolis proposals, 2 = inline */
+  int32_t proposals;  /* 0 = auto, 1 = precompute a pass's Metropolis proposals, 2 = inline, 3 = learned
+                         network (scemc_batch_set_learned; kernels 2 or 3, per-colour modes 1 or 3) */
 } scemc_run_params;
 
 /* Inverse temperatures per rung (n_slots values, table-major like the slots). */
@@ -215,6 +216,46 @@ int32_t scemc_batch_profile(scemc_batch* b, int32_t on);
 int32_t scemc_batch_autotune(scemc_batch* b, int32_t or_per_metropolis, int32_t sweeps_per_trial, int32_t* mode,
                              int32_t* proposals, int32_t* lanes, int32_t* kernel, double* ms_per_sweep);
 int32_t scemc_batch_kernel_time(const scemc_batch* b, double* ms, int64_t* passes);
+/* ---------------------------------------------------------------------------
+ * Learned proposal network (no counterpart in the reference): a per-site MLP
+ * 43 -> 128 -> 128 -> 20 (SiLU; BF16 weights on the tcgen05 tensor cores, FP32
+ * accumulate) whose 20 outputs parameterise a 4-component von Mises-Fisher mixture
+ * on S^2 (per component: logit, raw mean (3), raw concentration c; kappa =
+ * softplus(c) / kT[meV] + 1e-3). Inputs per row: the 14 environment spins (x, y, z)
+ * in the environment table's order, then kT in meV (43 floats).
+ * Parameters travel as one FP32 block of SCEMC_MLP_PARAMS floats: W1 [128][64]
+ * (input columns 43..63 zero), b1 [128], W2 [128][128], b2 [128], W3 [32][128]
+ * (output rows 20..31 zero), b3 [32].
+ * ------------------------------------------------------------------------- */
+#define SCEMC_MLP_PARAMS 28960
+typedef struct scemc_mlp scemc_mlp;
+int32_t scemc_mlp_create(uint64_t seed, scemc_mlp** out);
+int32_t scemc_mlp_destroy(scemc_mlp* m);
+int32_t scemc_mlp_get_params(const scemc_mlp* m, float* params);
+int32_t scemc_mlp_set_params(scemc_mlp* m, const float* params);
+/* out: n x 20 network outputs for the n x 43 inputs x. */
+int32_t scemc_mlp_forward(scemc_mlp* m, const float* x, int64_t n, float* out);
+/* Mean negative log-likelihood of the unit targets y (n x 3) under the mixture and
+ * its gradient (SCEMC_MLP_PARAMS floats); n a multiple of 128; no update. */
+int32_t scemc_mlp_loss_grad(scemc_mlp* m, const float* x, const float* y, int64_t n, double* loss, float* grad);
+/* Adam (beta 0.9 / 0.999) on minibatches of `batch` rows (a multiple of 128), `epochs`
+ * shuffled passes over the n rows; epoch_loss (may be NULL) gets each epoch's mean
+ * minibatch loss. */
+int32_t scemc_mlp_train(scemc_mlp* m, const float* x, const float* y, int64_t n, int32_t batch, int32_t epochs,
+                        double lr, uint64_t seed, double* epoch_loss);
+
+/* Registers a learned proposal network with a batch (m = NULL unregisters). env:
+ * for every table of the batch in order, n_sites x k 0-based site ids, the sites
+ * whose spins (in that order) form a site's network input; k must be 14 and no
+ * environment site may share its site's colour. The network is not copied: it must
+ * outlive the batch's learned runs. Runs with proposals = 3 then draw every
+ * Metropolis proposal from the network's vMF mixture and accept it with
+ * probability min(1, exp(-beta dE) q(e | env) / q(e' | env)). */
+int32_t scemc_batch_set_learned(scemc_batch* b, const scemc_mlp* m, const int32_t* env, int32_t k);
+/* log q(e | env) - log q(e' | env) of the recorded learned Metropolis pass (slot 0
+ * of table 0; n_sites values, 0 where no learned proposal was recorded). */
+int32_t scemc_batch_fetch_record_ratio(const scemc_batch* b, double* lqr);
+
 /* Number of kernels the batch has enqueued on its stream since creation: sweep
  * passes, proposal precompute, tails, recomputes and measurements; a replayed
  * sweep graph adds its kernel nodes. */

@@ -95,6 +95,16 @@ SIGNATURES = [
     ("scemc_batch_profile", C.c_int32, [C.c_void_p, C.c_int32]),
     ("scemc_batch_kernel_time", C.c_int32, [C.c_void_p, F64P, I64P]),
     ("scemc_batch_launches", C.c_int32, [C.c_void_p, I64P]),
+    ("scemc_batch_set_learned", C.c_int32, [C.c_void_p, C.c_void_p, I32P, C.c_int32]),
+    ("scemc_batch_fetch_record_ratio", C.c_int32, [C.c_void_p, F64P]),
+    ("scemc_mlp_create", C.c_int32, [C.c_uint64, C.POINTER(C.c_void_p)]),
+    ("scemc_mlp_destroy", C.c_int32, [C.c_void_p]),
+    ("scemc_mlp_get_params", C.c_int32, [C.c_void_p, F32P]),
+    ("scemc_mlp_set_params", C.c_int32, [C.c_void_p, F32P]),
+    ("scemc_mlp_forward", C.c_int32, [C.c_void_p, F32P, C.c_int64, F32P]),
+    ("scemc_mlp_loss_grad", C.c_int32, [C.c_void_p, F32P, F32P, C.c_int64, F64P, F32P]),
+    ("scemc_mlp_train", C.c_int32, [C.c_void_p, F32P, F32P, C.c_int64, C.c_int32, C.c_int32, C.c_double, C.c_uint64,
+                                    F64P]),
     ("scemc_batch_autotune", C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, I32P, I32P, I32P, I32P, F64P]),
     ("scemc_batch_download", C.c_int32, [C.c_void_p, F64P, F64P, I32P, I64P, I64P, F64P, F64P]),
     ("scemc_batch_reset_counters", C.c_int32, [C.c_void_p]),

@@ -2,10 +2,13 @@
 
 The library is compiled in-tree next to this file so that it travels with the
 repository; it links the CUDA runtime statically, so loading it needs only the
-driver (and no driver at all for the host-only entry points).
+driver (and no driver at all for the host-only entry points). The two
+translation units (the sweep library and the learned-proposal network) compile in
+parallel and link into one shared object.
 """
 from __future__ import annotations
 
+import concurrent.futures as cf
 import os
 import pathlib
 import shutil
@@ -13,16 +16,13 @@ import subprocess
 
 PKG = pathlib.Path(__file__).resolve().parent
 ROOT = PKG.parent
-SRC = PKG / "csrc" / "scemc.cu"
-HDRS = [PKG / "csrc" / "scemc_device.cuh", ROOT / "include" / "scemc.h"]
+SRCS = [PKG / "csrc" / "scemc.cu", PKG / "csrc" / "learned.cu"]
+HDRS = [PKG / "csrc" / "scemc_device.cuh", PKG / "csrc" / "umma.cuh", PKG / "csrc" / "vmf.cuh",
+        PKG / "csrc" / "mlp.h", ROOT / "include" / "scemc.h"]
 LIB = PKG / "libscemc_cuda.so"
 
-NVCC_FLAGS = [
-    "-gencode", "arch=compute_100a,code=sm_100a",
-    "-O3", "-lineinfo", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared", "-cudart", "static",
-    "-diag-suppress", "177",
-]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = [*ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-diag-suppress", "177"]
 
 
 def nvcc() -> str:
@@ -36,22 +36,36 @@ def stale() -> bool:
     if not LIB.exists():
         return True
     t = LIB.stat().st_mtime
-    return any(p.stat().st_mtime > t for p in [SRC, *HDRS])
+    return any(p.stat().st_mtime > t for p in [*SRCS, *HDRS])
 
 
-def build(force: bool = False, verbose: bool = False) -> pathlib.Path:
+def _compile(src: pathlib.Path, obj: pathlib.Path, extra) -> subprocess.CompletedProcess:
+    cmd = [nvcc(), *NVCC_FLAGS, *extra, f"-I{ROOT / 'include'}", "-c", "-o", str(obj), str(src)]
+    return subprocess.run(cmd, capture_output=True, text=True)
+
+
+def build(force: bool = False, verbose: bool = False, extra=(), out: pathlib.Path | None = None) -> pathlib.Path:
     """Compile libscemc_cuda.so if it is missing or older than its sources."""
-    if not force and not stale():
+    out = out or LIB
+    if out == LIB and not force and not stale():
         return LIB
-    tmp = LIB.with_suffix(".so.tmp")
-    cmd = [nvcc(), *NVCC_FLAGS, f"-I{ROOT / 'include'}", "-o", str(tmp), str(SRC)]
-    res = subprocess.run(cmd, capture_output=True, text=True)
-    if res.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)
-    if verbose:
-        print(res.stdout + res.stderr)
-    os.replace(tmp, LIB)
-    return LIB
+    objdir = PKG / "_build"
+    objdir.mkdir(exist_ok=True)
+    objs = [objdir / (s.stem + ".o") for s in SRCS]
+    with cf.ThreadPoolExecutor(len(SRCS)) as ex:
+        res = list(ex.map(lambda so: _compile(so[0], so[1], list(extra)), zip(SRCS, objs)))
+    for r in res:
+        if r.returncode != 0:
+            raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+        if verbose:
+            print(r.stdout + r.stderr)
+    tmp = out.with_suffix(".so.tmp")
+    link = subprocess.run([nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", str(tmp), *map(str, objs)],
+                          capture_output=True, text=True)
+    if link.returncode != 0:
+        raise RuntimeError("link failed:\n" + link.stdout + link.stderr)
+    os.replace(tmp, out)
+    return out
 
 
 if __name__ == "__main__":

@@ -30,6 +30,8 @@
 //     (fixed 1024-instance chunks, fixed-order reduction) and the observables.
 #include "scemc.h"
 #include "scemc_device.cuh"
+#include "mlp.h"
+#include "vmf.cuh"
 
 #include <cuda_runtime.h>
 
@@ -124,6 +126,9 @@ struct DevLattice {
                                  //   record offset, n_pair | n_trip << 8 | n_quad << 16 | n_nb << 24}
   const uint2* frec;             // {kind<<26 | tensor offset, local neighbour indices (8 bits each)}
   const float* ftensor;          // dense blocks, rows padded to the kernel's row count
+  // learned proposal: environment of every site (n_sites x env_k, 0-based), per batch
+  const int32_t* env;
+  int32_t env_k, pad3;
 };
 
 // Grid barrier state (one per ensemble).
@@ -170,6 +175,8 @@ struct SweepArgs {
   const int32_t* item_base;  // max_colors+1: first global item of each colour
   float4* prop;
   double* propu;
+  const double* lqr;  // learned proposals: log q(e | env) - log q(e' | env) per item (null otherwise)
+  double* rec_lqr;
   int32_t dmax, rmax;
 };
 
@@ -663,11 +670,12 @@ __device__ void fast_colour(const SweepArgs& a, int col, unsigned long long* s_d
     // independent loads of the item, issued before the table walk
     const float4 e = load_spin<PERSIST>(sp + (int64_t)s * R + r);
     float4 p4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    double u_pre = 0.0;
+    double u_pre = 0.0, lq = 0.0;
     if (!do_or && a.prop != nullptr) {
       const int idx = a.item_base[col] + item;
       p4 = a.prop[idx];
       u_pre = a.propu[idx];
+      if (a.lqr != nullptr) lq = a.lqr[idx];
     }
     const int n0 = dsc.y, j0 = dsc.z;
     const uint32_t cnt = (uint32_t)dsc.w;
@@ -799,7 +807,13 @@ __device__ void fast_colour(const SweepArgs& a, int col, unsigned long long* s_d
 #pragma unroll
     for (int o = G / 2; o >= 1; o >>= 1) term += __shfl_xor_sync(0xffffffffu, term, o);
     const float dE = attempted ? term : 0.0f;
-    const bool acc_ok = attempted && (dE <= 0.0f || u < exp(-beta * (double)dE));
+    bool acc_ok;
+    if (!do_or && a.lqr != nullptr) {  // Metropolis-Hastings with the learned proposal's density ratio
+      const double la = -beta * (double)dE + lq;
+      acc_ok = la >= 0.0 || u < exp(la);
+    } else {
+      acc_ok = attempted && (dE <= 0.0f || u < exp(-beta * (double)dE));
+    }
     if (lane != 0) continue;
     if (acc_ok) {
       a.spins[L.spin_off + (int64_t)s * R + r] = make_float4(px, py, pz, 0.0f);
@@ -819,12 +833,19 @@ __device__ void fast_colour(const SweepArgs& a, int col, unsigned long long* s_d
       a.rec_u[qq] = u;
       a.rec_dE[qq] = dE;
       a.rec_acc[qq] = (uint8_t)(acc_ok ? 1 : (attempted ? 0 : 2));
+      if (a.rec_lqr != nullptr && !do_or) a.rec_lqr[s] = lq;
     }
   }
 }
 
+#ifdef SCEMC_FAST_MINB
+#define SCEMC_FAST_BOUNDS __launch_bounds__(256, SCEMC_FAST_MINB)
+#else
+#define SCEMC_FAST_BOUNDS __launch_bounds__(256)
+#endif
+
 template <int LMAX>
-__global__ void __launch_bounds__(256) k_fast_colour(SweepArgs a) {
+__global__ void SCEMC_FAST_BOUNDS k_fast_colour(SweepArgs a) {
   extern __shared__ __align__(16) float zsm[];
   __shared__ unsigned long long s_dE[kMaxSlots];
   __shared__ unsigned int s_cnt[3 * kMaxSlots];
@@ -857,39 +878,60 @@ __global__ void __launch_bounds__(256) k_fast_persistent(SweepArgs a) {
 __global__ void __launch_bounds__(256) k_proposals(SweepArgs a) { make_proposals<false>(a); }
 
 // ---------------------------------------------------------------------------
-// Replica-parallel sweep (same tables as the row-parallel kernel). One thread per
-// (site, replica) item; items run replica-fastest, so when a lattice carries 32 or
-// more replicas a warp holds consecutive replicas of one site: every table word
-// (descriptor, record, W block) is a warp-uniform broadcast and each neighbour
-// gather spins[nb * R + r] is one coalesced transaction. Each thread keeps the
-// site's NR coefficients in registers, c_t = sum_j W_j[t, :] . z_j, and forms
-// dE = sum_t c_t (znew_t - zold_t) itself, so no shuffles or shared-memory rows are
-// needed. Built for large replica counts (many PT rungs of one Hamiltonian).
+// Replica-parallel sweep (same tables as the row-parallel kernel). A thread owns P
+// replicas of one site: r = g, g + G, ..., g + (P-1) G with G = ceil(R / P), so the
+// G threads of a site read each neighbour's replicas as contiguous float4 runs.
+// Every coupling word (descriptor, record, W block) a thread loads serves its P
+// replicas: the load's register writeback, not the FMA pipe, bounds a one-replica
+// thread; P = 2 at 80 registers (three 256-thread blocks per SM) measured fastest.
+// Each replica keeps its NR coefficients in registers, c_t = sum_j W_j[t, :] . z_j,
+// and forms
+// dE = sum_t c_t (znew_t - zold_t) itself (no shuffles or shared-memory rows). Built
+// for large replica counts (many PT rungs of one Hamiltonian).
 // ---------------------------------------------------------------------------
-template <int LMAX>
+#ifndef SCEMC_REP_MINB
+#define SCEMC_REP_MINB 3
+#endif
+#ifndef SCEMC_REP_P
+#define SCEMC_REP_P 2
+#endif
+constexpr int kRepP = SCEMC_REP_P;  // replicas per thread
+
+template <int LMAX, int P>
 __device__ void rep_colour(const SweepArgs& a, int col, unsigned long long* s_dE, unsigned int* s_cnt,
                            const float* zsm) {
   constexpr int NR = (LMAX + 1) * (LMAX + 1) - 1;
   const int32_t* seg_c = a.seg + (size_t)col * (a.n_lat + 1);
-  const int n_items = seg_c[a.n_lat];
   const double* p_beta = reinterpret_cast<const double*>(zsm);
   const double* p_step = p_beta + a.n_slots;
   const unsigned long long* p_seed = reinterpret_cast<const unsigned long long*>(p_step + a.n_slots);
   const bool do_or = a.pass >= 0;
+  int n_threads = 0;  // threads of this colour over every lattice (G per site)
+  for (int l = 0; l < a.n_lat; ++l) {
+    const int R = a.lat[l].R;
+    n_threads += (seg_c[l + 1] - seg_c[l]) / R * ((R + P - 1) / P);
+  }
   const int stride = gridDim.x * blockDim.x;
-  for (int item = blockIdx.x * blockDim.x + threadIdx.x; item < n_items; item += stride) {
-    const int li = find_lattice(seg_c, a.n_lat, item);
+  for (int tid = blockIdx.x * blockDim.x + threadIdx.x; tid < n_threads; tid += stride) {
+    int li = 0, base = 0, G = 1, R = 1;
+    for (; li < a.n_lat; ++li) {
+      R = a.lat[li].R;
+      G = (R + P - 1) / P;
+      const int nt = (seg_c[li + 1] - seg_c[li]) / R * G;
+      if (tid < base + nt) break;
+      base += nt;
+    }
     const DevLattice& L = a.lat[li];
-    const int local = item - seg_c[li];
-    const int R = L.R;
-    const int q = local / R;
-    const int r = local - q * R;
+    const int q = (tid - base) / G;
+    const int g = (tid - base) - q * G;
     const int4 dsc = __ldg(L.idesc + __ldg(L.color_ptr + col) + q);
     const int s = dsc.x & 0x3fffffff;
     if (do_or && !(dsc.x & (1 << 30))) continue;  // no l = 1 channel
-    const int slot = L.slot0 + r;
     const float4* __restrict__ sp = a.spins + L.spin_off;
-    const float4 e = __ldg(sp + (int64_t)s * R + r);
+    const int64_t row0 = (int64_t)s * R;
+    bool ok[P];
+#pragma unroll
+    for (int k = 0; k < P; ++k) ok[k] = g + k * G < R;
     const int n0 = dsc.y, j0 = dsc.z;
     const uint32_t cnt = (uint32_t)dsc.w;
     const int n_pair = (int)(cnt & 0xffu), n_trip = (int)((cnt >> 8) & 0xffu), n_quad = (int)((cnt >> 16) & 0xffu);
@@ -897,172 +939,295 @@ __device__ void rep_colour(const SweepArgs& a, int col, unsigned long long* s_dE
     const uint2* __restrict__ fr = L.frec + j0;
     const int32_t* __restrict__ nbl = L.nb_list + n0;
     const float* __restrict__ ft = L.ftensor;
-    float c[NR];
+    // the P replicas' spins of neighbour `loc` (unused replicas read replica g)
+    auto gather = [&](int loc, float4* v) {
+      const float4* b = sp + (int64_t)__ldg(nbl + loc) * R + g;
 #pragma unroll
-    for (int t = 0; t < NR; ++t) c[t] = 0.0f;
+      for (int k = 0; k < P; ++k) v[k] = __ldcg(b + (ok[k] ? k * G : 0));
+    };
+    float c[P][NR];
+#pragma unroll
+    for (int k = 0; k < P; ++k)
+#pragma unroll
+      for (int t = 0; t < NR; ++t) c[k][t] = 0.0f;
     // merged per-neighbour pair blocks: c += W z_nb
-#pragma unroll 2
+#pragma unroll 1
     for (int j = 0; j < n_pair; ++j) {
       const uint2 rec = __ldg(fr + j);
-      const float4 v = __ldcg(sp + (int64_t)__ldg(nbl + (rec.y & 0xffu)) * R + r);
-      float z[NR];
-      zrow_nr<NR>(v.x, v.y, v.z, z);
-      const float4* w4 = reinterpret_cast<const float4*>(ft + (rec.x & kOffMask));
+      float4 v[P];
+      gather((int)(rec.y & 0xffu), v);
+      float z[P][NR];
+#pragma unroll
+      for (int k = 0; k < P; ++k) zrow_nr<NR>(v[k].x, v[k].y, v[k].z, z[k]);
+      const float* w = ft + (rec.x & kOffMask);
       if constexpr (NR == 8) {
+        const float4* w4 = reinterpret_cast<const float4*>(w);
 #pragma unroll
         for (int t = 0; t < 8; ++t) {
           const float4 a0 = __ldg(w4 + 2 * t), a1 = __ldg(w4 + 2 * t + 1);
-          float x = c[t];
-          x = fmaf(a0.x, z[0], x);
-          x = fmaf(a0.y, z[1], x);
-          x = fmaf(a0.z, z[2], x);
-          x = fmaf(a0.w, z[3], x);
-          x = fmaf(a1.x, z[4], x);
-          x = fmaf(a1.y, z[5], x);
-          x = fmaf(a1.z, z[6], x);
-          x = fmaf(a1.w, z[7], x);
-          c[t] = x;
+#pragma unroll
+          for (int k = 0; k < P; ++k) {
+            float x = c[k][t];
+            x = fmaf(a0.x, z[k][0], x);
+            x = fmaf(a0.y, z[k][1], x);
+            x = fmaf(a0.z, z[k][2], x);
+            x = fmaf(a0.w, z[k][3], x);
+            x = fmaf(a1.x, z[k][4], x);
+            x = fmaf(a1.y, z[k][5], x);
+            x = fmaf(a1.z, z[k][6], x);
+            x = fmaf(a1.w, z[k][7], x);
+            c[k][t] = x;
+          }
         }
       } else {
-        const float4 a0 = __ldg(w4), a1 = __ldg(w4 + 1);
-        const float a8 = __ldg(ft + (rec.x & kOffMask) + 8);
-        const float w[9] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a8};
+        const float4 a0 = __ldg(reinterpret_cast<const float4*>(w)), a1 = __ldg(reinterpret_cast<const float4*>(w) + 1);
+        const float a8 = __ldg(w + 8);
+        const float ww[9] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a8};
 #pragma unroll
-        for (int t = 0; t < 3; ++t)
-          c[t] = fmaf(w[3 * t], z[0], fmaf(w[3 * t + 1], z[1], fmaf(w[3 * t + 2], z[2], c[t])));
+        for (int k = 0; k < P; ++k)
+#pragma unroll
+          for (int t = 0; t < 3; ++t)
+            c[k][t] = fmaf(ww[3 * t], z[k][0], fmaf(ww[3 * t + 1], z[k][1], fmaf(ww[3 * t + 2], z[k][2], c[k][t])));
       }
     }
     // l = 1 triplets: c_t += sum_p z1_p sum_q W[t][3p + q] z2_q (rows padded to 12)
+#pragma unroll 1
     for (int j = n_pair; j < n_pair + n_trip; ++j) {
       const uint2 rec = __ldg(fr + j);
-      const float4 v1 = __ldcg(sp + (int64_t)__ldg(nbl + (rec.y & 0xffu)) * R + r);
-      const float4 v2 = __ldcg(sp + (int64_t)__ldg(nbl + ((rec.y >> 8) & 0xffu)) * R + r);
-      float z1[3], z2[3];
-      zrow_l1(v1.x, v1.y, v1.z, z1);
-      zrow_l1(v2.x, v2.y, v2.z, z2);
+      float4 v1[P], v2[P];
+      gather((int)(rec.y & 0xffu), v1);
+      gather((int)((rec.y >> 8) & 0xffu), v2);
+      float z1[P][3], z2[P][3];
+#pragma unroll
+      for (int k = 0; k < P; ++k) {
+        zrow_l1(v1[k].x, v1[k].y, v1[k].z, z1[k]);
+        zrow_l1(v2[k].x, v2[k].y, v2[k].z, z2[k]);
+      }
       const float4* w4 = reinterpret_cast<const float4*>(ft + (rec.x & kOffMask));
 #pragma unroll
       for (int t = 0; t < 3; ++t) {
         const float4 a0 = __ldg(w4 + 3 * t), a1 = __ldg(w4 + 3 * t + 1), a2 = __ldg(w4 + 3 * t + 2);
         const float w[9] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a2.x};
-        float x = c[t];
 #pragma unroll
-        for (int p = 0; p < 3; ++p) {
-          const float u = fmaf(w[p * 3 + 0], z2[0], fmaf(w[p * 3 + 1], z2[1], w[p * 3 + 2] * z2[2]));
-          x = fmaf(z1[p], u, x);
+        for (int k = 0; k < P; ++k) {
+          float x = c[k][t];
+#pragma unroll
+          for (int p = 0; p < 3; ++p) {
+            const float u = fmaf(w[p * 3 + 0], z2[k][0], fmaf(w[p * 3 + 1], z2[k][1], w[p * 3 + 2] * z2[k][2]));
+            x = fmaf(z1[k][p], u, x);
+          }
+          c[k][t] = x;
         }
-        c[t] = x;
       }
     }
     // l = 1 quads (rows padded to 28)
+#pragma unroll 1
     for (int j = n_pair + n_trip; j < n_pair + n_trip + n_quad; ++j) {
       const uint2 rec = __ldg(fr + j);
-      const float4 v1 = __ldcg(sp + (int64_t)__ldg(nbl + (rec.y & 0xffu)) * R + r);
-      const float4 v2 = __ldcg(sp + (int64_t)__ldg(nbl + ((rec.y >> 8) & 0xffu)) * R + r);
-      const float4 v3 = __ldcg(sp + (int64_t)__ldg(nbl + ((rec.y >> 16) & 0xffu)) * R + r);
-      float z1[3], z2[3], z3[3];
-      zrow_l1(v1.x, v1.y, v1.z, z1);
-      zrow_l1(v2.x, v2.y, v2.z, z2);
-      zrow_l1(v3.x, v3.y, v3.z, z3);
+      float z1[P][3], z2[P][3], z3[P][3];
+      {
+        float4 v[P];
+        gather((int)(rec.y & 0xffu), v);
+#pragma unroll
+        for (int k = 0; k < P; ++k) zrow_l1(v[k].x, v[k].y, v[k].z, z1[k]);
+        gather((int)((rec.y >> 8) & 0xffu), v);
+#pragma unroll
+        for (int k = 0; k < P; ++k) zrow_l1(v[k].x, v[k].y, v[k].z, z2[k]);
+        gather((int)((rec.y >> 16) & 0xffu), v);
+#pragma unroll
+        for (int k = 0; k < P; ++k) zrow_l1(v[k].x, v[k].y, v[k].z, z3[k]);
+      }
       const float4* w4 = reinterpret_cast<const float4*>(ft + (rec.x & kOffMask));
 #pragma unroll
       for (int t = 0; t < 3; ++t) {
-        float w[28];
-#pragma unroll
-        for (int k = 0; k < 7; ++k) {
-          const float4 v = __ldg(w4 + 7 * t + k);
-          w[4 * k] = v.x, w[4 * k + 1] = v.y, w[4 * k + 2] = v.z, w[4 * k + 3] = v.w;
-        }
-        float x = c[t];
 #pragma unroll
         for (int p = 0; p < 3; ++p) {
-          float t2 = 0.0f;
+          // W[t][p][qq][:] for qq = 0..2 lives in floats 9p .. 9p + 8 of row t
+          float w[9];
 #pragma unroll
-          for (int qq = 0; qq < 3; ++qq) {
-            const int o = (p * 3 + qq) * 3;
-            const float t3 = fmaf(w[o], z3[0], fmaf(w[o + 1], z3[1], w[o + 2] * z3[2]));
-            t2 = fmaf(z2[qq], t3, t2);
+          for (int m = 0; m < 9; ++m) w[m] = __ldg(reinterpret_cast<const float*>(w4 + 7 * t) + 9 * p + m);
+#pragma unroll
+          for (int k = 0; k < P; ++k) {
+            float t2 = 0.0f;
+#pragma unroll
+            for (int qq = 0; qq < 3; ++qq) {
+              const float t3 = fmaf(w[qq * 3], z3[k][0], fmaf(w[qq * 3 + 1], z3[k][1], w[qq * 3 + 2] * z3[k][2]));
+              t2 = fmaf(z2[k][qq], t3, t2);
+            }
+            c[k][t] = fmaf(z1[k][p], t2, c[k][t]);
           }
-          x = fmaf(z1[p], t2, x);
         }
-        c[t] = x;
       }
     }
     if (n_one) {
       const float* w = ft + (__ldg(fr + n_pair + n_trip + n_quad).x & kOffMask);
 #pragma unroll
-      for (int t = 0; t < NR; ++t) c[t] += __ldg(w + t);
-    }
-    const double beta = p_beta[slot];
-    float px, py, pz;
-    double u;
-    bool attempted = true;
-    if (!do_or) {
-      if (a.prop != nullptr) {
-        const int idx = a.item_base[col] + item;
-        const float4 p4 = a.prop[idx];
-        px = p4.x, py = p4.y, pz = p4.z;
-        u = a.propu[idx];
-      } else {
-        u = keyed_proposal(p_seed[slot], (uint32_t)(s + 1), a.st->sweep + 1u, e.x, e.y, e.z, p_step[slot], px, py, pz);
-      }
-    } else {
-      // reflection about h = (c4, c2, c3) = rows (3, 1, 2)
-      const double h0 = c[2], h1 = c[0], h2 = c[1];
-      const double hn = sqrt((h0 * h0 + h1 * h1) + h2 * h2);
-      if (hn < 1e-12) {
-        attempted = false;
-        px = e.x, py = e.y, pz = e.z;
-      } else {
-        const double a0 = h0 / hn, a1 = h1 / hn, a2 = h2 / hn;
-        const double d2 = 2.0 * (((double)e.x * a0 + (double)e.y * a1) + (double)e.z * a2);
-        const double r0 = d2 * a0 - e.x, r1 = d2 * a1 - e.y, r2 = d2 * a2 - e.z;
-        const double rn = sqrt((r0 * r0 + r1 * r1) + r2 * r2);
-        px = (float)(r0 / rn);
-        py = (float)(r1 / rn);
-        pz = (float)(r2 / rn);
-      }
-      const Blk bk = philox_block(p_seed[slot], (uint32_t)(s + 1), a.st->sweep + 1u, (uint32_t)a.pass, kTagOR);
-      u = philox_uniform(bk.w0, bk.w1);
-    }
-    float zo[NR], zn[NR];
-    zrow_nr<NR>(e.x, e.y, e.z, zo);
-    zrow_nr<NR>(px, py, pz, zn);
-    float term = 0.0f;
+      for (int t = 0; t < NR; ++t) {
+        const float wt = __ldg(w + t);
 #pragma unroll
-    for (int t = 0; t < NR; ++t) term = fmaf(c[t], zn[t] - zo[t], term);
-    const float dE = attempted ? term : 0.0f;
-    const bool acc_ok = attempted && (dE <= 0.0f || u < exp(-beta * (double)dE));
-    if (acc_ok) {
-      a.spins[L.spin_off + (int64_t)s * R + r] = make_float4(px, py, pz, 0.0f);
-      atomicAdd(s_dE + slot, (unsigned long long)llrint((double)dE * kFixScale));
+        for (int k = 0; k < P; ++k) c[k][t] += wt;
+      }
     }
-    if (do_or) {
-      if (attempted) atomicAdd(s_cnt + 3 * slot + 2, 1u);
-      if (acc_ok) atomicAdd(s_cnt + 3 * slot + 1, 1u);
-    } else if (acc_ok) {
-      atomicAdd(s_cnt + 3 * slot + 0, 1u);
-    }
-    if (a.rec_prop != nullptr && li == 0 && r == 0 && a.pass + 1 < kRecPasses) {
-      const int64_t qq = (int64_t)(a.pass + 1) * L.n_sites + s;
-      a.rec_prop[3 * qq + 0] = px;
-      a.rec_prop[3 * qq + 1] = py;
-      a.rec_prop[3 * qq + 2] = pz;
-      a.rec_u[qq] = u;
-      a.rec_dE[qq] = dE;
-      a.rec_acc[qq] = (uint8_t)(acc_ok ? 1 : (attempted ? 0 : 2));
+    // per replica: proposal, dE, decision, write-back
+#pragma unroll
+    for (int k = 0; k < P; ++k) {
+      if (!ok[k]) continue;
+      const int r = g + k * G;
+      const int slot = L.slot0 + r;
+      const float4 e = __ldg(sp + row0 + r);
+      const double beta = p_beta[slot];
+      float px, py, pz;
+      double u, lq = 0.0;
+      bool attempted = true;
+      if (!do_or) {
+        if (a.prop != nullptr) {
+          const int idx = a.item_base[col] + seg_c[li] + q * R + r;
+          const float4 p4 = a.prop[idx];
+          px = p4.x, py = p4.y, pz = p4.z;
+          u = a.propu[idx];
+          if (a.lqr != nullptr) lq = a.lqr[idx];
+        } else {
+          u = keyed_proposal(p_seed[slot], (uint32_t)(s + 1), a.st->sweep + 1u, e.x, e.y, e.z, p_step[slot], px, py,
+                             pz);
+        }
+      } else {
+        // reflection about h = (c4, c2, c3) = rows (3, 1, 2)
+        const double h0 = c[k][2], h1 = c[k][0], h2 = c[k][1];
+        const double hn = sqrt((h0 * h0 + h1 * h1) + h2 * h2);
+        if (hn < 1e-12) {
+          attempted = false;
+          px = e.x, py = e.y, pz = e.z;
+        } else {
+          const double a0 = h0 / hn, a1 = h1 / hn, a2 = h2 / hn;
+          const double d2 = 2.0 * (((double)e.x * a0 + (double)e.y * a1) + (double)e.z * a2);
+          const double r0 = d2 * a0 - e.x, r1 = d2 * a1 - e.y, r2 = d2 * a2 - e.z;
+          const double rn = sqrt((r0 * r0 + r1 * r1) + r2 * r2);
+          px = (float)(r0 / rn);
+          py = (float)(r1 / rn);
+          pz = (float)(r2 / rn);
+        }
+        const Blk bk = philox_block(p_seed[slot], (uint32_t)(s + 1), a.st->sweep + 1u, (uint32_t)a.pass, kTagOR);
+        u = philox_uniform(bk.w0, bk.w1);
+      }
+      float zo[NR], zn[NR];
+      zrow_nr<NR>(e.x, e.y, e.z, zo);
+      zrow_nr<NR>(px, py, pz, zn);
+      float term = 0.0f;
+#pragma unroll
+      for (int t = 0; t < NR; ++t) term = fmaf(c[k][t], zn[t] - zo[t], term);
+      const float dE = attempted ? term : 0.0f;
+      bool acc_ok;
+      if (!do_or && a.lqr != nullptr) {  // Metropolis-Hastings with the learned proposal's density ratio
+        const double la = -beta * (double)dE + lq;
+        acc_ok = la >= 0.0 || u < exp(la);
+      } else {
+        acc_ok = attempted && (dE <= 0.0f || u < exp(-beta * (double)dE));
+      }
+      if (acc_ok) {
+        a.spins[L.spin_off + row0 + r] = make_float4(px, py, pz, 0.0f);
+        atomicAdd(s_dE + slot, (unsigned long long)llrint((double)dE * kFixScale));
+      }
+      if (do_or) {
+        if (attempted) atomicAdd(s_cnt + 3 * slot + 2, 1u);
+        if (acc_ok) atomicAdd(s_cnt + 3 * slot + 1, 1u);
+      } else if (acc_ok) {
+        atomicAdd(s_cnt + 3 * slot + 0, 1u);
+      }
+      if (a.rec_prop != nullptr && li == 0 && r == 0 && a.pass + 1 < kRecPasses) {
+        const int64_t qq = (int64_t)(a.pass + 1) * L.n_sites + s;
+        a.rec_prop[3 * qq + 0] = px;
+        a.rec_prop[3 * qq + 1] = py;
+        a.rec_prop[3 * qq + 2] = pz;
+        a.rec_u[qq] = u;
+        a.rec_dE[qq] = dE;
+        a.rec_acc[qq] = (uint8_t)(acc_ok ? 1 : (attempted ? 0 : 2));
+        if (a.rec_lqr != nullptr && !do_or) a.rec_lqr[s] = lq;
+      }
     }
   }
 }
 
+// ---------------------------------------------------------------------------
+// Learned proposal of one colour: network inputs, then (after the tensor-core MLP)
+// a draw from each item's vMF mixture with its density ratio. Items are numbered as
+// in the sweep kernels (lattice, then site, then replica), row = item.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void item_of(const SweepArgs& a, const int32_t* seg_c, int item, int& li, int& q, int& r) {
+  li = find_lattice(seg_c, a.n_lat, item);
+  const int local = item - seg_c[li];
+  const int R = a.lat[li].R;
+  q = local / R;
+  r = local - q * R;
+}
+
+// kT in meV of a slot, the network's 43rd input and the head's temperature
+__device__ __forceinline__ float slot_kt_mev(const SweepArgs& a, int slot) {
+  return (float)(1.0e3 / a.beta[a.rung_of_slot[slot]]);
+}
+
+__global__ void __launch_bounds__(256) k_learned_rows(SweepArgs a, __nv_bfloat16* X, int64_t M) {
+  const int col = a.colour;
+  const int32_t* seg_c = a.seg + (size_t)col * (a.n_lat + 1);
+  const int n_items = seg_c[a.n_lat];
+  for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < M; row += (int64_t)gridDim.x * blockDim.x) {
+    alignas(16) __nv_bfloat16 x[vmf::kInPad];
+#pragma unroll
+    for (int k = 0; k < vmf::kInPad; ++k) x[k] = __float2bfloat16_rn(0.0f);
+    if (row < n_items) {
+      int li, q, r;
+      item_of(a, seg_c, (int)row, li, q, r);
+      const DevLattice& L = a.lat[li];
+      const int s = L.color_sites[L.color_ptr[col] + q];
+      const float4* sp = a.spins + L.spin_off;
+      const int32_t* env = L.env + (int64_t)s * L.env_k;
+      for (int k = 0; k < 14; ++k) {
+        const float4 v = __ldg(sp + (int64_t)__ldg(env + k) * L.R + r);
+        x[3 * k] = __float2bfloat16_rn(v.x);
+        x[3 * k + 1] = __float2bfloat16_rn(v.y);
+        x[3 * k + 2] = __float2bfloat16_rn(v.z);
+      }
+      x[42] = __float2bfloat16_rn(slot_kt_mev(a, L.slot0 + r));
+    }
+    uint4* dst = reinterpret_cast<uint4*>(X + row * vmf::kInPad);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) dst[k] = reinterpret_cast<const uint4*>(x)[k];
+  }
+}
+
+__global__ void __launch_bounds__(128) k_learned_propose(SweepArgs a, const float* O, double* lqr) {
+  const int col = a.colour;
+  const int32_t* seg_c = a.seg + (size_t)col * (a.n_lat + 1);
+  const int n_items = seg_c[a.n_lat];
+  for (int item = blockIdx.x * blockDim.x + threadIdx.x; item < n_items; item += gridDim.x * blockDim.x) {
+    int li, q, r;
+    item_of(a, seg_c, item, li, q, r);
+    const DevLattice& L = a.lat[li];
+    const int s = L.color_sites[L.color_ptr[col] + q];
+    const int slot = L.slot0 + r;
+    const int rung = a.rung_of_slot[slot];
+    const float4 e = a.spins[L.spin_off + (int64_t)s * L.R + r];
+    vmf::Mix mix;
+    vmf::mixture(O + (int64_t)item * vmf::kOutPad, (double)slot_kt_mev(a, slot), mix);
+    const Blk b0 = philox_block(a.seed[rung], (uint32_t)(s + 1), a.st->sweep + 1u, 0u, kTagLearn);
+    const Blk b1 = philox_block(a.seed[rung], (uint32_t)(s + 1), a.st->sweep + 1u, 1u, kTagLearn);
+    double x[3];
+    vmf::sample(mix, philox_uniform(b0.w0, b0.w1), philox_uniform(b0.w2, b0.w3), philox_uniform(b1.w0, b1.w1), x);
+    const float px = (float)x[0], py = (float)x[1], pz = (float)x[2];
+    const int idx = a.item_base[col] + item;
+    a.prop[idx] = make_float4(px, py, pz, 0.0f);
+    a.propu[idx] = philox_uniform(b1.w2, b1.w3);
+    lqr[idx] = vmf::log_q(mix, e.x, e.y, e.z) - vmf::log_q(mix, px, py, pz);
+  }
+}
+
 template <int LMAX>
-__global__ void __launch_bounds__(256) k_rep_colour(SweepArgs a) {
+__global__ void __launch_bounds__(256, SCEMC_REP_MINB) k_rep_colour(SweepArgs a) {
   extern __shared__ __align__(16) float zsm[];
   __shared__ unsigned long long s_dE[kMaxSlots];
   __shared__ unsigned int s_cnt[3 * kMaxSlots];
   zero_block(a.n_slots, s_dE, s_cnt);
   stage_params(a, zsm);
-  rep_colour<LMAX>(a, a.colour, s_dE, s_cnt, zsm);
+  rep_colour<LMAX, kRepP>(a, a.colour, s_dE, s_cnt, zsm);
   flush_block(a, s_dE, s_cnt);
 }
 
@@ -1304,6 +1469,7 @@ struct scemc_tables {
   DevLattice dl{};
   std::vector<void*> allocs;
   std::vector<int32_t> color_ptr;  // 0-based host copy
+  std::vector<int32_t> site_col_of;  // colour (1-based) of every site, 0 = inactive
   std::vector<uint8_t> active;
   int32_t n_sites = 0, nlm = 0, lmax = 0, n_colors = 0, n_active = 0, n_cell_atoms = 1;
   int64_t n_inst = 0;
@@ -1365,6 +1531,14 @@ struct scemc_ensemble {
   int coop_blocks = 0;  // cached co-resident grid size for the persistent form
   int coop_G = -1;
   float4* h_stage = nullptr;  // pinned host staging of the spins (n_spins float4)
+  // learned proposal (network not owned), per-colour work buffers
+  const scemc_mlp* mlp = nullptr;
+  std::vector<int32_t*> d_env;
+  __nv_bfloat16 *d_lx = nullptr, *d_lh1 = nullptr, *d_lh2 = nullptr;
+  float* d_lo = nullptr;
+  double* d_lqr = nullptr;
+  double* d_rlqr = nullptr;
+  int64_t lcap = 0;
   // row-parallel fast kernel
   bool fast = false;
   int32_t dmax = 0, rmax = 0;
@@ -1400,7 +1574,9 @@ struct scemc_ensemble {
     }
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
     for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
-    void* qs[] = {d_item_base, d_prop, d_propu};
+    void* qs[] = {d_item_base, d_prop, d_propu, d_lx, d_lh1, d_lh2, d_lo, d_lqr, d_rlqr};
+    for (int32_t* p : d_env)
+      if (p) cudaFree(p);
     for (void* p : qs)
       if (p) cudaFree(p);
     void* ps[] = {d_lat,   d_spins, d_seg,  d_energy,       d_dEfix,        d_cnt,       d_win,    d_swaps,
@@ -1817,6 +1993,9 @@ int32_t compile_tables(const scemc_tables_desc* d, scemc_tables* T) {
   T->has_generic = keep_generic;
   T->fast_records = (int64_t)F.frec.size();
   T->color_ptr = cp;
+  T->site_col_of.assign(ns, 0);
+  for (int32_t c = 0; c < d->n_colors; ++c)
+    for (int32_t q = cp[c]; q < cp[c + 1]; ++q) T->site_col_of[d->color_sites[q] - 1] = c + 1;
   T->active = active;
   T->n_sites = ns;
   T->nlm = d->nlm;
@@ -2053,6 +2232,7 @@ SweepArgs make_args(scemc_ensemble* E, int pass) {
     a.rec_u = E->d_ru;
     a.rec_dE = E->d_rdE;
     a.rec_acc = E->d_racc;
+    a.rec_lqr = E->d_rlqr;
   }
   return a;
 }
@@ -2097,6 +2277,7 @@ struct Launch {
   bool fast = false;  // row-parallel fast kernel (one warp per item)
   bool rep = false;   // replica-parallel kernel (one thread per item, per-colour launches)
   bool precompute = false;  // Metropolis proposals computed before the colour loop
+  bool learned = false;     // Metropolis proposals from the learned network, per colour
 };
 
 using FastFn = void (*)(SweepArgs);
@@ -2151,8 +2332,88 @@ int max_colour_items(const scemc_ensemble* E) {
   return m;
 }
 
+int32_t ensure_learned(scemc_ensemble* E, int64_t M) {
+  if (E->lcap >= M) return SCEMC_OK;
+  void* ps[] = {E->d_lx, E->d_lh1, E->d_lh2, E->d_lo};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  E->d_lx = E->d_lh1 = E->d_lh2 = nullptr;
+  E->d_lo = nullptr;
+  E->lcap = 0;
+  int32_t rc;
+  if ((rc = dalloc(&E->d_lx, (size_t)M * vmf::kInPad)) || (rc = dalloc(&E->d_lh1, (size_t)M * vmf::kHid)) ||
+      (rc = dalloc(&E->d_lh2, (size_t)M * vmf::kHid)) || (rc = dalloc(&E->d_lo, (size_t)M * vmf::kOutPad)))
+    return rc;
+  E->lcap = M;
+  return SCEMC_OK;
+}
+
+// Learned Metropolis pass: per colour, the network inputs, the tensor-core MLP, the
+// mixture draws with their density ratios, then the sweep kernel on those proposals.
+int32_t prepare_learned(scemc_ensemble* E) {
+  int32_t rc;
+  if ((rc = ensure_props(E))) return rc;
+  if (!E->d_lqr && (rc = dalloc(&E->d_lqr, (size_t)std::max<int32_t>(E->item_base.back(), 1)))) return rc;
+  return ensure_learned(E, ((int64_t)max_colour_items(E) + 127) / 128 * 128);
+}
+
+int32_t run_learned_pass(scemc_ensemble* E, const Launch& Lc) {
+  SweepArgs a = make_args(E, -1);
+  int32_t rc;
+  if ((rc = prepare_learned(E))) return rc;
+  a.item_base = E->d_item_base;
+  a.prop = E->d_prop;
+  a.propu = E->d_propu;
+  a.dmax = std::max(E->dmax, 1);
+  a.rmax = std::max(E->rmax, 1);
+  const int cap = sm_count(E->device) * 64;
+  for (int c = 0; c < E->max_colors; ++c) {
+    const int n = E->seg[(size_t)c * (E->tabs.size() + 1) + E->tabs.size()];
+    if (n == 0) continue;
+    a.colour = c;
+    const int64_t Mc = ((int64_t)n + 127) / 128 * 128;
+    a.lqr = nullptr;
+    ++E->launches;
+    k_learned_rows<<<(unsigned)std::min<int64_t>(cap, (Mc + 255) / 256), 256, 0, E->stream>>>(a, E->d_lx, Mc);
+    CUDA_TRY(cudaGetLastError());
+    E->launches += 3;
+    if ((rc = scemc_detail::mlp_forward_dev(E->mlp, E->d_lx, Mc, E->d_lh1, E->d_lh2, E->d_lo, E->stream,
+                                            &E->d_gs->error)))
+      return rc;
+    ++E->launches;
+    k_learned_propose<<<(unsigned)std::min<int64_t>(cap, ((int64_t)n + 127) / 128), 128, 0, E->stream>>>(a, E->d_lo,
+                                                                                                      E->d_lqr);
+    CUDA_TRY(cudaGetLastError());
+    a.lqr = E->d_lqr;
+    ++E->launches;
+    if (Lc.rep) {
+      const int threads = 256;
+      const size_t smem = fast_param_floats(E->n_slots) * sizeof(float);
+      int64_t nt = 0;
+      const int32_t* sc = E->seg.data() + (size_t)c * (E->tabs.size() + 1);
+      for (size_t li = 0; li < E->tabs.size(); ++li)
+        nt += (int64_t)(sc[li + 1] - sc[li]) / E->R[li] * ((E->R[li] + kRepP - 1) / kRepP);
+      FastFn fn = E->lmax == 1 ? k_rep_colour<1> : k_rep_colour<2>;
+      CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      fn<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(cap, (nt + threads - 1) / threads)), threads, smem,
+           E->stream>>>(a);
+    } else {
+      int threads;
+      size_t smem;
+      fast_shape(E, &threads, &smem);
+      FastFn fn = fast_kernel(E->lmax, false);
+      CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      const int blocks = (int)std::min<int64_t>(sm_count(E->device) * 16, ((int64_t)n * 32 + threads - 1) / threads);
+      fn<<<std::max(blocks, 1), threads, smem, E->stream>>>(a);
+    }
+    CUDA_TRY(cudaGetLastError());
+  }
+  return SCEMC_OK;
+}
+
 int32_t run_pass_impl(scemc_ensemble* E, int pass, const Launch& Lc) {
   const int lmax = E->lmax;
+  if (Lc.learned && pass < 0) return run_learned_pass(E, Lc);
   SweepArgs a = make_args(E, pass);
   const int max_items = max_colour_items(E);
   if (Lc.rep) {
@@ -2171,11 +2432,16 @@ int32_t run_pass_impl(scemc_ensemble* E, int pass, const Launch& Lc) {
       CUDA_TRY(cudaGetLastError());
     }
     FastFn fn = lmax == 1 ? k_rep_colour<1> : k_rep_colour<2>;
+    CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     for (int c = 0; c < E->max_colors; ++c) {
       const int n = E->seg[(size_t)c * (E->tabs.size() + 1) + E->tabs.size()];
       if (n == 0) continue;
       a.colour = c;
-      const int blocks = (int)std::min<int64_t>(cap, ((int64_t)n + threads - 1) / threads);
+      int64_t nt = 0;  // kRepP replicas per thread
+      const int32_t* sc = E->seg.data() + (size_t)c * (E->tabs.size() + 1);
+      for (size_t li = 0; li < E->tabs.size(); ++li)
+        nt += (int64_t)(sc[li + 1] - sc[li]) / E->R[li] * ((E->R[li] + kRepP - 1) / kRepP);
+      const int blocks = (int)std::min<int64_t>(cap, (nt + threads - 1) / threads);
       ++E->launches;
       fn<<<std::max(blocks, 1), threads, smem, E->stream>>>(a);
       CUDA_TRY(cudaGetLastError());
@@ -2407,10 +2673,17 @@ int32_t resolve_launch(const scemc_ensemble* E, int lanes, int mode, int kernel,
     kernel = E->tuned_kernel;
     if (proposals == 0) proposals = E->tuned_proposals;
     if (lanes == 0) lanes = E->tuned_lanes;
+    if (proposals == 3 && mode == 2) mode = 3;  // learned passes run per colour
   }
   if (mode < 0 || mode > 3) return fail(SCEMC_ERR_ARG, "mode must be 0..3");
-  if (kernel < 0 || kernel > 3 || proposals < 0 || proposals > 2)
-    return fail(SCEMC_ERR_ARG, "kernel must be 0..3 and proposals 0, 1 or 2");
+  if (kernel < 0 || kernel > 3 || proposals < 0 || proposals > 3)
+    return fail(SCEMC_ERR_ARG, "kernel must be 0..3 and proposals 0..3");
+  if (proposals == 3) {
+    if (!E->mlp) return fail(SCEMC_ERR_ARG, "learned proposals need scemc_batch_set_learned first");
+    if (!E->fast) return fail(SCEMC_ERR_ARG, "learned proposals need the fast tables (lmax 1 or 2 dense programs)");
+    if (kernel == 1) return fail(SCEMC_ERR_ARG, "learned proposals run with kernel 2 or 3, not the generic walk");
+    if (mode == 2) return fail(SCEMC_ERR_ARG, "learned proposals run per-colour launches (mode 1 or 3)");
+  }
   bool generic_ok = true;
   for (const scemc_tables* T : E->tabs) generic_ok = generic_ok && T->has_generic;
   if ((kernel == 2 || kernel == 3) && !E->fast)
@@ -2427,13 +2700,16 @@ int32_t resolve_launch(const scemc_ensemble* E, int lanes, int mode, int kernel,
                         (int64_t)max_colour_items(E) >= (int64_t)sm_count(E->device) * 2048;
   L.rep = kernel == 3 || (kernel == 0 && rep_auto);
   L.fast = !L.rep && (kernel == 2 || (kernel == 0 && E->fast));
-  L.mode = mode == 0 ? (L.rep ? 1 : 2) : mode;
+  L.learned = proposals == 3;
+  L.mode = mode == 0 ? ((L.rep || L.learned) ? 1 : 2) : mode;
   if (L.mode == 3) {
     L.graph = true;
     L.mode = 1;
   }
   L.G = lanes ? norm_lanes(lanes) : auto_lanes(E);
-  if (L.fast) {
+  if (L.learned) {
+    L.precompute = false;
+  } else if (L.fast) {
     const int64_t groups = (int64_t)max_colour_items(E) * 32;
     L.precompute = proposals == 1 || (proposals == 0 && groups < (int64_t)sm_count(E->device) * 2048);
   } else if (L.rep) {
@@ -2457,8 +2733,8 @@ int32_t sweep_once(scemc_ensemble* E, int n_or, const Launch& L) {
 // configuration, replayed every sweep). Every launch reads the sweep counter from
 // device memory and the tail advances it, so one capture serves all sweeps.
 int32_t sweep_graph(scemc_ensemble* E, int n_or, const Launch& L, cudaGraphExec_t* out, int64_t* n_launch) {
-  const int key[5] = {n_or, L.rep ? 2 : (L.fast ? 1 : 0), L.precompute ? 1 : 0, (L.fast || L.rep) ? 0 : L.G,
-                      E->recording ? 1 : 0};
+  const int key[5] = {n_or, L.rep ? 2 : (L.fast ? 1 : 0), L.learned ? 2 : (L.precompute ? 1 : 0),
+                      (L.fast || L.rep) ? 0 : L.G, E->recording ? 1 : 0};
   for (auto& g : E->graphs)
     if (std::equal(key, key + 5, g.key)) {
       *out = g.exec;
@@ -2468,11 +2744,18 @@ int32_t sweep_graph(scemc_ensemble* E, int n_or, const Launch& L, cudaGraphExec_
   int32_t rc;
   if ((L.fast || L.rep) && L.precompute)
     if ((rc = ensure_props(E))) return rc;
+  if (L.learned)
+    if ((rc = prepare_learned(E))) return rc;
   if (L.fast) {  // attributes are set outside the capture
     int threads;
     size_t smem;
     fast_shape(E, &threads, &smem);
     CUDA_TRY(cudaFuncSetAttribute((const void*)fast_kernel(E->lmax, false),
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  }
+  if (L.rep) {
+    const size_t smem = fast_param_floats(E->n_slots) * sizeof(float);
+    CUDA_TRY(cudaFuncSetAttribute((const void*)(E->lmax == 1 ? k_rep_colour<1> : k_rep_colour<2>),
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   }
   const bool prof = E->profiling;
@@ -2510,6 +2793,10 @@ int32_t sweep_graph(scemc_ensemble* E, int n_or, const Launch& L, cudaGraphExec_
 // =============================================================================
 // C ABI
 // =============================================================================
+namespace scemc_detail {
+int32_t set_error(int32_t code, const char* msg) { return fail(code, msg); }
+}  // namespace scemc_detail
+
 extern "C" {
 
 int32_t scemc_last_error(char* buf, size_t len) {
@@ -2973,9 +3260,10 @@ int32_t scemc_batch_record(scemc_batch* b, int32_t on) {
   if (b->recording && !b->d_rprop) {
     int32_t rc;
     if ((rc = dalloc(&b->d_rprop, 3 * n)) || (rc = dalloc(&b->d_ru, n)) || (rc = dalloc(&b->d_rdE, n)) ||
-        (rc = dalloc(&b->d_racc, n)))
+        (rc = dalloc(&b->d_racc, n)) || (rc = dalloc(&b->d_rlqr, (size_t)b->tabs[0]->n_sites)))
       return rc;
   }
+  if (b->recording) CUDA_TRY(cudaMemset(b->d_rlqr, 0, sizeof(double) * b->tabs[0]->n_sites));
   if (b->recording) CUDA_TRY(cudaMemset(b->d_racc, 3, n));  // 3 = site not visited
   return SCEMC_OK;
 }
@@ -2989,6 +3277,54 @@ int32_t scemc_batch_fetch_record(const scemc_batch* b, int32_t pass, float* prop
   if (u) CUDA_TRY(cudaMemcpy(u, b->d_ru + o, 8 * n, cudaMemcpyDeviceToHost));
   if (dE) CUDA_TRY(cudaMemcpy(dE, b->d_rdE + o, 4 * n, cudaMemcpyDeviceToHost));
   if (acc) CUDA_TRY(cudaMemcpy(acc, b->d_racc + o, n, cudaMemcpyDeviceToHost));
+  return SCEMC_OK;
+}
+
+int32_t scemc_batch_fetch_record_ratio(const scemc_batch* b, double* lqr) {
+  if (!b || !b->d_rlqr || !lqr) return fail(SCEMC_ERR_ARG, "recording was never enabled");
+  CUDA_TRY(cudaMemcpy(lqr, b->d_rlqr, sizeof(double) * b->tabs[0]->n_sites, cudaMemcpyDeviceToHost));
+  return SCEMC_OK;
+}
+
+int32_t scemc_batch_set_learned(scemc_batch* b, const scemc_mlp* m, const int32_t* env, int32_t k) {
+  if (!b) return fail(SCEMC_ERR_ARG, "batch is NULL");
+  std::vector<DevLattice> lats(b->tabs.size());
+  CUDA_TRY(cudaMemcpy(lats.data(), b->d_lat, sizeof(DevLattice) * lats.size(), cudaMemcpyDeviceToHost));
+  for (int32_t* p : b->d_env)
+    if (p) cudaFree(p);
+  b->d_env.assign(b->tabs.size(), nullptr);
+  b->mlp = nullptr;
+  for (auto& g : b->graphs) cudaGraphExecDestroy(g.exec);
+  b->graphs.clear();
+  if (m) {
+    if (!env) return fail(SCEMC_ERR_ARG, "env is NULL");
+    if (k != 14) return fail(SCEMC_ERR_ARG, "the network reads 14 environment spins (k = 14)");
+    int64_t off = 0;
+    for (size_t i = 0; i < b->tabs.size(); ++i) {
+      const scemc_tables* T = b->tabs[i];
+      const int64_t n = (int64_t)T->n_sites * k;
+      for (int64_t j = 0; j < n; ++j)
+        if (env[off + j] < 0 || env[off + j] >= T->n_sites)
+          return fail(SCEMC_ERR_ARG, "environment site outside 0..n_sites-1 of table " + std::to_string(i));
+      for (int32_t s = 0; s < T->n_sites; ++s)
+        for (int j = 0; j < k; ++j) {
+          const int32_t t = env[off + (int64_t)s * k + j];
+          if (T->site_col_of[s] > 0 && T->site_col_of[s] == T->site_col_of[t])
+            return fail(SCEMC_ERR_ARG, "an environment site shares its site's colour (the proposal would not "
+                                       "be reversible)");
+        }
+      int32_t rc;
+      if ((rc = dalloc(&b->d_env[i], (size_t)n))) return rc;
+      CUDA_TRY(cudaMemcpy(b->d_env[i], env + off, sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+      off += n;
+    }
+    b->mlp = m;
+  }
+  for (size_t i = 0; i < lats.size(); ++i) {
+    lats[i].env = b->d_env[i];
+    lats[i].env_k = m ? k : 0;
+  }
+  CUDA_TRY(cudaMemcpy(b->d_lat, lats.data(), sizeof(DevLattice) * lats.size(), cudaMemcpyHostToDevice));
   return SCEMC_OK;
 }
 

@@ -17,7 +17,7 @@ namespace scemc {
 
 constexpr double kTwoPi = 6.283185307179586;  // src/gpu/philox.jl:18
 constexpr double kFlipFraction = 0.2;         // src/updates.jl:20
-constexpr uint32_t kTagMetro = 0u, kTagOR = 1u, kTagExchange = 3u;
+constexpr uint32_t kTagMetro = 0u, kTagOR = 1u, kTagExchange = 3u, kTagLearn = 4u;
 
 // ---------------------------------------------------------------------------
 // Philox4x32-10 (src/gpu/philox.jl:26-60)

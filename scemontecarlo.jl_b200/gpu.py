@@ -276,6 +276,25 @@ class GPUBatch:
                                               C.byref(q), C.byref(g), C.byref(k), C.byref(ms)))
         return {"mode": m.value, "proposals": q.value, "lanes": g.value, "kernel": k.value, "ms_per_sweep": ms.value}
 
+    def set_learned(self, net, env) -> None:
+        """Registers a learned proposal network (scemc.learned.ProposalNet, or None to
+        unregister) with its environment table (n_sites x 14 per table, 0-based);
+        runs with proposals=3 then use it for every Metropolis proposal."""
+        if net is None:
+            check(_lib.lib().scemc_batch_set_learned(self.h, None, None, 14))
+            self._net = None
+            return
+        env = np.ascontiguousarray(np.concatenate([np.asarray(e, np.int32).reshape(-1) for e in
+                                                   (env if isinstance(env, (list, tuple)) else [env])]), np.int32)
+        check(_lib.lib().scemc_batch_set_learned(self.h, net.h, ptr(env, C.c_int32), 14))
+        self._net = net  # the batch does not own the network: keep it alive
+
+    def fetch_record_ratio(self) -> np.ndarray:
+        """log q(e|env) - log q(e'|env) of the recorded learned Metropolis pass."""
+        out = np.zeros(self.gHs[0].n_sites)
+        check(_lib.lib().scemc_batch_fetch_record_ratio(self.h, ptr(out, C.c_double)))
+        return out
+
     def launches(self) -> int:
         """Kernels this batch has enqueued (graph replays count their kernel nodes)."""
         n = C.c_int64()

@@ -1,0 +1,142 @@
+"""Learned proposal: the per-site network, its training data and the environment
+table (no counterpart in the reference; the acceptance it feeds is the
+reference's Metropolis test of src/updates.jl:37-64 with the Hastings factor
+q(e | env) / q(e' | env), so the stationary distribution is unchanged).
+
+The network (43 -> 128 -> 128 -> 20, SiLU) and its training run in
+libscemc_cuda.so on the tcgen05 tensor cores; this module is the host side.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import itertools
+
+import numpy as np
+
+from . import _lib
+from ._lib import F32P, F64P, check, ptr
+
+N_PARAMS = 28960
+N_IN, N_OUT = 43, 20
+MEV = 1e-3
+
+# (name, offset, shape) of the parameter block
+LAYOUT = [("W1", 0, (128, 64)), ("b1", 8192, (128,)), ("W2", 8320, (128, 128)), ("b2", 24704, (128,)),
+          ("W3", 24832, (32, 128)), ("b3", 28928, (32,))]
+
+
+def unpack(flat: np.ndarray) -> dict:
+    return {n: flat[o:o + int(np.prod(s))].reshape(s) for n, o, s in LAYOUT}
+
+
+def pack(P: dict) -> np.ndarray:
+    flat = np.zeros(N_PARAMS, np.float32)
+    for n, o, s in LAYOUT:
+        flat[o:o + int(np.prod(s))] = np.asarray(P[n], np.float32).reshape(-1)
+    return flat
+
+
+class ProposalNet:
+    """The learned proposal network (device resident)."""
+
+    def __init__(self, seed: int = 0):
+        h = C.c_void_p()
+        check(_lib.lib().scemc_mlp_create(int(seed) & (2 ** 64 - 1), C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            _lib.lib().scemc_mlp_destroy(self.h)
+            self.h = None
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(N_PARAMS, np.float32)
+        check(_lib.lib().scemc_mlp_get_params(self.h, ptr(out, C.c_float)))
+        return out
+
+    def set_params(self, flat) -> None:
+        flat = np.ascontiguousarray(flat, np.float32)
+        if flat.size != N_PARAMS:
+            raise ValueError(f"expected {N_PARAMS} parameters")
+        check(_lib.lib().scemc_mlp_set_params(self.h, ptr(flat, C.c_float)))
+
+    def forward(self, X) -> np.ndarray:
+        X = np.ascontiguousarray(X, np.float32)
+        n = X.shape[0]
+        out = np.zeros((n, N_OUT), np.float32)
+        check(_lib.lib().scemc_mlp_forward(self.h, ptr(X, C.c_float), n, ptr(out, C.c_float)))
+        return out
+
+    def loss_grad(self, X, Y):
+        X = np.ascontiguousarray(X, np.float32)
+        Y = np.ascontiguousarray(Y, np.float32)
+        loss = C.c_double()
+        g = np.zeros(N_PARAMS, np.float32)
+        check(_lib.lib().scemc_mlp_loss_grad(self.h, ptr(X, C.c_float), ptr(Y, C.c_float), X.shape[0],
+                                             C.byref(loss), ptr(g, C.c_float)))
+        return loss.value, g
+
+    def train(self, X, Y, batch: int = 1024, epochs: int = 10, lr: float = 1e-3, seed: int = 0) -> np.ndarray:
+        """Adam on shuffled minibatches; returns each epoch's mean minibatch loss."""
+        X = np.ascontiguousarray(X, np.float32)
+        Y = np.ascontiguousarray(Y, np.float32)
+        losses = np.zeros(max(epochs, 1))
+        check(_lib.lib().scemc_mlp_train(self.h, ptr(X, C.c_float), ptr(Y, C.c_float), X.shape[0], int(batch),
+                                         int(epochs), float(lr), int(seed) & (2 ** 64 - 1), ptr(losses, C.c_double)))
+        return losses[:epochs]
+
+
+def environment_table(positions: np.ndarray, dims, n_shells: int = 2, tol: float = 1e-6) -> np.ndarray:
+    """Canonical environment of every site: the sites of the first `n_shells`
+    neighbour shells, ordered by displacement vector (lexicographic in x, y, z).
+    positions: fractional atom positions of the cubic cell (n_atoms, 3); site
+    numbering as TiledHamiltonian.site_index (0-based here). Returns (n_sites, K)
+    int32."""
+    pos = np.asarray(positions, float)
+    na = pos.shape[0]
+    d1, d2, d3 = (int(x) for x in dims)
+    # displacement list per atom: all (atom b, cell offset) within the shell radii
+    cands = []
+    for a in range(na):
+        lst = []
+        for off in itertools.product(range(-2, 3), repeat=3):
+            for b in range(na):
+                v = pos[b] + np.asarray(off) - pos[a]
+                r = float(np.linalg.norm(v))
+                if r > tol:
+                    lst.append((r, tuple(np.round(v, 9)), b, off))
+        cands.append(lst)
+    radii = sorted({round(c[0], 6) for c in cands[0]})[:n_shells]
+    rmax = radii[-1] + tol
+    per_atom = []
+    for a in range(na):
+        sel = sorted([c for c in cands[a] if c[0] <= rmax], key=lambda c: c[1])
+        per_atom.append(sel)
+    K = len(per_atom[0])
+    if any(len(p) != K for p in per_atom):
+        raise ValueError("sublattices have different environment sizes")
+    n_sites = na * d1 * d2 * d3
+    env = np.zeros((n_sites, K), np.int32)
+    for c2 in range(d3):
+        for c1 in range(d2):
+            for c0 in range(d1):
+                for a in range(na):
+                    s = a + na * (c0 + d1 * (c1 + d2 * c2))
+                    for k, (_, _, b, off) in enumerate(per_atom[a]):
+                        t0 = (c0 + off[0]) % d1
+                        t1 = (c1 + off[1]) % d2
+                        t2 = (c2 + off[2]) % d3
+                        env[s, k] = b + na * (t0 + d1 * (t1 + d2 * t2))
+    return env
+
+
+def environment_rows(configs, env: np.ndarray, kts_ev, sites=None) -> np.ndarray:
+    """Network inputs (n, 43) for the given sites of each configuration: the
+    environment spins in table order, then kT in meV."""
+    rows = []
+    for cfg, kt in zip(configs, kts_ev):
+        cfg = np.asarray(cfg).reshape(-1, 3)
+        ss = np.arange(cfg.shape[0]) if sites is None else np.asarray(sites)
+        x = cfg[env[ss]].reshape(len(ss), -1)
+        rows.append(np.concatenate([x, np.full((len(ss), 1), kt / MEV)], axis=1))
+    return np.concatenate(rows).astype(np.float32)
