@@ -21,7 +21,17 @@ rungs followed by an on-device replica-exchange attempt. The spins alone
 The metric counts attempts on active sites (Metropolis + overrelaxation) per
 second, summed over chains and GPUs. Synthetic, seeded inputs (no fitted model).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl scemc|reference] [--workload bcc16|fcc]
+--workload learned (the learned-proposal configuration): bcc 32^3 (65,536 spins),
+J1 = -1.0 / J2 = -0.2 meV isotropic l = 1 plus l = 1 body-4 plaquettes N(0, 0.05 meV),
+16 chains at kT geometric in [0.2, 2.0] meV. The network is trained on 200k site
+environments from plain-Metropolis chains at the 16 kT values; then the plain
+(adaptive-step) and the learned (Metropolis-Hastings) samplers each run 2000
+thermalisation and --steps measurement sweeps (default 10000) of the 16 chains. The
+metric is tau_int-corrected independent samples per second, ESS/s = sum over
+chains of n_meas / (1 + 2 max(tau_int(E), tau_int(|m|))) over the measurement wall
+time; the line reports the learned value with the plain one and their ratio.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl scemc|reference] [--workload bcc16|fcc|learned]
 
 --impl reference times the FP64 CPU restatement of the reference's
 metropolis_sweep!/overrelaxation_sweep! (oracle/, colour-parallel over all host
@@ -46,6 +56,7 @@ sys.path.insert(0, str(ROOT))
 WORKLOADS = {
     "bcc16": "bcc16_l2_plaquette_zeeman_5T_metropolis+OR",
     "fcc": "fcc{n}_l2_tri_zeeman_32rungs_metropolis+OR+exchange",
+    "learned": "bcc32_J1J2_body4_16T_learned_vs_plain",
 }
 
 
@@ -75,6 +86,52 @@ def cpu_model() -> str:
     except OSError:
         pass
     return "unknown"
+
+
+def run_learned(args) -> int:
+    """The learned-vs-plain tau_int-corrected samples/s on the bcc 32^3 body-4 model."""
+    import torch
+    import scemc
+    from scemc import learned, models
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    n = 32
+    w = models.config4_bcc_body4(n)
+    H = w.hamiltonians()[0]
+    gH = scemc.GPUTiledHamiltonian(H)
+    env = learned.environment_table(models.BCC.positions, (n, n, n))
+    t0 = time.perf_counter()
+    X, Y = learned.collect_training_set(gH, env, w.kts, 200_000, sweeps_therm=2000, snapshots=4, spacing=50, seed=4)
+    t1 = time.perf_counter()
+    net = learned.ProposalNet(seed=4)
+    losses = net.train(X, Y, batch=1024, epochs=20, lr=1e-3, seed=4)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    measure = args.steps
+    kw = dict(kT=w.kts, exchange=False, sweeps_therm=2000, sweeps_measure=measure, seed=4, kernel=args.kernel)
+    plain = scemc.gpu_run_pt(gH, **kw)
+    lrn = scemc.gpu_run_pt(gH, learned=(net, env), proposals=3, **kw)
+    ess_p, _, tau_p = learned.ess_per_second(plain)
+    ess_l, _, tau_l = learned.ess_per_second(lrn)
+    ms = 1e3 * lrn.extra["measure_s"] / measure
+    line = {"metric": "tau_int-corrected samples/s", "value": ess_l, "unit": "samples/s", "n_gpus": 1,
+            "steps": measure, "warmup": 2000, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 dE, bf16 network", "data": "synthetic",
+            "config": {"workload": WORKLOADS["learned"], "sites_per_chain": H.n_sites, "chains": len(w.kts),
+                       "step": "one sweep of every chain (Metropolis or learned Metropolis-Hastings)",
+                       "kernel": args.kernel or "auto",
+                       "plain_ess_per_s": ess_p, "learned_over_plain": ess_l / ess_p,
+                       "tau_max_plain": tau_p.tolist(), "tau_max_learned": tau_l.tolist(),
+                       "acceptance_plain": [p.acceptance_metropolis for p in plain.points],
+                       "acceptance_learned": [p.acceptance_metropolis for p in lrn.points],
+                       "plain_ms_per_sweep": 1e3 * plain.extra["measure_s"] / measure,
+                       "training_rows": int(X.shape[0]), "collect_s": t1 - t0, "train_s": t2 - t1,
+                       "train_loss_first_last": [float(losses[0]), float(losses[-1])],
+                       "energy_plain": [float(p.stats["energy"].mean[0]) for p in plain.points],
+                       "energy_learned": [float(p.stats["energy"].mean[0]) for p in lrn.points],
+                       "energy_err_plain": [float(p.stats["energy"].err[0]) for p in plain.points],
+                       "energy_err_learned": [float(p.stats["energy"].err[0]) for p in lrn.points]}}
+    print(json.dumps(line))
+    return 0
 
 
 def run_cpu_reference(w, H, steps: int, warmup: int, budget_s: float, max_chains: int = 0):
@@ -177,7 +234,13 @@ def main():
         ap.error("--warmup must be >= 3")
     big = args.workload == "fcc"
     if args.steps is None:
-        args.steps = 20 if big else 2000
+        args.steps = {"fcc": 20, "learned": 10000}.get(args.workload, 2000)
+    if args.workload == "learned":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned proposal; "
+                              "its plain sampler is the plain arm inside this workload's line"}))
+            return 0
+        return run_learned(args)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -203,6 +266,7 @@ def main():
 
     import torch
     import scemc
+    from scemc import ranks
 
     torch.cuda.set_device(local)
     dist = None
@@ -218,7 +282,7 @@ def main():
     R = len(w.kts)
     rng = np.random.default_rng(2 + 1000 * rank)
     configs = [models_random(H.n_sites, rng) for _ in range(R)]
-    seeds = [int(x) for x in rng.integers(0, 2 ** 63, size=R)]
+    seeds = ranks.rank_keys(2, rank, R)
     batch = scemc.GPUBatch([gH], [R], configs, seeds, 0.6)
     batch.set_betas(1.0 / w.kts)
     n_or = w.or_per_metropolis
@@ -275,13 +339,7 @@ def main():
     att = cnt1 - cnt0
     attempts = int(att[:, 1].sum() + att[:, 3].sum())
     total_ms = float(np.sum(step_ms))
-    t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-    a = torch.tensor([attempts], device="cuda", dtype=torch.float64)
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(a, op=dist.ReduceOp.SUM)
-    total_ms_max = float(t.item())
-    attempts_all = float(a.item())
+    total_ms_max, attempts_all = ranks.aggregate(total_ms, attempts, dist, device="cuda")
     value = attempts_all / (total_ms_max * 1e-3)
 
     # roofline of the sweep kernel: algorithmic bytes per attempt (own spin read +

@@ -584,9 +584,19 @@ __device__ __forceinline__ void stage_params(const SweepArgs& a, float* zsm) {
 // Shared-memory floats one warp of the fast kernel uses (host and device agree):
 // rmax records (uint2) then dmax Z rows of NR floats, each region a multiple of 16 bytes.
 __host__ __device__ __forceinline__ size_t fast_rec_floats(int rmax) { return (2 * (size_t)rmax + 3) & ~(size_t)3; }
+__host__ __device__ __forceinline__ size_t fast_nbid_words(int dmax) { return ((size_t)dmax + 3) & ~(size_t)3; }
 __host__ __device__ __forceinline__ size_t fast_group_floats(int dmax, int rmax, int NR) {
-  return fast_rec_floats(rmax) + (((size_t)dmax * NR + 3) & ~(size_t)3);
+  return fast_rec_floats(rmax) + fast_nbid_words(dmax) + (((size_t)dmax * NR + 3) & ~(size_t)3);
 }
+
+// A warp's first item of the next colour, read before the grid barrier: its
+// descriptor and own spin (registers) and its records and neighbour ids (the
+// warp's shared memory). None of these change while the current colour updates.
+struct FastPre {
+  int item;  // -1: nothing prefetched
+  int4 dsc;
+  float4 e;
+};
 
 template <int N>
 __device__ __forceinline__ float pick(const float* v, int k) {
@@ -633,7 +643,7 @@ __device__ void make_proposals(const SweepArgs& a) {
 
 template <int LMAX, bool PERSIST>
 __device__ void fast_colour(const SweepArgs& a, int col, unsigned long long* s_dE, unsigned int* s_cnt,
-                            float* zsm) {
+                            float* zsm, FastPre& pre, int next_col) {
   // One warp per (site, replica) item: lane = slice * G + row. The G row lanes own
   // coefficient rows 1..NR; the S = 32 / G slices split the site's records
   // (record j goes to slice j % S) and are summed with a fixed butterfly.
@@ -650,7 +660,10 @@ __device__ void fast_colour(const SweepArgs& a, int col, unsigned long long* s_d
   const int n_warps = gridDim.x * warps_per_block;
   const size_t per_warp = fast_group_floats(a.dmax, a.rmax, NR);
   uint2* rb = reinterpret_cast<uint2*>(zsm + fast_param_floats(a.n_slots) + (size_t)wib * per_warp);
-  float* zb = zsm + fast_param_floats(a.n_slots) + (size_t)wib * per_warp + fast_rec_floats(a.rmax);
+  int* nbid = reinterpret_cast<int*>(zsm + fast_param_floats(a.n_slots) + (size_t)wib * per_warp +
+                                     fast_rec_floats(a.rmax));
+  float* zb = zsm + fast_param_floats(a.n_slots) + (size_t)wib * per_warp + fast_rec_floats(a.rmax) +
+              fast_nbid_words(a.dmax);
   const double* p_beta = reinterpret_cast<const double*>(zsm);
   const double* p_step = p_beta + a.n_slots;
   const unsigned long long* p_seed = reinterpret_cast<const unsigned long long*>(p_step + a.n_slots);
@@ -662,13 +675,14 @@ __device__ void fast_colour(const SweepArgs& a, int col, unsigned long long* s_d
     const int R = L.R;
     const int q = local / R;
     const int r = local - q * R;
-    const int4 dsc = __ldg(L.idesc + __ldg(L.color_ptr + col) + q);
+    const bool have = item == pre.item;  // warp-uniform
+    const int4 dsc = have ? pre.dsc : __ldg(L.idesc + __ldg(L.color_ptr + col) + q);
     const int s = dsc.x & 0x3fffffff;
     if (do_or && !(dsc.x & (1 << 30))) continue;  // warp-uniform: no l = 1 channel
     const int slot = L.slot0 + r;
     const float4* __restrict__ sp = a.spins + L.spin_off;
     // independent loads of the item, issued before the table walk
-    const float4 e = load_spin<PERSIST>(sp + (int64_t)s * R + r);
+    const float4 e = have ? pre.e : load_spin<PERSIST>(sp + (int64_t)s * R + r);
     float4 p4 = make_float4(0.f, 0.f, 0.f, 0.f);
     double u_pre = 0.0, lq = 0.0;
     if (!do_or && a.prop != nullptr) {
@@ -684,11 +698,18 @@ __device__ void fast_colour(const SweepArgs& a, int col, unsigned long long* s_d
     const int n_one = (dsc.x >> 31) & 1;
     const int nrec = n_pair + n_trip + n_quad + n_one;
     // every record and neighbour spin of the site is requested before any is used
-    for (int k = lane; k < nrec; k += 32) rb[k] = __ldg(L.frec + j0 + k);
-    for (int k = lane; k < nd; k += 32) {
-      const int nb = __ldg(L.nb_list + n0 + k);
-      const float4 v = load_spin<PERSIST>(sp + (int64_t)nb * R + r);
-      zrow_nr<NR>(v.x, v.y, v.z, zb + k * NR);
+    if (have) {
+      for (int k = lane; k < nd; k += 32) {
+        const float4 v = load_spin<PERSIST>(sp + (int64_t)nbid[k] * R + r);
+        zrow_nr<NR>(v.x, v.y, v.z, zb + k * NR);
+      }
+    } else {
+      for (int k = lane; k < nrec; k += 32) rb[k] = __ldg(L.frec + j0 + k);
+      for (int k = lane; k < nd; k += 32) {
+        const int nb = __ldg(L.nb_list + n0 + k);
+        const float4 v = load_spin<PERSIST>(sp + (int64_t)nb * R + r);
+        zrow_nr<NR>(v.x, v.y, v.z, zb + k * NR);
+      }
     }
     __syncwarp();
     float acc = 0.0f, acc2 = 0.0f;
@@ -836,6 +857,28 @@ __device__ void fast_colour(const SweepArgs& a, int col, unsigned long long* s_d
       if (a.rec_lqr != nullptr && !do_or) a.rec_lqr[s] = lq;
     }
   }
+  // prefetch this warp's first item of the next colour (before the grid barrier)
+  pre.item = -1;
+  if (next_col < 0) return;
+  const int32_t* seg_n = a.seg + (size_t)next_col * (a.n_lat + 1);
+  if (warp >= seg_n[a.n_lat]) return;
+  __syncwarp();
+  const int li = find_lattice(seg_n, a.n_lat, warp);
+  const DevLattice& L = a.lat[li];
+  const int local = warp - seg_n[li];
+  const int q = local / L.R, r = local - q * L.R;
+  const int4 dsc = __ldg(L.idesc + __ldg(L.color_ptr + next_col) + q);
+  if (do_or && !(dsc.x & (1 << 30))) return;
+  const int s = dsc.x & 0x3fffffff;
+  const uint32_t cnt = (uint32_t)dsc.w;
+  const int nd = (int)(cnt >> 24);
+  const int nrec = (int)(cnt & 0xffu) + (int)((cnt >> 8) & 0xffu) + (int)((cnt >> 16) & 0xffu) + ((dsc.x >> 31) & 1);
+  for (int k = lane; k < nrec; k += 32) rb[k] = __ldg(L.frec + dsc.z + k);
+  for (int k = lane; k < nd; k += 32) nbid[k] = __ldg(L.nb_list + dsc.y + k);
+  pre.e = load_spin<PERSIST>(a.spins + L.spin_off + (int64_t)s * L.R + r);
+  pre.dsc = dsc;
+  pre.item = warp;
+  __syncwarp();
 }
 
 #ifdef SCEMC_FAST_MINB
@@ -851,7 +894,9 @@ __global__ void SCEMC_FAST_BOUNDS k_fast_colour(SweepArgs a) {
   __shared__ unsigned int s_cnt[3 * kMaxSlots];
   zero_block(a.n_slots, s_dE, s_cnt);
   stage_params(a, zsm);
-  fast_colour<LMAX, false>(a, a.colour, s_dE, s_cnt, zsm);
+  FastPre pre;
+  pre.item = -1;
+  fast_colour<LMAX, false>(a, a.colour, s_dE, s_cnt, zsm, pre, -1);
   flush_block(a, s_dE, s_cnt);
 }
 
@@ -868,8 +913,10 @@ __global__ void __launch_bounds__(256) k_fast_persistent(SweepArgs a) {
     make_proposals<true>(a);
     ok = grid_barrier(a.gs, a.bar_base, k++, gridDim.x, a.barrier_limit_ns);
   }
+  FastPre pre;
+  pre.item = -1;
   for (int col = 0; ok && col < a.max_colors; ++col) {
-    fast_colour<LMAX, true>(a, col, s_dE, s_cnt, zsm);
+    fast_colour<LMAX, true>(a, col, s_dE, s_cnt, zsm, pre, col + 1 < a.max_colors ? col + 1 : -1);
     if (col + 1 < a.max_colors) ok = grid_barrier(a.gs, a.bar_base, k++, gridDim.x, a.barrier_limit_ns);
   }
   flush_block(a, s_dE, s_cnt);

@@ -14,6 +14,7 @@ src/updates.jl:231-248) and the batched ensemble the PT driver runs on.
 from __future__ import annotations
 
 import ctypes as C
+import time
 from dataclasses import dataclass
 from typing import Optional, Sequence
 
@@ -378,7 +379,8 @@ def gpu_run_pt(gHs, *, temperature=None, kT=None, exchange: bool = True, exchang
                sweeps_therm: int = 2000, sweeps_measure: int = 10000, measure_interval: int = 1,
                or_per_metropolis: int = 0, step: float = 0.6, adapt_target: float = 0.5, adapt_interval: int = 50,
                renorm_interval: int = 1000, nbins: int = 32, init=None, seed: Optional[int] = None,
-               lanes_per_site: int = 0, mode: int = 0, chunk: int = 2000) -> PTResult:
+               lanes_per_site: int = 0, mode: int = 0, chunk: int = 2000, kernel: int = 0, proposals: int = 0,
+               learned=None) -> PTResult:
     """Parallel tempering on the device (gpu_pt.jl:261-316 semantics; exchanges run on
     the device). `gHs` is one GPUTiledHamiltonian or a list of them: every table set
     gets its own ladder over the same kT values (chains of uneven supercells), and
@@ -386,7 +388,11 @@ def gpu_run_pt(gHs, *, temperature=None, kT=None, exchange: bool = True, exchang
     chains at their temperatures (run_mc with one chain per temperature).
 
     Seeds: a numpy Generator seeded with `seed` draws, in order, the initial spins of
-    every slot (uniform on S^2) and then one 64-bit device key per slot."""
+    every slot (uniform on S^2) and then one 64-bit device key per slot.
+
+    learned=(net, env) registers a learned proposal network (scemc.learned) with the
+    batch; proposals=3 then draws every Metropolis proposal from it. The wall time
+    of the measurement phase is returned in extra["measure_s"]."""
     if isinstance(gHs, GPUTiledHamiltonian):
         gHs = [gHs]
     kts = resolve_kt(temperature, kT)
@@ -421,8 +427,11 @@ def gpu_run_pt(gHs, *, temperature=None, kT=None, exchange: bool = True, exchang
     seeds = rng.integers(0, 2 ** 64, size=R * len(gHs), dtype=np.uint64)
     batch = GPUBatch(gHs, [R] * len(gHs), configs, seeds, step)
     batch.set_betas(np.tile(1.0 / kts, len(gHs)))
+    if learned is not None:
+        batch.set_learned(*learned)
     common = dict(or_per_metropolis=or_per_metropolis, exchange=exchange, exchange_interval=exchange_interval,
-                  renorm_interval=renorm_interval, lanes_per_site=lanes_per_site, mode=mode)
+                  renorm_interval=renorm_interval, lanes_per_site=lanes_per_site, mode=mode, kernel=kernel,
+                  proposals=proposals)
     done = 0
     while done < sweeps_therm:
         n = min(chunk, sweeps_therm - done)
@@ -438,6 +447,7 @@ def gpu_run_pt(gHs, *, temperature=None, kT=None, exchange: bool = True, exchang
     for g in gHs:
         rec_off.append(rec_off[-1] + R)
     done = 0
+    t_meas = time.perf_counter()
     while done < sweeps_measure:
         n = min(chunk, sweeps_measure - done)
         batch.run(n, measure_interval=measure_interval, phase_done=done, phase_total=sweeps_measure, **common)
@@ -448,6 +458,7 @@ def gpu_run_pt(gHs, *, temperature=None, kT=None, exchange: bool = True, exchang
             A = gHs[li].host.n_cell_atoms
             if len(rec):
                 acc.push_records(rec[:, i, : 4 + 3 * A])
+    measure_s = time.perf_counter() - t_meas
     st = batch.download()
     points = []
     for i, acc in enumerate(accs):
@@ -467,4 +478,5 @@ def gpu_run_pt(gHs, *, temperature=None, kT=None, exchange: bool = True, exchang
             swaps.append(b / a if a else np.nan)
     finals = [st["configs"][st["slot_of_rung"][i]] for i in range(len(accs))]
     return PTResult(points, np.asarray(swaps), finals, seed,
-                    extra=dict(energies=st["energies"], slot_of_rung=st["slot_of_rung"], batch=batch))
+                    extra=dict(energies=st["energies"], slot_of_rung=st["slot_of_rung"], batch=batch,
+                               measure_s=measure_s))

@@ -140,3 +140,50 @@ def environment_rows(configs, env: np.ndarray, kts_ev, sites=None) -> np.ndarray
         x = cfg[env[ss]].reshape(len(ss), -1)
         rows.append(np.concatenate([x, np.full((len(ss), 1), kt / MEV)], axis=1))
     return np.concatenate(rows).astype(np.float32)
+
+
+def collect_training_set(H, env, kts, n_rows: int, *, sweeps_therm: int = 2000, snapshots: int = 4,
+                         spacing: int = 50, seed: int = 0, kernel: int = 0):
+    """Site environments from plain-Metropolis chains, one per kT (one batch on the
+    device): after `sweeps_therm` adaptive-step sweeps, `snapshots` configurations
+    `spacing` sweeps apart; n_rows rows drawn evenly over kT values and snapshots.
+    Returns (X (n, 43) float32, Y (n, 3) float32): inputs and the site's own spin."""
+    from .gpu import GPUBatch, GPUTiledHamiltonian
+    gH = H if isinstance(H, GPUTiledHamiltonian) else GPUTiledHamiltonian(H)
+    host = gH.host
+    rng = np.random.default_rng(seed)
+    R = len(kts)
+    cfgs = []
+    for _ in range(R):
+        v = rng.standard_normal((host.n_sites, 3))
+        cfgs.append(v / np.linalg.norm(v, axis=1, keepdims=True))
+    b = GPUBatch([gH], [R], cfgs, rng.integers(0, 2 ** 63, size=R).tolist(), 0.6)
+    b.set_betas(1.0 / np.asarray(kts))
+    b.run(sweeps_therm, adapt_interval=50, adapt_target=0.5, phase_total=sweeps_therm, kernel=kernel)
+    per = int(np.ceil(n_rows / (R * snapshots)))
+    X, Y = [], []
+    for _ in range(snapshots):
+        b.run(spacing, kernel=kernel)
+        st = b.download()
+        for r in range(R):
+            cfg = st["configs"][st["slot_of_rung"][r]]
+            sites = rng.choice(host.n_sites, size=per, replace=per > host.n_sites)
+            X.append(environment_rows([cfg], env, [kts[r]], sites))
+            Y.append(np.asarray(cfg)[sites].astype(np.float32))
+    X = np.concatenate(X)[:n_rows]
+    Y = np.concatenate(Y)[:n_rows]
+    return X, Y
+
+
+def ess_per_second(result) -> tuple:
+    """(ESS/s, per-point ESS, per-point max tau_int) of a PT/run_mc result:
+    ESS = n_meas / (1 + 2 max(tau_int(E), tau_int(|m|))) summed over the points
+    (the reference's tau_int convention, binning.jl:120-128), over the measurement
+    phase's wall time."""
+    ess, taus = [], []
+    for p in result.points:
+        t = max(float(np.nanmax(p.stats["energy"].tau_int)), float(np.nanmax(p.stats["absm"].tau_int)), 0.0)
+        n = p.stats["energy"].count
+        taus.append(t)
+        ess.append(n / (1.0 + 2.0 * t))
+    return float(np.sum(ess) / result.extra["measure_s"]), np.asarray(ess), np.asarray(taus)
