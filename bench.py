@@ -21,6 +21,12 @@ rungs followed by an on-device replica-exchange attempt. The spins alone
 The metric counts attempts on active sites (Metropolis + overrelaxation) per
 second, summed over chains and GPUs. Synthetic, seeded inputs (no fitted model).
 
+--workload pt (the batched parallel-tempering configuration): 4 ladders of 16 rungs
+(kT geometric in [0.1, 3.0] meV) on bcc 8^3, 12^3, 16^3 and 24^3 (645,120 spins
+per rung set), J1/J2 isotropic l = 1 + (NN, NN, NNN) triangles N(0, 0.1 meV), all
+64 chains in one batch. One step = one Metropolis sweep of every chain followed by
+an on-device exchange attempt in every ladder.
+
 --workload learned (the learned-proposal configuration): bcc 32^3 (65,536 spins),
 J1 = -1.0 / J2 = -0.2 meV isotropic l = 1 plus l = 1 body-4 plaquettes N(0, 0.05 meV),
 16 chains at kT geometric in [0.2, 2.0] meV. The network is trained on 200k site
@@ -57,6 +63,7 @@ WORKLOADS = {
     "bcc16": "bcc16_l2_plaquette_zeeman_5T_metropolis+OR",
     "fcc": "fcc{n}_l2_tri_zeeman_32rungs_metropolis+OR+exchange",
     "learned": "bcc32_J1J2_body4_16T_learned_vs_plain",
+    "pt": "bcc8-12-16-24_J1J2_triangles_4x16rungs_PT",
 }
 
 
@@ -74,6 +81,9 @@ def workload(args):
     if args.workload == "fcc":
         w = models.config5_fcc(n=args.fcc_n, replicas=32)
         return WORKLOADS["fcc"].format(n=args.fcc_n), w, w.hamiltonians()[0], True
+    if args.workload == "pt":
+        w = models.config3_bcc_pt()
+        return WORKLOADS["pt"], w, w.hamiltonians(), True
     w = models.config2_bcc_l2(16)
     return WORKLOADS["bcc16"], w, w.hamiltonians()[0], False
 
@@ -107,7 +117,11 @@ def run_learned(args) -> int:
     torch.cuda.synchronize()
     t2 = time.perf_counter()
     measure = args.steps
-    kw = dict(kT=w.kts, exchange=False, sweeps_therm=2000, sweeps_measure=measure, seed=4, kernel=args.kernel)
+    # both samplers start from the ordered state (every kT of the ladder lies below the
+    # ordering temperature), so neither number carries a coarsening transient
+    up = np.tile([0.0, 0.0, 1.0], (H.n_sites, 1))
+    kw = dict(kT=w.kts, exchange=False, sweeps_therm=2000, sweeps_measure=measure, seed=4, kernel=args.kernel,
+              init=up)
     plain = scemc.gpu_run_pt(gH, **kw)
     lrn = scemc.gpu_run_pt(gH, learned=(net, env), proposals=3, **kw)
     ess_p, _, tau_p = learned.ess_per_second(plain)
@@ -232,9 +246,9 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
-    big = args.workload == "fcc"
+    big = args.workload in ("fcc", "pt")
     if args.steps is None:
-        args.steps = {"fcc": 20, "learned": 10000}.get(args.workload, 2000)
+        args.steps = {"fcc": 20, "learned": 10000, "pt": 200}.get(args.workload, 2000)
     if args.workload == "learned":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned proposal; "
@@ -250,6 +264,7 @@ def main():
         if rank != 0:
             return 0
         name, w, H, _ = workload(args)
+        H = H[0] if isinstance(H, list) else H  # the CPU sample runs on the first table set
         steps = max(1, min(args.steps, 50))
         v, threads, sample, ms = run_cpu_reference(w, H, steps, min(args.warmup, 3) if not big else 1,
                                                    args.cpu_budget, max_chains=1 if big else 0)
@@ -277,14 +292,20 @@ def main():
         dist = dist_
 
     name, w, H, exchange = workload(args)
-    gH = scemc.GPUTiledHamiltonian(H)
-    d_mean, a_mean, table_bytes = gH.stats()
+    Hs = H if isinstance(H, list) else [H]
+    gHs = [scemc.GPUTiledHamiltonian(h) for h in Hs]
+    st_ = [g.stats() for g in gHs]
+    wts = np.array([h.n_sites for h in Hs], float)
+    d_mean = float(np.dot([x[0] for x in st_], wts) / wts.sum())
+    a_mean = float(np.dot([x[1] for x in st_], wts) / wts.sum())
+    table_bytes = int(sum(x[2] for x in st_))
     R = len(w.kts)
     rng = np.random.default_rng(2 + 1000 * rank)
-    configs = [models_random(H.n_sites, rng) for _ in range(R)]
-    seeds = ranks.rank_keys(2, rank, R)
-    batch = scemc.GPUBatch([gH], [R], configs, seeds, 0.6)
-    batch.set_betas(1.0 / w.kts)
+    configs = [models_random(h.n_sites, rng) for h in Hs for _ in range(R)]
+    seeds = ranks.rank_keys(2, rank, R * len(Hs))
+    batch = scemc.GPUBatch(gHs, [R] * len(Hs), configs, seeds, 0.6)
+    batch.set_betas(np.tile(1.0 / w.kts, len(Hs)))
+    H = Hs[0]
     n_or = w.or_per_metropolis
     form = dict(lanes_per_site=args.lanes, mode=args.mode, kernel=args.kernel)
     # exchange after every sweep: phase_total far ahead so that no sweep is a phase's last
@@ -382,9 +403,10 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": name, "sites_per_chain": H.n_sites, "chains_per_gpu": R,
+            "config": {"workload": name, "sites_per_chain": [h.n_sites for h in Hs] if len(Hs) > 1 else H.n_sites,
+                       "chains_per_gpu": R * len(Hs),
                        "compound_sweep": f"1 Metropolis + {n_or} OR" + (" + exchange" if exchange else ""),
-                       "l2": ("inputs larger than L2 (spins alone %.0f MiB)" % (R * H.n_sites * 16 / 2 ** 20)) if big
+                       "l2": ("inputs larger than L2 (spins alone %.0f MiB)" % (R * wts.sum() * 16 / 2 ** 20)) if big
                        else "flushed (256 MiB) before every step",
                        "lanes_per_site": args.lanes or "auto", "mode": args.mode or "auto",
                        "kernel": args.kernel or "auto", "autotuned": tuned,

@@ -31,6 +31,7 @@
 #include "scemc.h"
 #include "scemc_device.cuh"
 #include "mlp.h"
+#include "umma.cuh"
 #include "vmf.cuh"
 
 #include <cuda_runtime.h>
@@ -1212,19 +1213,103 @@ __device__ __forceinline__ float slot_kt_mev(const SweepArgs& a, int slot) {
   return (float)(1.0e3 / a.beta[a.rung_of_slot[slot]]);
 }
 
-__global__ void __launch_bounds__(256) k_learned_rows(SweepArgs a, __nv_bfloat16* X, int64_t M) {
+// Fused learned proposal of one colour: one warpgroup per tile of 128 items (persistent
+// over tiles). Each thread gathers its item's environment into the BF16 input tile;
+// the three layers run on the tcgen05 tensor cores (weights resident in shared
+// memory, FP32 accumulators in TMEM, bias + SiLU epilogues writing the next layer's
+// BF16 operand tile); each thread then reads its 20 outputs and draws from the vMF
+// mixture. Shared-memory operand tiles use the K-major no-swizzle layout in 64-column
+// chunks (umma.cuh).
+struct LearnedNet {
+  const __nv_bfloat16* W1;  // [128][64]
+  const __nv_bfloat16* W2;  // [128][128]
+  const __nv_bfloat16* W3;  // [32][128]
+  const float* b1;          // [128]
+  const float* b2;          // [128]
+  const float* b3;          // [32]
+  int* err;
+};
+
+constexpr int kTile = 128;
+constexpr uint32_t kChunkBytes = 128u * 64u * 2u;  // one 128-row x 64-column BF16 chunk
+// dynamic shared memory of k_learned_fused (bytes): W1 (1 chunk), W2 (2), W3 (2 x 32 rows),
+// X (1), H (2), biases
+constexpr size_t kLearnedSmem = 1024 + kChunkBytes * (1 + 2 + 1 + 2) + 2u * (32u * 64u * 2u) + 4 * (128 + 128 + 32);
+
+__device__ __forceinline__ void stage_rows_kmajor(uint8_t* dst, const __nv_bfloat16* src, int rows, int K) {
+  // src [rows][K] row-major -> chunks of 64 columns, each rows x 64 K-major no-swizzle
+  const int pieces = rows * (K / 8);
+  for (int p = threadIdx.x; p < pieces; p += blockDim.x) {
+    const int row = p / (K / 8), kg = p % (K / 8);
+    const int chunk = kg >> 3, kk = (kg & 7) * 8;
+    const uint4 v = *reinterpret_cast<const uint4*>(src + (int64_t)row * K + kg * 8);
+    *reinterpret_cast<uint4*>(dst + (size_t)chunk * rows * 128 + umma::kmajor_offset(row, kk, 64)) = v;
+  }
+}
+
+// issue one layer: D (TMEM) = A (128 x K, chunks) . B (N x K, chunks)^T
+__device__ __forceinline__ void learned_layer(uint32_t tmem_d, const uint8_t* A, const uint8_t* B, int n_rows_b,
+                                              int K, int N, uint64_t* mbar) {
+  umma::fence_after();
+  const uint32_t a0 = umma::smem_u32(A), b0 = umma::smem_u32(B);
+  const uint32_t idesc = umma::idesc_bf16_f32(N);
+  for (int kk = 0; kk < K / 16; ++kk) {
+    const uint32_t ch = (uint32_t)(kk >> 2), in = (uint32_t)(kk & 3) * 256u;
+    const uint64_t ad = umma::smem_desc(a0 + ch * (128u * 128u) + in, 128u, 1024u);
+    const uint64_t bd = umma::smem_desc(b0 + ch * ((uint32_t)n_rows_b * 128u) + in, 128u, 1024u);
+    umma::mma_bf16(tmem_d, ad, bd, idesc, kk > 0 ? 1u : 0u);
+  }
+  umma::commit(mbar);
+}
+
+__global__ void __launch_bounds__(128) k_learned_fused(SweepArgs a, LearnedNet net, double* lqr) {
+  extern __shared__ __align__(1024) uint8_t lsm[];
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(lsm) + 1023) & ~(uintptr_t)1023);
+  uint8_t* sW1 = base;
+  uint8_t* sW2 = sW1 + kChunkBytes;
+  uint8_t* sW3 = sW2 + 2 * kChunkBytes;
+  uint8_t* sX = sW3 + 2 * (32u * 64u * 2u);
+  uint8_t* sH = sX + kChunkBytes;
+  float* sb = reinterpret_cast<float*>(sH + 2 * kChunkBytes);
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tslot;
+  const int tid = threadIdx.x, warp = tid >> 5;
   const int col = a.colour;
   const int32_t* seg_c = a.seg + (size_t)col * (a.n_lat + 1);
   const int n_items = seg_c[a.n_lat];
-  for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < M; row += (int64_t)gridDim.x * blockDim.x) {
+  const int n_tiles = (n_items + kTile - 1) / kTile;
+  if ((int)blockIdx.x >= n_tiles) return;
+  if (warp == 0) umma::tmem_alloc(&tslot, 256u);
+  if (tid == 0) umma::mbar_init(&mbar, 1);
+  stage_rows_kmajor(sW1, net.W1, 128, 64);
+  stage_rows_kmajor(sW2, net.W2, 128, 128);
+  stage_rows_kmajor(sW3, net.W3, 32, 128);
+  for (int i = tid; i < 128; i += blockDim.x) {
+    sb[i] = net.b1[i];
+    sb[128 + i] = net.b2[i];
+    if (i < 32) sb[256 + i] = net.b3[i];
+  }
+  umma::fence_async_smem();
+  umma::fence_before();
+  __syncthreads();
+  umma::fence_after();
+  const uint32_t tmem = tslot;
+  const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+  uint32_t phase = 0;
+  bool ok = true;
+  for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
+    const int item = tile * kTile + tid;
+    const bool valid = item < n_items;
+    int li = 0, q = 0, r = 0, s = 0;
+    float4 e = make_float4(0.f, 0.f, 1.f, 0.f);
+    float tau = 1.0f;
     alignas(16) __nv_bfloat16 x[vmf::kInPad];
 #pragma unroll
     for (int k = 0; k < vmf::kInPad; ++k) x[k] = __float2bfloat16_rn(0.0f);
-    if (row < n_items) {
-      int li, q, r;
-      item_of(a, seg_c, (int)row, li, q, r);
+    if (valid) {
+      item_of(a, seg_c, item, li, q, r);
       const DevLattice& L = a.lat[li];
-      const int s = L.color_sites[L.color_ptr[col] + q];
+      s = L.color_sites[L.color_ptr[col] + q];
       const float4* sp = a.spins + L.spin_off;
       const int32_t* env = L.env + (int64_t)s * L.env_k;
       for (int k = 0; k < 14; ++k) {
@@ -1233,37 +1318,90 @@ __global__ void __launch_bounds__(256) k_learned_rows(SweepArgs a, __nv_bfloat16
         x[3 * k + 1] = __float2bfloat16_rn(v.y);
         x[3 * k + 2] = __float2bfloat16_rn(v.z);
       }
-      x[42] = __float2bfloat16_rn(slot_kt_mev(a, L.slot0 + r));
+      tau = slot_kt_mev(a, L.slot0 + r);
+      x[42] = __float2bfloat16_rn(tau);
+      e = sp[(int64_t)s * L.R + r];
     }
-    uint4* dst = reinterpret_cast<uint4*>(X + row * vmf::kInPad);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) dst[k] = reinterpret_cast<const uint4*>(x)[k];
-  }
-}
-
-__global__ void __launch_bounds__(128) k_learned_propose(SweepArgs a, const float* O, double* lqr) {
-  const int col = a.colour;
-  const int32_t* seg_c = a.seg + (size_t)col * (a.n_lat + 1);
-  const int n_items = seg_c[a.n_lat];
-  for (int item = blockIdx.x * blockDim.x + threadIdx.x; item < n_items; item += gridDim.x * blockDim.x) {
-    int li, q, r;
-    item_of(a, seg_c, item, li, q, r);
+    for (int kg = 0; kg < 8; ++kg)
+      *reinterpret_cast<uint4*>(sX + umma::kmajor_offset(tid, kg * 8, 64)) = reinterpret_cast<const uint4*>(x)[kg];
+    umma::fence_async_smem();
+    umma::fence_before();
+    __syncthreads();
+    // layer 1 -> TMEM columns 0..127
+    if (tid == 0) learned_layer(tmem, sX, sW1, 128, 64, 128, &mbar);
+    ok = umma::mbar_wait(&mbar, phase, 1000000000ull);
+    phase ^= 1u;
+    umma::fence_after();
+    for (int c0 = 0; c0 < 128; c0 += 8) {
+      float v[8];
+      umma::tmem_ld8(tmem + lane_base + (uint32_t)c0, v);
+      alignas(16) __nv_bfloat16 h[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const float z = v[i] + sb[c0 + i];
+        h[i] = __float2bfloat16_rn(z / (1.0f + __expf(-z)));
+      }
+      *reinterpret_cast<uint4*>(sH + (c0 >> 6) * kChunkBytes + umma::kmajor_offset(tid, c0 & 63, 64)) =
+          *reinterpret_cast<const uint4*>(h);
+    }
+    umma::fence_async_smem();
+    umma::fence_before();
+    __syncthreads();
+    // layer 2 -> TMEM columns 128..255
+    if (tid == 0) learned_layer(tmem + 128u, sH, sW2, 128, 128, 128, &mbar);
+    ok = ok && umma::mbar_wait(&mbar, phase, 1000000000ull);
+    phase ^= 1u;
+    umma::fence_after();
+    for (int c0 = 0; c0 < 128; c0 += 8) {
+      float v[8];
+      umma::tmem_ld8(tmem + lane_base + 128u + (uint32_t)c0, v);
+      alignas(16) __nv_bfloat16 h[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const float z = v[i] + sb[128 + c0 + i];
+        h[i] = __float2bfloat16_rn(z / (1.0f + __expf(-z)));
+      }
+      *reinterpret_cast<uint4*>(sH + (c0 >> 6) * kChunkBytes + umma::kmajor_offset(tid, c0 & 63, 64)) =
+          *reinterpret_cast<const uint4*>(h);
+    }
+    umma::fence_async_smem();
+    umma::fence_before();
+    __syncthreads();
+    // layer 3 -> TMEM columns 0..31
+    if (tid == 0) learned_layer(tmem, sH, sW3, 32, 128, 32, &mbar);
+    ok = ok && umma::mbar_wait(&mbar, phase, 1000000000ull);
+    phase ^= 1u;
+    umma::fence_after();
+    float o[32];
+#pragma unroll
+    for (int c0 = 0; c0 < 32; c0 += 8) umma::tmem_ld8(tmem + lane_base + (uint32_t)c0, o + c0);
+    umma::fence_before();
+    __syncthreads();  // every thread has read TMEM and the tiles before the next tile reuses them
+    if (!valid || !ok) continue;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) o[j] += sb[256 + j];
     const DevLattice& L = a.lat[li];
-    const int s = L.color_sites[L.color_ptr[col] + q];
     const int slot = L.slot0 + r;
     const int rung = a.rung_of_slot[slot];
-    const float4 e = a.spins[L.spin_off + (int64_t)s * L.R + r];
     vmf::Mix mix;
-    vmf::mixture(O + (int64_t)item * vmf::kOutPad, (double)slot_kt_mev(a, slot), mix);
+    vmf::mixture(o, (double)tau, mix);
     const Blk b0 = philox_block(a.seed[rung], (uint32_t)(s + 1), a.st->sweep + 1u, 0u, kTagLearn);
     const Blk b1 = philox_block(a.seed[rung], (uint32_t)(s + 1), a.st->sweep + 1u, 1u, kTagLearn);
-    double x[3];
-    vmf::sample(mix, philox_uniform(b0.w0, b0.w1), philox_uniform(b0.w2, b0.w3), philox_uniform(b1.w0, b1.w1), x);
-    const float px = (float)x[0], py = (float)x[1], pz = (float)x[2];
+    double xs[3];
+    vmf::sample(mix, philox_uniform(b0.w0, b0.w1), philox_uniform(b0.w2, b0.w3), philox_uniform(b1.w0, b1.w1), xs);
+    const float px = (float)xs[0], py = (float)xs[1], pz = (float)xs[2];
     const int idx = a.item_base[col] + item;
     a.prop[idx] = make_float4(px, py, pz, 0.0f);
     a.propu[idx] = philox_uniform(b1.w2, b1.w3);
     lqr[idx] = vmf::log_q(mix, e.x, e.y, e.z) - vmf::log_q(mix, px, py, pz);
+  }
+  if (!ok && tid == 0 && net.err) atomicExch(net.err, 1);
+  umma::fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    umma::fence_after();
+    umma::tmem_free(tmem, 256u);
   }
 }
 
@@ -1578,14 +1716,11 @@ struct scemc_ensemble {
   int coop_blocks = 0;  // cached co-resident grid size for the persistent form
   int coop_G = -1;
   float4* h_stage = nullptr;  // pinned host staging of the spins (n_spins float4)
-  // learned proposal (network not owned), per-colour work buffers
+  // learned proposal (network not owned)
   const scemc_mlp* mlp = nullptr;
   std::vector<int32_t*> d_env;
-  __nv_bfloat16 *d_lx = nullptr, *d_lh1 = nullptr, *d_lh2 = nullptr;
-  float* d_lo = nullptr;
   double* d_lqr = nullptr;
   double* d_rlqr = nullptr;
-  int64_t lcap = 0;
   // row-parallel fast kernel
   bool fast = false;
   int32_t dmax = 0, rmax = 0;
@@ -1621,7 +1756,7 @@ struct scemc_ensemble {
     }
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
     for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
-    void* qs[] = {d_item_base, d_prop, d_propu, d_lx, d_lh1, d_lh2, d_lo, d_lqr, d_rlqr};
+    void* qs[] = {d_item_base, d_prop, d_propu, d_lqr, d_rlqr};
     for (int32_t* p : d_env)
       if (p) cudaFree(p);
     for (void* p : qs)
@@ -2379,29 +2514,15 @@ int max_colour_items(const scemc_ensemble* E) {
   return m;
 }
 
-int32_t ensure_learned(scemc_ensemble* E, int64_t M) {
-  if (E->lcap >= M) return SCEMC_OK;
-  void* ps[] = {E->d_lx, E->d_lh1, E->d_lh2, E->d_lo};
-  for (void* p : ps)
-    if (p) cudaFree(p);
-  E->d_lx = E->d_lh1 = E->d_lh2 = nullptr;
-  E->d_lo = nullptr;
-  E->lcap = 0;
-  int32_t rc;
-  if ((rc = dalloc(&E->d_lx, (size_t)M * vmf::kInPad)) || (rc = dalloc(&E->d_lh1, (size_t)M * vmf::kHid)) ||
-      (rc = dalloc(&E->d_lh2, (size_t)M * vmf::kHid)) || (rc = dalloc(&E->d_lo, (size_t)M * vmf::kOutPad)))
-    return rc;
-  E->lcap = M;
-  return SCEMC_OK;
-}
-
-// Learned Metropolis pass: per colour, the network inputs, the tensor-core MLP, the
-// mixture draws with their density ratios, then the sweep kernel on those proposals.
+// Learned Metropolis pass: per colour, the fused network + mixture-draw kernel, then
+// the sweep kernel on those proposals.
 int32_t prepare_learned(scemc_ensemble* E) {
   int32_t rc;
   if ((rc = ensure_props(E))) return rc;
   if (!E->d_lqr && (rc = dalloc(&E->d_lqr, (size_t)std::max<int32_t>(E->item_base.back(), 1)))) return rc;
-  return ensure_learned(E, ((int64_t)max_colour_items(E) + 127) / 128 * 128);
+  CUDA_TRY(cudaFuncSetAttribute((const void*)k_learned_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kLearnedSmem));
+  return SCEMC_OK;
 }
 
 int32_t run_learned_pass(scemc_ensemble* E, const Launch& Lc) {
@@ -2414,22 +2535,23 @@ int32_t run_learned_pass(scemc_ensemble* E, const Launch& Lc) {
   a.dmax = std::max(E->dmax, 1);
   a.rmax = std::max(E->rmax, 1);
   const int cap = sm_count(E->device) * 64;
+  LearnedNet net;
+  net.W1 = E->mlp->d_W1;
+  net.W2 = E->mlp->d_W2;
+  net.W3 = E->mlp->d_W3;
+  net.b1 = E->mlp->d_master + mlpl::oB1;
+  net.b2 = E->mlp->d_master + mlpl::oB2;
+  net.b3 = E->mlp->d_master + mlpl::oB3;
+  net.err = &E->d_gs->error;
   for (int c = 0; c < E->max_colors; ++c) {
     const int n = E->seg[(size_t)c * (E->tabs.size() + 1) + E->tabs.size()];
     if (n == 0) continue;
     a.colour = c;
-    const int64_t Mc = ((int64_t)n + 127) / 128 * 128;
     a.lqr = nullptr;
+    const int tiles = (n + kTile - 1) / kTile;
     ++E->launches;
-    k_learned_rows<<<(unsigned)std::min<int64_t>(cap, (Mc + 255) / 256), 256, 0, E->stream>>>(a, E->d_lx, Mc);
-    CUDA_TRY(cudaGetLastError());
-    E->launches += 3;
-    if ((rc = scemc_detail::mlp_forward_dev(E->mlp, E->d_lx, Mc, E->d_lh1, E->d_lh2, E->d_lo, E->stream,
-                                            &E->d_gs->error)))
-      return rc;
-    ++E->launches;
-    k_learned_propose<<<(unsigned)std::min<int64_t>(cap, ((int64_t)n + 127) / 128), 128, 0, E->stream>>>(a, E->d_lo,
-                                                                                                      E->d_lqr);
+    k_learned_fused<<<(unsigned)std::min(tiles, 2 * sm_count(E->device)), 128, kLearnedSmem, E->stream>>>(
+        a, net, E->d_lqr);
     CUDA_TRY(cudaGetLastError());
     a.lqr = E->d_lqr;
     ++E->launches;
@@ -2739,12 +2861,12 @@ int32_t resolve_launch(const scemc_ensemble* E, int lanes, int mode, int kernel,
   if (kernel == 1 && !generic_ok) return fail(SCEMC_ERR_ARG, "generic records were not kept for these tables");
   if (kernel == 3 && mode == 2)
     return fail(SCEMC_ERR_ARG, "the replica-parallel kernel runs per-colour launches (mode 1 or 3)");
-  // untuned auto choice: one thread per item once a colour's items fill every SM
-  // and warps hold (mostly) one site's replicas
+  // untuned auto choice: threads that carry replicas once every site has at least 16
+  // of them and a colour holds enough items to fill the SMs (256 per SM)
   int min_r = 1 << 30;
   for (int r : E->R) min_r = std::min(min_r, r);
   const bool rep_auto = E->fast && mode != 2 && min_r >= 16 &&
-                        (int64_t)max_colour_items(E) >= (int64_t)sm_count(E->device) * 2048;
+                        (int64_t)max_colour_items(E) >= (int64_t)sm_count(E->device) * 256;
   L.rep = kernel == 3 || (kernel == 0 && rep_auto);
   L.fast = !L.rep && (kernel == 2 || (kernel == 0 && E->fast));
   L.learned = proposals == 3;

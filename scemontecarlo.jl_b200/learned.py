@@ -46,7 +46,10 @@ class ProposalNet:
 
     def __del__(self):
         if getattr(self, "h", None):
-            _lib.lib().scemc_mlp_destroy(self.h)
+            try:
+                _lib.lib().scemc_mlp_destroy(self.h)
+            except Exception:  # interpreter shutdown: the module may already be gone
+                pass
             self.h = None
 
     def params(self) -> np.ndarray:
@@ -143,10 +146,11 @@ def environment_rows(configs, env: np.ndarray, kts_ev, sites=None) -> np.ndarray
 
 
 def collect_training_set(H, env, kts, n_rows: int, *, sweeps_therm: int = 2000, snapshots: int = 4,
-                         spacing: int = 50, seed: int = 0, kernel: int = 0):
+                         spacing: int = 50, seed: int = 0, kernel: int = 0, init=None):
     """Site environments from plain-Metropolis chains, one per kT (one batch on the
-    device): after `sweeps_therm` adaptive-step sweeps, `snapshots` configurations
-    `spacing` sweeps apart; n_rows rows drawn evenly over kT values and snapshots.
+    device): after `sweeps_therm` adaptive-step sweeps from random spins (or from
+    `init`, one configuration for every chain), `snapshots` configurations `spacing`
+    sweeps apart; n_rows rows drawn evenly over kT values and snapshots.
     Returns (X (n, 43) float32, Y (n, 3) float32): inputs and the site's own spin."""
     from .gpu import GPUBatch, GPUTiledHamiltonian
     gH = H if isinstance(H, GPUTiledHamiltonian) else GPUTiledHamiltonian(H)
@@ -155,6 +159,9 @@ def collect_training_set(H, env, kts, n_rows: int, *, sweeps_therm: int = 2000, 
     R = len(kts)
     cfgs = []
     for _ in range(R):
+        if init is not None:
+            cfgs.append(np.asarray(init, np.float64).reshape(-1, 3).copy())
+            continue
         v = rng.standard_normal((host.n_sites, 3))
         cfgs.append(v / np.linalg.norm(v, axis=1, keepdims=True))
     b = GPUBatch([gH], [R], cfgs, rng.integers(0, 2 ** 63, size=R).tolist(), 0.6)
