@@ -1384,17 +1384,17 @@ __global__ void __launch_bounds__(128) k_learned_fused(SweepArgs a, LearnedNet n
     const DevLattice& L = a.lat[li];
     const int slot = L.slot0 + r;
     const int rung = a.rung_of_slot[slot];
-    vmf::Mix mix;
-    vmf::mixture(o, (double)tau, mix);
+    vmf::MixF mix;
+    vmf::mixture_f(o, tau, mix);
     const Blk b0 = philox_block(a.seed[rung], (uint32_t)(s + 1), a.st->sweep + 1u, 0u, kTagLearn);
     const Blk b1 = philox_block(a.seed[rung], (uint32_t)(s + 1), a.st->sweep + 1u, 1u, kTagLearn);
-    double xs[3];
-    vmf::sample(mix, philox_uniform(b0.w0, b0.w1), philox_uniform(b0.w2, b0.w3), philox_uniform(b1.w0, b1.w1), xs);
-    const float px = (float)xs[0], py = (float)xs[1], pz = (float)xs[2];
+    float xs[3];
+    vmf::sample_f(mix, (float)philox_uniform(b0.w0, b0.w1), (float)philox_uniform(b0.w2, b0.w3),
+                  (float)philox_uniform(b1.w0, b1.w1), xs);
     const int idx = a.item_base[col] + item;
-    a.prop[idx] = make_float4(px, py, pz, 0.0f);
+    a.prop[idx] = make_float4(xs[0], xs[1], xs[2], 0.0f);
     a.propu[idx] = philox_uniform(b1.w2, b1.w3);
-    lqr[idx] = vmf::log_q(mix, e.x, e.y, e.z) - vmf::log_q(mix, px, py, pz);
+    lqr[idx] = (double)(vmf::log_q_f(mix, e.x, e.y, e.z) - vmf::log_q_f(mix, xs[0], xs[1], xs[2]));
   }
   if (!ok && tid == 0 && net.err) atomicExch(net.err, 1);
   umma::fence_before();

@@ -1,7 +1,8 @@
 // The learned proposal's output head: a 4-component von Mises-Fisher mixture on S^2
 // read from the MLP's 20 outputs (per component: logit, 3 raw mean components, raw
 // concentration). kappa = softplus(c) / tau + kKappaMin with tau = kT in meV, so the
-// network predicts kappa * kT. FP64 throughout (per item, negligible next to dE).
+// network predicts kappa * kT. The FP64 forms serve training and the host; the sweep
+// draws and evaluates the mixture in FP32 (MixF below).
 #pragma once
 #include <math.h>
 #include <stdint.h>
@@ -121,6 +122,75 @@ __host__ __device__ inline double nll_grad(const float* o, double tau, const dou
       dout[5 * k + 1 + i] = (float)(scale * (-r * kap * (y[i] - d[k] * m.mu[k][i]) * inv));
   }
   return -lq;
+}
+
+// Single-precision form of the mixture used inside the sweep (the draw and the
+// density ratio of one item; the same function evaluates q(e) and q(e'), so the
+// Hastings ratio is exactly that of the distribution sampled up to FP32 rounding).
+struct MixF {
+  float logpi[kComp];
+  float mu[kComp][3];
+  float kappa[kComp];
+};
+
+__device__ inline float softplus_f(float x) { return x > 20.0f ? x : log1pf(expf(x)); }
+
+__device__ inline void mixture_f(const float* o, float tau, MixF& m) {
+  float amax = o[0];
+  for (int k = 1; k < kComp; ++k) amax = fmaxf(amax, o[5 * k]);
+  float s = 0.0f;
+  for (int k = 0; k < kComp; ++k) s += expf(o[5 * k] - amax);
+  const float lse = amax + logf(s);
+  for (int k = 0; k < kComp; ++k) {
+    m.logpi[k] = o[5 * k] - lse;
+    const float x = o[5 * k + 1], y = o[5 * k + 2], z = o[5 * k + 3];
+    const float inv = 1.0f / fmaxf(sqrtf(x * x + y * y + z * z), 1e-12f);
+    m.mu[k][0] = x * inv;
+    m.mu[k][1] = y * inv;
+    m.mu[k][2] = z * inv;
+    m.kappa[k] = softplus_f(o[5 * k + 4]) / tau + (float)kKappaMin;
+  }
+}
+
+__device__ inline float log_q_f(const MixF& m, float x0, float x1, float x2) {
+  float l[kComp], lm = -3.0e38f;
+  for (int k = 0; k < kComp; ++k) {
+    const float d = m.mu[k][0] * x0 + m.mu[k][1] * x1 + m.mu[k][2] * x2;
+    const float kap = m.kappa[k];
+    l[k] = m.logpi[k] + logf(kap) - logf((float)kTwoPi) - logf(-expm1f(-2.0f * kap)) + kap * (d - 1.0f);
+    lm = fmaxf(lm, l[k]);
+  }
+  float s = 0.0f;
+  for (int k = 0; k < kComp; ++k) s += expf(l[k] - lm);
+  return lm + logf(s);
+}
+
+// the draw of sample() in single precision (same inverse CDFs and frame)
+__device__ inline void sample_f(const MixF& m, float u_comp, float u_w, float u_phi, float* out) {
+  int k = 0;
+  float acc = expf(m.logpi[0]);
+  while (k < kComp - 1 && u_comp >= acc) {
+    ++k;
+    acc += expf(m.logpi[k]);
+  }
+  const float kap = m.kappa[k];
+  float w = 1.0f + logf(u_w + (1.0f - u_w) * expf(-2.0f * kap)) / kap;
+  w = fminf(1.0f, fmaxf(-1.0f, w));
+  const float v = sqrtf(fmaxf(0.0f, 1.0f - w * w));
+  const float* mu = m.mu[k];
+  const float a0 = fabsf(mu[0]), a1 = fabsf(mu[1]), a2 = fabsf(mu[2]);
+  const int ax = (a0 <= a1 && a0 <= a2) ? 0 : (a1 <= a2 ? 1 : 2);
+  float t1[3] = {-mu[ax] * mu[0], -mu[ax] * mu[1], -mu[ax] * mu[2]};
+  t1[ax] += 1.0f;
+  const float tn = 1.0f / sqrtf(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
+  t1[0] *= tn, t1[1] *= tn, t1[2] *= tn;
+  const float t2[3] = {mu[1] * t1[2] - mu[2] * t1[1], mu[2] * t1[0] - mu[0] * t1[2], mu[0] * t1[1] - mu[1] * t1[0]};
+  float sp, cp;
+  sincosf((float)kTwoPi * u_phi, &sp, &cp);
+  float x[3];
+  for (int i = 0; i < 3; ++i) x[i] = w * mu[i] + v * (cp * t1[i] + sp * t2[i]);
+  const float n = 1.0f / sqrtf(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+  out[0] = x[0] * n, out[1] = x[1] * n, out[2] = x[2] * n;
 }
 
 }  // namespace vmf
