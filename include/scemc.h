@@ -244,6 +244,14 @@ int32_t scemc_mlp_loss_grad(scemc_mlp* m, const float* x, const float* y, int64_
 int32_t scemc_mlp_train(scemc_mlp* m, const float* x, const float* y, int64_t n, int32_t batch, int32_t epochs,
                         double lr, uint64_t seed, double* epoch_loss);
 
+/* All-site energy gradient (gpu_energy_gradient!, src/gpu/gpu_gradient.jl:193-231):
+ * grad[s] = sum_t c_t(s) grad Z_t(e_s), the tangent gradient of the energy at each
+ * spin (c the leave-one-out coefficients, grad Z the tangent-projected gradient rows
+ * of src/gpu/grad_device.jl). config and grad: replicas x 3 x n_sites FP64 (payload
+ * order); spins are rounded to FP32 as in a chain, c is accumulated in FP32 and the
+ * gradient rows and the sum are FP64. No colouring: one launch over every site. */
+int32_t scemc_energy_gradient(const scemc_tables* t, const double* config, int32_t replicas, double* grad);
+
 /* Registers a learned proposal network with a batch (m = NULL unregisters). env:
  * for every table of the batch in order, n_sites x k 0-based site ids, the sites
  * whose spins (in that order) form a site's network input; k must be 14 and no

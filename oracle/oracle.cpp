@@ -202,6 +202,48 @@ inline void zlm_row(int lmax, const double* u, double* z) {  // zlm_device.jl:12
     for (int m = -l; m <= l; ++m) z[i++] = zlm_one(l, m, u, cache);
 }
 
+// Tangent-projected gradient of Z_lm at u — src/gpu/grad_device.jl:27-67 (the
+// device twin of Harmonics.grad_Zlm_unsafe): d^{n+1}P_l is +0 when l < n + 1; the
+// radial part (u . dZ) u / |u|^2 is removed.
+inline void grad_zlm_one(int l, int m, const double* u, double* cache, double* g) {
+  const double x = u[0], y = u[1], z = u[2];
+  const int n = m < 0 ? -m : m;
+  const double par = (n & 1) ? -1.0 : 1.0;
+  const double plm = par * plm_norm(l, n) * dnpl(z, l, n, cache);
+  const double dplm = par * plm_norm(l, n) * (l < n + 1 ? 0.0 : dnpl(z, l, n + 1, cache));
+  const double r2 = x * x + y * y + z * z;
+  if (m == 0) {
+    const double zz = z * dplm / r2;
+    g[0] = -x * zz;
+    g[1] = -y * zz;
+    g[2] = dplm - z * zz;
+    return;
+  }
+  const double c = par * std::sqrt(2.0);
+  const Cx zpn = cpow(Cx{x, y}, n), zpn1 = cpow(Cx{x, y}, n - 1);
+  double dx, dy, dz;
+  if (m > 0) {
+    dx = c * n * plm * zpn1.re;
+    dy = -c * n * plm * zpn1.im;
+    dz = c * dplm * zpn.re;
+  } else {
+    dx = c * n * plm * zpn1.im;
+    dy = c * n * plm * zpn1.re;
+    dz = c * dplm * zpn.im;
+  }
+  const double zz = (x * dx + y * dy + z * dz) / r2;
+  g[0] = dx - x * zz;
+  g[1] = dy - y * zz;
+  g[2] = dz - z * zz;
+}
+
+inline void grad_zlm_row(int lmax, const double* u, double* g) {  // grad_device.jl:77-89, component-fastest
+  double cache[16];
+  int i = 0;
+  for (int l = 0; l <= lmax; ++l)
+    for (int m = -l; m <= l; ++m, ++i) grad_zlm_one(l, m, u, cache, g + 3 * i);
+}
+
 inline int lm_index0(int l, int m) { return l * l + l + m; }  // Harmonics.lm_index - 1
 
 // ---------------------------------------------------------------------------
@@ -1190,6 +1232,31 @@ double or_total_energy(void* h, const double* zrows) { return total_energy(*stat
 
 double or_total_energy_ref(void* h, const double* zrows) {
   return total_energy_ref(*static_cast<Ham*>(h), zrows);
+}
+
+void or_grad_zlm_row(int lmax, const double* u, double* g) { grad_zlm_row(lmax, u, g); }
+
+// All-site energy gradient (gpu_gradient.jl:131-243 semantics): G[s] = sum_t c_t(s)
+// grad Z_t(e_s), c the leave-one-out coefficients of site s (energy.jl:100-139);
+// config and G are 3 x n_sites (payload order).
+void or_energy_gradient(void* h, const double* config, double* G) {
+  const Ham& H = *static_cast<Ham*>(h);
+  std::vector<double> zr((size_t)H.nlm * H.n_sites), c(H.nlm), g(3 * (size_t)H.nlm);
+  zrows_of(H, config, zr.data());
+  for (int s = 0; s < H.n_sites; ++s) {
+    std::fill(c.begin(), c.end(), 0.0);
+    site_coeffs(H, s + 1, zr.data(), c.data());
+    grad_zlm_row(H.lmax, config + 3 * (size_t)s, g.data());
+    double gx = 0.0, gy = 0.0, gz = 0.0;
+    for (int t = 0; t < H.nlm; ++t) {
+      gx += c[t] * g[3 * t];
+      gy += c[t] * g[3 * t + 1];
+      gz += c[t] * g[3 * t + 2];
+    }
+    G[3 * (size_t)s] = gx;
+    G[3 * (size_t)s + 1] = gy;
+    G[3 * (size_t)s + 2] = gz;
+  }
 }
 
 void or_site_coeffs(void* h, int s, const double* zrows, double* c) {

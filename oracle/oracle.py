@@ -46,6 +46,8 @@ def lib() -> C.CDLL:
             "or_keyed_proposal": (None, [C.c_uint64, C.c_int32, C.c_int32, F64P, C.c_double, F64P, F64P]),
             "or_rotate": (None, [F64P, F64P, C.c_double, F64P]),
             "or_zlm_row": (None, [C.c_int, F64P, F64P]),
+            "or_grad_zlm_row": (None, [C.c_int, F64P, F64P]),
+            "or_energy_gradient": (None, [C.c_void_p, F64P, F64P]),
             "or_cpow": (None, [C.c_double, C.c_double, C.c_int, F64P]),
             "or_ham_build": (C.c_void_p, [C.c_int, C.c_int, F64P, I32P, I32P, I32P, I32P, F64P, I32P, F64P, F64P]),
             "or_ham_free": (None, [C.c_void_p]),
@@ -102,6 +104,14 @@ def philox_block(seed, site, sweep, slot, tag=0):
     out = np.zeros(4, np.uint32)
     lib().or_philox_block(C.c_uint64(seed), site, sweep, slot, tag, _p(out, C.c_uint32))
     return tuple(int(x) for x in out)
+
+
+def grad_zlm_row(lmax, u):
+    """Tangent gradients of the tesseral row at u: ((lmax+1)^2, 3)."""
+    uu = np.ascontiguousarray(u, dtype=np.float64)
+    g = np.zeros(((lmax + 1) ** 2, 3))
+    lib().or_grad_zlm_row(int(lmax), _p(uu, C.c_double), _p(g, C.c_double))
+    return g
 
 
 def philox_uniform(hi, lo):
@@ -222,6 +232,13 @@ class OracleHamiltonian:
     def total_energy_ref(self, config):
         z = self.zrows(config)
         return lib().or_total_energy_ref(self.h, _p(z, C.c_double))
+
+    def energy_gradient(self, config):
+        """All-site tangent gradient G[s] = sum_t c_t(s) grad Z_t(e_s) (n_sites x 3)."""
+        cfg = np.ascontiguousarray(config, dtype=np.float64).reshape(self.n_sites, 3)
+        G = np.zeros((self.n_sites, 3))
+        lib().or_energy_gradient(self.h, _p(cfg, C.c_double), _p(G, C.c_double))
+        return G
 
     def site_coeffs(self, s, zrows, ref=False):
         z = np.ascontiguousarray(zrows, dtype=np.float64)

@@ -95,6 +95,7 @@ SIGNATURES = [
     ("scemc_batch_profile", C.c_int32, [C.c_void_p, C.c_int32]),
     ("scemc_batch_kernel_time", C.c_int32, [C.c_void_p, F64P, I64P]),
     ("scemc_batch_launches", C.c_int32, [C.c_void_p, I64P]),
+    ("scemc_energy_gradient", C.c_int32, [C.c_void_p, F64P, C.c_int32, F64P]),
     ("scemc_batch_set_learned", C.c_int32, [C.c_void_p, C.c_void_p, I32P, C.c_int32]),
     ("scemc_batch_fetch_record_ratio", C.c_int32, [C.c_void_p, F64P]),
     ("scemc_mlp_create", C.c_int32, [C.c_uint64, C.POINTER(C.c_void_p)]),

@@ -1262,7 +1262,10 @@ __device__ __forceinline__ void learned_layer(uint32_t tmem_d, const uint8_t* A,
   umma::commit(mbar);
 }
 
-__global__ void __launch_bounds__(128) k_learned_fused(SweepArgs a, LearnedNet net, double* lqr) {
+// Two warpgroups per CTA: both gather half of a row's environment and each runs the
+// epilogue of half the hidden columns (a warp reads TMEM lanes 32 (warp % 4) ..);
+// warpgroup 0 reads the 20 outputs and draws for its rows.
+__global__ void __launch_bounds__(256) k_learned_fused(SweepArgs a, LearnedNet net, double* lqr) {
   extern __shared__ __align__(1024) uint8_t lsm[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(lsm) + 1023) & ~(uintptr_t)1023);
   uint8_t* sW1 = base;
@@ -1274,6 +1277,7 @@ __global__ void __launch_bounds__(128) k_learned_fused(SweepArgs a, LearnedNet n
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tslot;
   const int tid = threadIdx.x, warp = tid >> 5;
+  const int row = tid & 127, wg = tid >> 7;
   const int col = a.colour;
   const int32_t* seg_c = a.seg + (size_t)col * (a.n_lat + 1);
   const int n_items = seg_c[a.n_lat];
@@ -1294,37 +1298,46 @@ __global__ void __launch_bounds__(128) k_learned_fused(SweepArgs a, LearnedNet n
   __syncthreads();
   umma::fence_after();
   const uint32_t tmem = tslot;
-  const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+  const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
   uint32_t phase = 0;
   bool ok = true;
   for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
-    const int item = tile * kTile + tid;
+    const int item = tile * kTile + row;
     const bool valid = item < n_items;
     int li = 0, q = 0, r = 0, s = 0;
     float4 e = make_float4(0.f, 0.f, 1.f, 0.f);
     float tau = 1.0f;
-    alignas(16) __nv_bfloat16 x[vmf::kInPad];
+    // warpgroup 0: environment spins 0..7 -> input columns 0..23 (chunks 0..2);
+    // warpgroup 1: spins 8..13 and kT -> columns 24..42 (chunks 3..5), chunks 6, 7 zero
+    alignas(16) __nv_bfloat16 x[24];
 #pragma unroll
-    for (int k = 0; k < vmf::kInPad; ++k) x[k] = __float2bfloat16_rn(0.0f);
+    for (int k = 0; k < 24; ++k) x[k] = __float2bfloat16_rn(0.0f);
     if (valid) {
       item_of(a, seg_c, item, li, q, r);
       const DevLattice& L = a.lat[li];
       s = L.color_sites[L.color_ptr[col] + q];
       const float4* sp = a.spins + L.spin_off;
       const int32_t* env = L.env + (int64_t)s * L.env_k;
-      for (int k = 0; k < 14; ++k) {
-        const float4 v = __ldg(sp + (int64_t)__ldg(env + k) * L.R + r);
-        x[3 * k] = __float2bfloat16_rn(v.x);
-        x[3 * k + 1] = __float2bfloat16_rn(v.y);
-        x[3 * k + 2] = __float2bfloat16_rn(v.z);
-      }
       tau = slot_kt_mev(a, L.slot0 + r);
-      x[42] = __float2bfloat16_rn(tau);
-      e = sp[(int64_t)s * L.R + r];
+      const int k0 = wg ? 8 : 0, k1 = wg ? 14 : 8;
+      for (int k = k0; k < k1; ++k) {
+        const float4 v = __ldg(sp + (int64_t)__ldg(env + k) * L.R + r);
+        x[3 * (k - k0)] = __float2bfloat16_rn(v.x);
+        x[3 * (k - k0) + 1] = __float2bfloat16_rn(v.y);
+        x[3 * (k - k0) + 2] = __float2bfloat16_rn(v.z);
+      }
+      if (wg) x[18] = __float2bfloat16_rn(tau);
+      else e = sp[(int64_t)s * L.R + r];
     }
 #pragma unroll
-    for (int kg = 0; kg < 8; ++kg)
-      *reinterpret_cast<uint4*>(sX + umma::kmajor_offset(tid, kg * 8, 64)) = reinterpret_cast<const uint4*>(x)[kg];
+    for (int kg = 0; kg < 3; ++kg)
+      *reinterpret_cast<uint4*>(sX + umma::kmajor_offset(row, (3 * wg + kg) * 8, 64)) =
+          reinterpret_cast<const uint4*>(x)[kg];
+    if (wg) {
+      const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+      *reinterpret_cast<uint4*>(sX + umma::kmajor_offset(row, 48, 64)) = z;
+      *reinterpret_cast<uint4*>(sX + umma::kmajor_offset(row, 56, 64)) = z;
+    }
     umma::fence_async_smem();
     umma::fence_before();
     __syncthreads();
@@ -1333,7 +1346,7 @@ __global__ void __launch_bounds__(128) k_learned_fused(SweepArgs a, LearnedNet n
     ok = umma::mbar_wait(&mbar, phase, 1000000000ull);
     phase ^= 1u;
     umma::fence_after();
-    for (int c0 = 0; c0 < 128; c0 += 8) {
+    for (int c0 = 64 * wg; c0 < 64 * wg + 64; c0 += 8) {
       float v[8];
       umma::tmem_ld8(tmem + lane_base + (uint32_t)c0, v);
       alignas(16) __nv_bfloat16 h[8];
@@ -1342,7 +1355,7 @@ __global__ void __launch_bounds__(128) k_learned_fused(SweepArgs a, LearnedNet n
         const float z = v[i] + sb[c0 + i];
         h[i] = __float2bfloat16_rn(z / (1.0f + __expf(-z)));
       }
-      *reinterpret_cast<uint4*>(sH + (c0 >> 6) * kChunkBytes + umma::kmajor_offset(tid, c0 & 63, 64)) =
+      *reinterpret_cast<uint4*>(sH + (c0 >> 6) * kChunkBytes + umma::kmajor_offset(row, c0 & 63, 64)) =
           *reinterpret_cast<const uint4*>(h);
     }
     umma::fence_async_smem();
@@ -1353,7 +1366,7 @@ __global__ void __launch_bounds__(128) k_learned_fused(SweepArgs a, LearnedNet n
     ok = ok && umma::mbar_wait(&mbar, phase, 1000000000ull);
     phase ^= 1u;
     umma::fence_after();
-    for (int c0 = 0; c0 < 128; c0 += 8) {
+    for (int c0 = 64 * wg; c0 < 64 * wg + 64; c0 += 8) {
       float v[8];
       umma::tmem_ld8(tmem + lane_base + 128u + (uint32_t)c0, v);
       alignas(16) __nv_bfloat16 h[8];
@@ -1362,7 +1375,7 @@ __global__ void __launch_bounds__(128) k_learned_fused(SweepArgs a, LearnedNet n
         const float z = v[i] + sb[128 + c0 + i];
         h[i] = __float2bfloat16_rn(z / (1.0f + __expf(-z)));
       }
-      *reinterpret_cast<uint4*>(sH + (c0 >> 6) * kChunkBytes + umma::kmajor_offset(tid, c0 & 63, 64)) =
+      *reinterpret_cast<uint4*>(sH + (c0 >> 6) * kChunkBytes + umma::kmajor_offset(row, c0 & 63, 64)) =
           *reinterpret_cast<const uint4*>(h);
     }
     umma::fence_async_smem();
@@ -1374,11 +1387,13 @@ __global__ void __launch_bounds__(128) k_learned_fused(SweepArgs a, LearnedNet n
     phase ^= 1u;
     umma::fence_after();
     float o[32];
+    if (wg == 0) {
 #pragma unroll
-    for (int c0 = 0; c0 < 32; c0 += 8) umma::tmem_ld8(tmem + lane_base + (uint32_t)c0, o + c0);
+      for (int c0 = 0; c0 < 32; c0 += 8) umma::tmem_ld8(tmem + lane_base + (uint32_t)c0, o + c0);
+    }
     umma::fence_before();
     __syncthreads();  // every thread has read TMEM and the tiles before the next tile reuses them
-    if (!valid || !ok) continue;
+    if (wg != 0 || !valid || !ok) continue;
 #pragma unroll
     for (int j = 0; j < 32; ++j) o[j] += sb[256 + j];
     const DevLattice& L = a.lat[li];
@@ -2550,7 +2565,7 @@ int32_t run_learned_pass(scemc_ensemble* E, const Launch& Lc) {
     a.lqr = nullptr;
     const int tiles = (n + kTile - 1) / kTile;
     ++E->launches;
-    k_learned_fused<<<(unsigned)std::min(tiles, 2 * sm_count(E->device)), 128, kLearnedSmem, E->stream>>>(
+    k_learned_fused<<<(unsigned)std::min(tiles, 2 * sm_count(E->device)), 256, kLearnedSmem, E->stream>>>(
         a, net, E->d_lqr);
     CUDA_TRY(cudaGetLastError());
     a.lqr = E->d_lqr;
@@ -3607,6 +3622,119 @@ __global__ void k_energy_fold_static(const double* partial, int n_chunks, int R,
 }
 
 }  // namespace
+
+namespace {
+// All-site energy gradient (gpu_gradient.jl:131-243 semantics): G lanes per (site,
+// replica) walk the site's records for its leave-one-out coefficients c (FP32, the
+// sweep's walk); lane 0 forms G = sum_t c_t grad Z_t(e) with FP64 tangent gradient
+// rows. Read-only in the spins, one launch over every site (no colouring).
+template <int LMAX, int G>
+__global__ void __launch_bounds__(256) k_energy_gradient(DevLattice L, const float4* spins, int R, double* grad) {
+  constexpr int NLM = (LMAX + 1) * (LMAX + 1);
+  const int lane = threadIdx.x % G;
+  const int group = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const int n_groups = (gridDim.x * blockDim.x) / G;
+  const int64_t n_items = (int64_t)L.n_sites * R;
+  const unsigned int gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x % 32) / G * G));
+  const int64_t rounds = (n_items + n_groups - 1) / n_groups;
+  for (int64_t rd = 0; rd < rounds; ++rd) {
+    const int64_t item = rd * n_groups + group;
+    const bool valid = item < n_items;
+    const int s = valid ? (int)(item / R) : 0, r = valid ? (int)(item % R) : 0;
+    float c[NLM];
+#pragma unroll
+    for (int k = 0; k < NLM; ++k) c[k] = 0.0f;
+    if (valid) accumulate_c<LMAX, G, false>(L, spins, R, r, s, lane, c);
+#pragma unroll
+    for (int o = G / 2; o >= 1; o >>= 1)
+#pragma unroll
+      for (int k = 0; k < NLM; ++k) c[k] += __shfl_xor_sync(gmask, c[k], o);
+    if (!valid || lane != 0) continue;
+    const float4 e = spins[(int64_t)s * R + r];
+    double gx = 0.0, gy = 0.0, gz = 0.0;
+    for (int t = 0; t < NLM; ++t) {
+      if (c[t] == 0.0f) continue;
+      int l, m;
+      row_lm(t, l, m);
+      double g[3];
+      grad_zlm_f64(l, m, e.x, e.y, e.z, g);
+      gx += (double)c[t] * g[0];
+      gy += (double)c[t] * g[1];
+      gz += (double)c[t] * g[2];
+    }
+    double* out = grad + ((int64_t)r * L.n_sites + s) * 3;
+    out[0] = gx;
+    out[1] = gy;
+    out[2] = gz;
+  }
+}
+
+using GradFn = void (*)(DevLattice, const float4*, int, double*);
+GradFn gradient_kernel(int lmax) {
+  switch (lmax) {
+    case 0: return k_energy_gradient<0, 8>;
+    case 1: return k_energy_gradient<1, 8>;
+    case 2: return k_energy_gradient<2, 8>;
+    case 3: return k_energy_gradient<3, 8>;
+    case 4: return k_energy_gradient<4, 8>;
+    case 5: return k_energy_gradient<5, 8>;
+    default: return k_energy_gradient<6, 8>;
+  }
+}
+
+__global__ void k_config_to_spins(const double* cfg, int64_t n, float4* spins) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    spins[i] = make_float4((float)cfg[3 * i], (float)cfg[3 * i + 1], (float)cfg[3 * i + 2], 0.0f);
+}
+}  // namespace
+
+// config: replicas x (3 x n_sites) FP64 host (payload order); grad the same shape.
+// The spins are rounded to FP32 as in a chain.
+extern "C" int32_t scemc_energy_gradient(const scemc_tables* t, const double* config, int32_t replicas,
+                                         double* grad) {
+  if (!t || !config || !grad) return fail(SCEMC_ERR_ARG, "NULL argument");
+  if (replicas < 1) return fail(SCEMC_ERR_ARG, "replicas must be >= 1");
+  if (!t->has_generic) return fail(SCEMC_ERR_UNSUPPORTED, "generic records were not kept for these tables");
+  const int64_t n = (int64_t)t->n_sites * replicas;
+  for (int64_t i = 0; i < 3 * n; ++i)
+    if (!std::isfinite(config[i])) return fail(SCEMC_ERR_NUMERIC, "non-finite spin component");
+  // device layout spins[site * R + r]: transpose the replica-major host payload
+  std::vector<double> cfg((size_t)3 * n);
+  for (int32_t r = 0; r < replicas; ++r)
+    for (int32_t s = 0; s < t->n_sites; ++s)
+      for (int d = 0; d < 3; ++d)
+        cfg[((size_t)s * replicas + r) * 3 + d] = config[((size_t)r * t->n_sites + s) * 3 + d];
+  double *d_cfg = nullptr, *d_grad = nullptr;
+  float4* d_spins = nullptr;
+  int32_t rc = SCEMC_OK;
+  if ((rc = dalloc(&d_cfg, (size_t)3 * n)) || (rc = dalloc(&d_grad, (size_t)3 * n)) ||
+      (rc = dalloc(&d_spins, (size_t)n))) {
+    cudaFree(d_cfg);
+    cudaFree(d_grad);
+    cudaFree(d_spins);
+    return rc;
+  }
+  auto done = [&](int32_t r) {
+    cudaFree(d_cfg);
+    cudaFree(d_grad);
+    cudaFree(d_spins);
+    return r;
+  };
+  if (cudaMemcpy(d_cfg, cfg.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice) != cudaSuccess)
+    return done(fail(SCEMC_ERR_CUDA, "config upload"));
+  k_config_to_spins<<<(unsigned)std::min<int64_t>(1024, (n + 255) / 256), 256>>>(d_cfg, n, d_spins);
+  DevLattice L = t->dl;
+  L.R = replicas;
+  L.spin_off = 0;
+  const int G = 8;
+  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sm_count(t->device) * 8, (n * G + 255) / 256));
+  gradient_kernel(t->lmax)<<<blocks, 256>>>(L, d_spins, replicas, d_grad);
+  if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess)
+    return done(fail(SCEMC_ERR_CUDA, "gradient kernel"));
+  if (cudaMemcpy(grad, d_grad, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return done(fail(SCEMC_ERR_CUDA, "gradient download"));
+  return done(SCEMC_OK);
+}
 
 extern "C" int32_t scemc_total_energy_static(const scemc_tables* t, const void* spins, int32_t replicas,
                                              double* energies, void* stream) {

@@ -128,13 +128,9 @@ __device__ __forceinline__ void zrow_l2(float x, float y, float z, float* o) {
   o[4] = kC22 * (x * x - y * y);
 }
 
-// General tesseral value Z_lm for l <= 6 (zlm_device.jl:20-109 in precision T).
+// d^n P_l(z)/dz^n for n <= l <= 6 by the zlm_device.jl:66-98 recursion (precision T).
 template <typename T>
-__device__ __forceinline__ T zlm_general(int l, int m, T x, T y, T z) {
-  const int n = m < 0 ? -m : m;
-  T acc = (T)(2 * l + 1) / (T)12.566370614359172;
-  for (int i = l - n + 1; i <= l + n; ++i) acc /= (T)i;
-  const T norm = sqrt(acc);
+__device__ __forceinline__ T dnpl_t(int l, int n, T z) {
   T cache[8];
   if (n == l) {
     T p = (T)1;
@@ -161,8 +157,22 @@ __device__ __forceinline__ T zlm_general(int l, int m, T x, T y, T z) {
                          (T)li;
     }
   }
+  return cache[l - n];
+}
+
+template <typename T>
+__device__ __forceinline__ T plm_norm_t(int l, int n) {
+  T acc = (T)(2 * l + 1) / (T)12.566370614359172;
+  for (int i = l - n + 1; i <= l + n; ++i) acc /= (T)i;
+  return sqrt(acc);
+}
+
+// General tesseral value Z_lm for l <= 6 (zlm_device.jl:20-109 in precision T).
+template <typename T>
+__device__ __forceinline__ T zlm_general(int l, int m, T x, T y, T z) {
+  const int n = m < 0 ? -m : m;
   const T par = (n & 1) ? (T)-1 : (T)1;
-  const T plm = par * norm * cache[l - n];
+  const T plm = par * plm_norm_t<T>(l, n) * dnpl_t<T>(l, n, z);
   if (n == 0) return plm;
   const T c = par * sqrt((T)2) * plm;
   T re = (T)1, im = (T)0;  // (x + iy)^n by repeated multiplication
@@ -172,6 +182,47 @@ __device__ __forceinline__ T zlm_general(int l, int m, T x, T y, T z) {
     re = nr;
   }
   return m > 0 ? c * re : c * im;
+}
+
+// Tangent-projected gradient of Z_lm at u (grad_device.jl:27-67), FP64: the
+// Cartesian derivative of par*norm*d^nP_l(z)*sqrt2*Re/Im((x+iy)^n) with the radial
+// part (u . dZ) u / |u|^2 removed.
+__device__ __forceinline__ void grad_zlm_f64(int l, int m, double x, double y, double z, double* g) {
+  const int n = m < 0 ? -m : m;
+  const double par = (n & 1) ? -1.0 : 1.0;
+  const double nrm = plm_norm_t<double>(l, n);
+  const double plm = par * nrm * dnpl_t<double>(l, n, z);
+  const double dplm = par * nrm * (l < n + 1 ? 0.0 : dnpl_t<double>(l, n + 1, z));
+  const double r2 = x * x + y * y + z * z;
+  if (m == 0) {
+    const double zz = z * dplm / r2;
+    g[0] = -x * zz;
+    g[1] = -y * zz;
+    g[2] = dplm - z * zz;
+    return;
+  }
+  const double c = par * sqrt(2.0);
+  double re = 1.0, im = 0.0, re1 = 1.0, im1 = 0.0;  // (x + iy)^n and (x + iy)^(n - 1)
+  for (int k = 0; k < n; ++k) {
+    re1 = re, im1 = im;
+    const double nr = re * x - im * y;
+    im = re * y + im * x;
+    re = nr;
+  }
+  double dx, dy, dz;
+  if (m > 0) {
+    dx = c * n * plm * re1;
+    dy = -c * n * plm * im1;
+    dz = c * dplm * re;
+  } else {
+    dx = c * n * plm * im1;
+    dy = c * n * plm * re1;
+    dz = c * dplm * im;
+  }
+  const double zz = (x * dx + y * dy + z * dz) / r2;
+  g[0] = dx - x * zz;
+  g[1] = dy - y * zz;
+  g[2] = dz - z * zz;
 }
 
 // Row index -> (l, m).

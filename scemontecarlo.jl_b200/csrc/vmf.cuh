@@ -133,14 +133,14 @@ struct MixF {
   float kappa[kComp];
 };
 
-__device__ inline float softplus_f(float x) { return x > 20.0f ? x : log1pf(expf(x)); }
+__device__ inline float softplus_f(float x) { return x > 20.0f ? x : log1pf(__expf(x)); }
 
 __device__ inline void mixture_f(const float* o, float tau, MixF& m) {
   float amax = o[0];
   for (int k = 1; k < kComp; ++k) amax = fmaxf(amax, o[5 * k]);
   float s = 0.0f;
-  for (int k = 0; k < kComp; ++k) s += expf(o[5 * k] - amax);
-  const float lse = amax + logf(s);
+  for (int k = 0; k < kComp; ++k) s += __expf(o[5 * k] - amax);
+  const float lse = amax + __logf(s);
   for (int k = 0; k < kComp; ++k) {
     m.logpi[k] = o[5 * k] - lse;
     const float x = o[5 * k + 1], y = o[5 * k + 2], z = o[5 * k + 3];
@@ -157,24 +157,24 @@ __device__ inline float log_q_f(const MixF& m, float x0, float x1, float x2) {
   for (int k = 0; k < kComp; ++k) {
     const float d = m.mu[k][0] * x0 + m.mu[k][1] * x1 + m.mu[k][2] * x2;
     const float kap = m.kappa[k];
-    l[k] = m.logpi[k] + logf(kap) - logf((float)kTwoPi) - logf(-expm1f(-2.0f * kap)) + kap * (d - 1.0f);
+    l[k] = m.logpi[k] + __logf(kap) - __logf((float)kTwoPi) - __logf(-expm1f(-2.0f * kap)) + kap * (d - 1.0f);
     lm = fmaxf(lm, l[k]);
   }
   float s = 0.0f;
-  for (int k = 0; k < kComp; ++k) s += expf(l[k] - lm);
-  return lm + logf(s);
+  for (int k = 0; k < kComp; ++k) s += __expf(l[k] - lm);
+  return lm + __logf(s);
 }
 
 // the draw of sample() in single precision (same inverse CDFs and frame)
 __device__ inline void sample_f(const MixF& m, float u_comp, float u_w, float u_phi, float* out) {
   int k = 0;
-  float acc = expf(m.logpi[0]);
+  float acc = __expf(m.logpi[0]);
   while (k < kComp - 1 && u_comp >= acc) {
     ++k;
-    acc += expf(m.logpi[k]);
+    acc += __expf(m.logpi[k]);
   }
   const float kap = m.kappa[k];
-  float w = 1.0f + logf(u_w + (1.0f - u_w) * expf(-2.0f * kap)) / kap;
+  float w = 1.0f + __logf(u_w + (1.0f - u_w) * __expf(-2.0f * kap)) / kap;
   w = fminf(1.0f, fmaxf(-1.0f, w));
   const float v = sqrtf(fmaxf(0.0f, 1.0f - w * w));
   const float* mu = m.mu[k];

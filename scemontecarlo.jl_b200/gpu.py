@@ -177,6 +177,18 @@ def from_host(gst: GPUChainState, st: ChainState) -> GPUChainState:
     return gst
 
 
+def gpu_energy_gradient(gH: GPUTiledHamiltonian, config) -> np.ndarray:
+    """All-site energy gradient (gpu_energy_gradient!, gpu_gradient.jl:193-231): the
+    tangent gradient of the energy at every spin, (n_sites, 3) for one configuration
+    or (R, n_sites, 3) for a stack of R configurations."""
+    cfg = np.ascontiguousarray(config, np.float64)
+    one = cfg.ndim == 2
+    cfg = cfg.reshape(-1, gH.n_sites, 3)
+    out = np.zeros_like(cfg)
+    check(_lib.lib().scemc_energy_gradient(gH.h, ptr(cfg, C.c_double), cfg.shape[0], ptr(out, C.c_double)))
+    return out[0] if one else out
+
+
 def gpu_run_sweeps(gst: GPUChainState, gH: GPUTiledHamiltonian, st: ChainState, beta: float, nsweeps: int,
                    renorm_interval: int = 1000, workgroupsize: int = 32) -> GPUChainState:
     """nsweeps device Metropolis sweeps with a device renormalisation + FP64 recompute

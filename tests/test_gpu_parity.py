@@ -508,3 +508,20 @@ def test_launch_count_matches_the_launch_form(gpu):
     n0 = b.launches()
     b.run(2, or_per_metropolis=1, mode=2, kernel=2, proposals=2)  # one persistent launch per pass + tail
     assert b.launches() - n0 == 2 * 3
+
+
+@pytest.mark.parametrize("name", ["dimer_zeeman", "biquadratic_zeeman", "mixed", "high_l", "fourbody",
+                                  "bcc_l2_plaq_zeeman", "fcc_l2_tri_zeeman"])
+def test_energy_gradient_matches_oracle(gpu, name):
+    """The all-site tangent gradient (gpu_energy_gradient!) against the FP64 oracle on
+    the same FP32-rounded spins: FP32 coefficients, FP64 gradient rows."""
+    H, OH = build(name)
+    gH = scemc.GPUTiledHamiltonian(H)
+    cfgs = np.stack([rand_cfg(H.n_sites, 60 + r) for r in range(3)])
+    G = scemc.gpu_energy_gradient(gH, cfgs)
+    assert G.shape == cfgs.shape
+    for r in range(3):
+        ref = OH.energy_gradient(cfgs[r].astype(np.float32).astype(np.float64))
+        tol = 2e-5 * np.abs(ref).max() + 1e-30
+        assert np.abs(G[r] - ref).max() <= tol, (name, r, np.abs(G[r] - ref).max(), tol)
+    np.testing.assert_allclose(scemc.gpu_energy_gradient(gH, cfgs[1]), G[1])

@@ -334,3 +334,38 @@ def test_logbinner_tau_of_ar1():
     assert b.mean()[0] == pytest.approx(m, rel=1e-12, abs=1e-15)
     assert b.std_error()[0] == pytest.approx(err, rel=1e-9)
     assert b.tau_int()[0] == pytest.approx(tau, rel=1e-9)
+
+
+def test_gradient_row_and_all_site_gradient_match_finite_differences():
+    """The tangent gradient of every tesseral row (grad_device.jl:27-67) and the
+    all-site energy gradient (gpu_gradient.jl semantics) against central finite
+    differences along the two tangent directions of each spin."""
+    rng = np.random.default_rng(3)
+    for lmax in (1, 2, 4, 6):
+        u = rng.standard_normal(3)
+        u /= np.linalg.norm(u)
+        g = O.grad_zlm_row(lmax, u)
+        assert np.allclose(g @ u, 0.0, atol=1e-12)  # tangent
+        t1 = np.cross(u, [1.0, 0.0, 0.0])
+        t1 /= np.linalg.norm(t1)
+        t2 = np.cross(u, t1)
+        h = 1e-6
+        for t in (t1, t2):
+            zp = O.zlm_row(lmax, (u + h * t) / np.linalg.norm(u + h * t))
+            zm = O.zlm_row(lmax, (u - h * t) / np.linalg.norm(u - h * t))
+            np.testing.assert_allclose(g @ t, (zp - zm) / (2 * h), atol=2e-7, rtol=1e-6)
+    from scemc import models
+    OH = O.OracleHamiltonian(2, models.config2_bcc_l2().terms, (2, 2, 2), magmoms=[2.0, 2.0], field=[0, 0, 1.0])
+    cfg = models.random_config(OH.n_sites, 4)
+    G = OH.energy_gradient(cfg)
+    h = 1e-6
+    for s in (0, 5, 11):
+        e = cfg[s]
+        t1 = np.cross(e, [0.0, 1.0, 0.0])
+        t1 /= np.linalg.norm(t1)
+        for t in (t1, np.cross(e, t1)):
+            cp, cm = cfg.copy(), cfg.copy()
+            cp[s] = (e + h * t) / np.linalg.norm(e + h * t)
+            cm[s] = (e - h * t) / np.linalg.norm(e - h * t)
+            fd = (OH.total_energy(cp) - OH.total_energy(cm)) / (2 * h)
+            assert G[s] @ t == pytest.approx(fd, rel=1e-5, abs=1e-10)
