@@ -177,7 +177,10 @@ typedef struct scemc_run_params {
   int32_t lanes_per_site;    /* 0 = autotuned */
   int32_t mode;              /* 0 = auto (autotuned if scemc_batch_autotune ran, else 2), 1 = one launch per
                                 colour, 2 = persistent grid kernel per pass, 3 = per-colour launches of a
-                                compound sweep captured once in a CUDA graph and replayed */
+                                compound sweep captured once in a CUDA graph and replayed, 4 = persistent
+                                data-flow kernel per pass (row-parallel kernel; an item waits for the
+                                completion flags of its earlier-colour neighbours instead of a grid barrier
+                                between colours) */
   /* Phase bookkeeping (the reference's lane.phase_sweeps): sweep i of this call is
    * sweep phase_done + i of its phase; adaptation, renormalisation, measurement and
    * exchange fire on that count, and no exchange follows the phase's last sweep

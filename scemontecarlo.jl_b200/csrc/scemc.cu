@@ -130,6 +130,7 @@ struct DevLattice {
   // learned proposal: environment of every site (n_sites x env_k, 0-based), per batch
   const int32_t* env;
   int32_t env_k, pad3;
+  const int16_t* site_colour;  // 1-based colour of every site, 0 = inactive
 };
 
 // Grid barrier state (one per ensemble).
@@ -178,6 +179,7 @@ struct SweepArgs {
   double* propu;
   const double* lqr;  // learned proposals: log q(e | env) - log q(e' | env) per item (null otherwise)
   double* rec_lqr;
+  uint32_t* flags;    // data-flow form: per item slot, the pass epoch its update completed (null otherwise)
   int32_t dmax, rmax;
 };
 
@@ -194,6 +196,37 @@ __device__ __forceinline__ unsigned long long ld_acquire(const unsigned long lon
   unsigned long long v;
   asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
+}
+
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u32(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Data-flow form: the pass epoch of a sweep (distinct for every (sweep, pass) with at
+// most 6 overrelaxation passes; never 0, the flags' initial value).
+__device__ __forceinline__ uint32_t flow_epoch(uint32_t sweep, int pass) { return sweep * 8u + (uint32_t)(pass + 2); }
+
+// Waits until an item slot's flag holds `epoch`; bounded by limit_ns, after which the
+// error word is set and every later wait gives up at once.
+__device__ __forceinline__ bool wait_flag(const uint32_t* f, uint32_t epoch, int* err, long long limit_ns) {
+  if (ld_acquire_u32(f) == epoch) return true;
+  const unsigned long long t0 = globaltimer();
+  for (unsigned int it = 0;; ++it) {
+    if (ld_acquire_u32(f) == epoch) return true;
+    if ((it & 15u) == 15u) {
+      if (*(volatile int*)err) return false;
+      if ((long long)(globaltimer() - t0) > limit_ns) {
+        atomicExch(err, 1);
+        return false;
+      }
+    }
+    __nanosleep(20);
+  }
 }
 
 // Barrier across all blocks of a cooperative launch on a monotonically increasing
@@ -679,7 +712,11 @@ __device__ void fast_colour(const SweepArgs& a, int col, unsigned long long* s_d
     const bool have = item == pre.item;  // warp-uniform
     const int4 dsc = have ? pre.dsc : __ldg(L.idesc + __ldg(L.color_ptr + col) + q);
     const int s = dsc.x & 0x3fffffff;
-    if (do_or && !(dsc.x & (1 << 30))) continue;  // warp-uniform: no l = 1 channel
+    const uint32_t epoch = a.flags ? flow_epoch(a.st->sweep, a.pass) : 0u;
+    if (do_or && !(dsc.x & (1 << 30))) {  // warp-uniform: no l = 1 channel
+      if (a.flags && lane == 0) st_release_u32(a.flags + L.spin_off + (int64_t)s * R + r, epoch);
+      continue;
+    }
     const int slot = L.slot0 + r;
     const float4* __restrict__ sp = a.spins + L.spin_off;
     // independent loads of the item, issued before the table walk
@@ -708,6 +745,11 @@ __device__ void fast_colour(const SweepArgs& a, int col, unsigned long long* s_d
       for (int k = lane; k < nrec; k += 32) rb[k] = __ldg(L.frec + j0 + k);
       for (int k = lane; k < nd; k += 32) {
         const int nb = __ldg(L.nb_list + n0 + k);
+        if (a.flags) {  // a neighbour of an earlier colour must have finished this pass
+          const int cn = __ldg(L.site_colour + nb);
+          if (cn > 0 && cn <= col) wait_flag(a.flags + L.spin_off + (int64_t)nb * R + r, epoch, &a.gs->error,
+                                             a.barrier_limit_ns);
+        }
         const float4 v = load_spin<PERSIST>(sp + (int64_t)nb * R + r);
         zrow_nr<NR>(v.x, v.y, v.z, zb + k * NR);
       }
@@ -841,6 +883,7 @@ __device__ void fast_colour(const SweepArgs& a, int col, unsigned long long* s_d
       a.spins[L.spin_off + (int64_t)s * R + r] = make_float4(px, py, pz, 0.0f);
       atomicAdd(s_dE + slot, (unsigned long long)llrint((double)dE * kFixScale));
     }
+    if (a.flags) st_release_u32(a.flags + L.spin_off + (int64_t)s * R + r, epoch);  // after the spin store
     if (do_or) {
       if (attempted) atomicAdd(s_cnt + 3 * slot + 2, 1u);
       if (acc_ok) atomicAdd(s_cnt + 3 * slot + 1, 1u);
@@ -902,7 +945,7 @@ __global__ void SCEMC_FAST_BOUNDS k_fast_colour(SweepArgs a) {
 }
 
 template <int LMAX>
-__global__ void __launch_bounds__(256) k_fast_persistent(SweepArgs a) {
+__global__ void SCEMC_FAST_BOUNDS k_fast_persistent(SweepArgs a) {
   extern __shared__ __align__(16) float zsm[];
   __shared__ unsigned long long s_dE[kMaxSlots];
   __shared__ unsigned int s_cnt[3 * kMaxSlots];
@@ -917,6 +960,10 @@ __global__ void __launch_bounds__(256) k_fast_persistent(SweepArgs a) {
   FastPre pre;
   pre.item = -1;
   for (int col = 0; ok && col < a.max_colors; ++col) {
+    if (a.flags) {  // data flow: items wait on their earlier-colour neighbours' flags instead of a barrier
+      fast_colour<LMAX, true>(a, col, s_dE, s_cnt, zsm, pre, -1);
+      continue;
+    }
     fast_colour<LMAX, true>(a, col, s_dE, s_cnt, zsm, pre, col + 1 < a.max_colors ? col + 1 : -1);
     if (col + 1 < a.max_colors) ok = grid_barrier(a.gs, a.bar_base, k++, gridDim.x, a.barrier_limit_ns);
   }
@@ -1736,6 +1783,7 @@ struct scemc_ensemble {
   std::vector<int32_t*> d_env;
   double* d_lqr = nullptr;
   double* d_rlqr = nullptr;
+  uint32_t* d_flags = nullptr;  // data-flow form: per item slot completion epochs
   // row-parallel fast kernel
   bool fast = false;
   int32_t dmax = 0, rmax = 0;
@@ -1771,7 +1819,7 @@ struct scemc_ensemble {
     }
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
     for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
-    void* qs[] = {d_item_base, d_prop, d_propu, d_lqr, d_rlqr};
+    void* qs[] = {d_item_base, d_prop, d_propu, d_lqr, d_rlqr, d_flags};
     for (int32_t* p : d_env)
       if (p) cudaFree(p);
     for (void* p : qs)
@@ -2193,6 +2241,11 @@ int32_t compile_tables(const scemc_tables_desc* d, scemc_tables* T) {
   T->site_col_of.assign(ns, 0);
   for (int32_t c = 0; c < d->n_colors; ++c)
     for (int32_t q = cp[c]; q < cp[c + 1]; ++q) T->site_col_of[d->color_sites[q] - 1] = c + 1;
+  if (d->n_colors > 32767) return fail(SCEMC_ERR_UNSUPPORTED, "more than 32767 colours");
+  {
+    std::vector<int16_t> sc(T->site_col_of.begin(), T->site_col_of.end());
+    if ((r = upload(T->allocs, sc, &L.site_colour))) return r;
+  }
   T->active = active;
   T->n_sites = ns;
   T->nlm = d->nlm;
@@ -2475,6 +2528,7 @@ struct Launch {
   bool rep = false;   // replica-parallel kernel (one thread per item, per-colour launches)
   bool precompute = false;  // Metropolis proposals computed before the colour loop
   bool learned = false;     // Metropolis proposals from the learned network, per colour
+  bool flow = false;        // persistent form with per-item completion flags instead of grid barriers
 };
 
 using FastFn = void (*)(SweepArgs);
@@ -2661,10 +2715,19 @@ int32_t run_pass_impl(scemc_ensemble* E, int pass, const Launch& Lc) {
       if (a.prop) need = std::max<int64_t>(need, ((int64_t)E->item_base.back() + threads - 1) / threads);
       const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(E->coop_blocks, need));
       a.bar_base = E->bar_base;
+      if (Lc.flow) {
+        if (!E->d_flags) {
+          int32_t rc;
+          if ((rc = dalloc(&E->d_flags, (size_t)std::max<int64_t>(E->n_spins, 1)))) return rc;
+          CUDA_TRY(cudaMemsetAsync(E->d_flags, 0, sizeof(uint32_t) * std::max<int64_t>(E->n_spins, 1), E->stream));
+        }
+        a.flags = E->d_flags;
+      }
       void* params[] = {&a};
       ++E->launches;
       CUDA_TRY(cudaLaunchCooperativeKernel((const void*)fn, dim3(blocks), dim3(threads), params, smem, E->stream));
-      E->bar_base += (unsigned long long)blocks * ((a.prop ? 1 : 0) + std::max(E->max_colors - 1, 0));
+      E->bar_base +=
+          (unsigned long long)blocks * ((a.prop ? 1 : 0) + (Lc.flow ? 0 : std::max(E->max_colors - 1, 0)));
       return SCEMC_OK;
     }
     const int cap = sm_count(E->device) * 16;
@@ -2857,9 +2920,11 @@ int32_t resolve_launch(const scemc_ensemble* E, int lanes, int mode, int kernel,
     kernel = E->tuned_kernel;
     if (proposals == 0) proposals = E->tuned_proposals;
     if (lanes == 0) lanes = E->tuned_lanes;
-    if (proposals == 3 && mode == 2) mode = 3;  // learned passes run per colour
+    if (proposals == 3 && (mode == 2 || mode == 4)) mode = 3;  // learned passes run per colour
   }
-  if (mode < 0 || mode > 3) return fail(SCEMC_ERR_ARG, "mode must be 0..3");
+  if (mode < 0 || mode > 4) return fail(SCEMC_ERR_ARG, "mode must be 0..4");
+  if (mode == 4 && (!E->fast || kernel == 1 || kernel == 3 || proposals == 3))
+    return fail(SCEMC_ERR_ARG, "the data-flow form (mode 4) runs the row-parallel kernel with plain proposals");
   if (kernel < 0 || kernel > 3 || proposals < 0 || proposals > 3)
     return fail(SCEMC_ERR_ARG, "kernel must be 0..3 and proposals 0..3");
   if (proposals == 3) {
@@ -2889,6 +2954,12 @@ int32_t resolve_launch(const scemc_ensemble* E, int lanes, int mode, int kernel,
   if (L.mode == 3) {
     L.graph = true;
     L.mode = 1;
+  }
+  if (L.mode == 4) {
+    L.flow = true;
+    L.mode = 2;
+    L.rep = false;
+    L.fast = true;
   }
   L.G = lanes ? norm_lanes(lanes) : auto_lanes(E);
   if (L.learned) {
@@ -3218,7 +3289,7 @@ int32_t scemc_batch_run_async(scemc_batch* b, const scemc_run_params* p) {
     if (rc) return rc;
   }
   if (p->phase_done < 0 || p->phase_total < 0) return fail(SCEMC_ERR_ARG, "bad phase bookkeeping");
-  if (p->mode < 0 || p->mode > 3) return fail(SCEMC_ERR_ARG, "mode must be 0..3");
+  if (p->mode < 0 || p->mode > 4) return fail(SCEMC_ERR_ARG, "mode must be 0..4");
   const int64_t total = p->phase_total > 0 ? p->phase_total : p->phase_done + p->nsweeps;
   int32_t rc;
   Launch L;
@@ -3275,6 +3346,7 @@ int32_t scemc_batch_autotune(scemc_batch* b, int32_t or_per_metropolis, int32_t 
   if (b->fast) {
     for (int m : {2, 3})
       for (int q : {1, 2}) cands.push_back({m, q, 0, 2});
+    cands.push_back({4, 2, 0, 2});
     for (int q : {1, 2}) cands.push_back({3, q, 0, 3});
   } else {
     for (int m : {2, 3})

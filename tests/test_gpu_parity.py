@@ -129,7 +129,8 @@ REPLAY_CASES = [(m, 4, 2, 1, 0) for m in MODELS] + [(m, 0, 2, 0, 1) for m in FAS
     ("fcc_l2_tri_zeeman", 0, 1, 0, 2), ("threebody", 0, 1, 0, 1), ("chain", 0, 2, 0, 2),
     ("bcc_l2_plaq_zeeman", 0, 3, 0, 1), ("fcc_l2_tri_zeeman", 0, 3, 0, 2), ("biquadratic", 4, 3, 1, 0),
     ("mixed", 8, 3, 0, 0),
-] + [(m, 0, 1, 3, 2) for m in FAST] + [("bcc_l2_plaq_zeeman", 0, 3, 3, 1), ("fcc_l2_tri_zeeman", 0, 3, 3, 2)]
+] + [(m, 0, 1, 3, 2) for m in FAST] + [("bcc_l2_plaq_zeeman", 0, 3, 3, 1), ("fcc_l2_tri_zeeman", 0, 3, 3, 2)] + [
+    (m, 0, 4, 2, 2) for m in FAST]
 
 
 @pytest.mark.parametrize("name,lanes,mode,kernel,proposals", REPLAY_CASES,
@@ -169,7 +170,8 @@ def test_fast_kernel_is_launch_shape_independent(gpu):
     H, _ = build("bcc_l2_plaq_zeeman")
     gH = scemc.GPUTiledHamiltonian(H)
     cfg = rand_cfg(H.n_sites, 3)
-    for kernel, forms in [(2, [(1, 1), (1, 2), (2, 1), (2, 2), (3, 1), (3, 2)]), (3, [(1, 1), (1, 2), (3, 1), (3, 2)])]:
+    for kernel, forms in [(2, [(1, 1), (1, 2), (2, 1), (2, 2), (3, 1), (3, 2), (4, 1), (4, 2)]),
+                          (3, [(1, 1), (1, 2), (3, 1), (3, 2)])]:
         outs = []
         for mode, prop in forms:
             b = scemc.GPUBatch([gH], [2], [cfg, cfg], [9, 10], 0.6)
@@ -505,9 +507,10 @@ def test_launch_count_matches_the_launch_form(gpu):
         n0 = b.launches()
         b.run(3, or_per_metropolis=1, mode=mode, kernel=kernel, proposals=1)
         assert b.launches() - n0 == 3 * per_sweep, (kernel, mode)
-    n0 = b.launches()
-    b.run(2, or_per_metropolis=1, mode=2, kernel=2, proposals=2)  # one persistent launch per pass + tail
-    assert b.launches() - n0 == 2 * 3
+    for mode in (2, 4):  # one persistent launch per pass + tail
+        n0 = b.launches()
+        b.run(2, or_per_metropolis=1, mode=mode, kernel=2, proposals=2)
+        assert b.launches() - n0 == 2 * 3
 
 
 @pytest.mark.parametrize("name", ["dimer_zeeman", "biquadratic_zeeman", "mixed", "high_l", "fourbody",
