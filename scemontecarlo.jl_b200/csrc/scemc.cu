@@ -1349,38 +1349,53 @@ __global__ void __launch_bounds__(256) k_learned_fused(SweepArgs a, LearnedNet n
   const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
   uint32_t phase = 0;
   bool ok = true;
+  // A thread's share of one tile's environment (warpgroup 0: spins 0..7 -> input
+  // columns 0..23; warpgroup 1: spins 8..13 and kT -> columns 24..42), gathered for
+  // the next tile while this tile draws.
+  struct Gather {
+    int li, q, r, s;
+    bool valid;
+    float4 e;
+    float tau;
+    alignas(16) __nv_bfloat16 x[24];
+  };
+  auto gather = [&](int tile, Gather& g) {
+    const int item = tile * kTile + row;
+    g.valid = tile < n_tiles && item < n_items;
+    g.li = g.q = g.r = g.s = 0;
+    g.e = make_float4(0.f, 0.f, 1.f, 0.f);
+    g.tau = 1.0f;
+#pragma unroll
+    for (int k = 0; k < 24; ++k) g.x[k] = __float2bfloat16_rn(0.0f);
+    if (!g.valid) return;
+    item_of(a, seg_c, item, g.li, g.q, g.r);
+    const DevLattice& L = a.lat[g.li];
+    g.s = L.color_sites[L.color_ptr[col] + g.q];
+    const float4* sp = a.spins + L.spin_off;
+    const int32_t* env = L.env + (int64_t)g.s * L.env_k;
+    g.tau = slot_kt_mev(a, L.slot0 + g.r);
+    const int k0 = wg ? 8 : 0, k1 = wg ? 14 : 8;
+    for (int k = k0; k < k1; ++k) {
+      const float4 v = __ldg(sp + (int64_t)__ldg(env + k) * L.R + g.r);
+      g.x[3 * (k - k0)] = __float2bfloat16_rn(v.x);
+      g.x[3 * (k - k0) + 1] = __float2bfloat16_rn(v.y);
+      g.x[3 * (k - k0) + 2] = __float2bfloat16_rn(v.z);
+    }
+    if (wg) g.x[18] = __float2bfloat16_rn(g.tau);
+    else g.e = sp[(int64_t)g.s * L.R + g.r];
+  };
+  Gather cur, nxt;
+  gather(blockIdx.x, cur);
   for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
     const int item = tile * kTile + row;
-    const bool valid = item < n_items;
-    int li = 0, q = 0, r = 0, s = 0;
-    float4 e = make_float4(0.f, 0.f, 1.f, 0.f);
-    float tau = 1.0f;
-    // warpgroup 0: environment spins 0..7 -> input columns 0..23 (chunks 0..2);
-    // warpgroup 1: spins 8..13 and kT -> columns 24..42 (chunks 3..5), chunks 6, 7 zero
-    alignas(16) __nv_bfloat16 x[24];
-#pragma unroll
-    for (int k = 0; k < 24; ++k) x[k] = __float2bfloat16_rn(0.0f);
-    if (valid) {
-      item_of(a, seg_c, item, li, q, r);
-      const DevLattice& L = a.lat[li];
-      s = L.color_sites[L.color_ptr[col] + q];
-      const float4* sp = a.spins + L.spin_off;
-      const int32_t* env = L.env + (int64_t)s * L.env_k;
-      tau = slot_kt_mev(a, L.slot0 + r);
-      const int k0 = wg ? 8 : 0, k1 = wg ? 14 : 8;
-      for (int k = k0; k < k1; ++k) {
-        const float4 v = __ldg(sp + (int64_t)__ldg(env + k) * L.R + r);
-        x[3 * (k - k0)] = __float2bfloat16_rn(v.x);
-        x[3 * (k - k0) + 1] = __float2bfloat16_rn(v.y);
-        x[3 * (k - k0) + 2] = __float2bfloat16_rn(v.z);
-      }
-      if (wg) x[18] = __float2bfloat16_rn(tau);
-      else e = sp[(int64_t)s * L.R + r];
-    }
+    const bool valid = cur.valid;
+    const int li = cur.li, r = cur.r, s = cur.s;
+    const float4 e = cur.e;
+    const float tau = cur.tau;
 #pragma unroll
     for (int kg = 0; kg < 3; ++kg)
       *reinterpret_cast<uint4*>(sX + umma::kmajor_offset(row, (3 * wg + kg) * 8, 64)) =
-          reinterpret_cast<const uint4*>(x)[kg];
+          reinterpret_cast<const uint4*>(cur.x)[kg];
     if (wg) {
       const uint4 z = make_uint4(0u, 0u, 0u, 0u);
       *reinterpret_cast<uint4*>(sX + umma::kmajor_offset(row, 48, 64)) = z;
@@ -1441,6 +1456,8 @@ __global__ void __launch_bounds__(256) k_learned_fused(SweepArgs a, LearnedNet n
     }
     umma::fence_before();
     __syncthreads();  // every thread has read TMEM and the tiles before the next tile reuses them
+    gather(tile + gridDim.x, nxt);  // the next tile's loads are in flight during this tile's draw
+    cur = nxt;
     if (wg != 0 || !valid || !ok) continue;
 #pragma unroll
     for (int j = 0; j < 32; ++j) o[j] += sb[256 + j];
