@@ -205,8 +205,16 @@ int32_t scemc_batch_sync(scemc_batch* b);
 /* The batch's cudaStream_t (as void*), for callers that order or time work on it. */
 int32_t scemc_batch_stream(const scemc_batch* b, void** stream);
 /* Replaces every slot's spins (3 x n_sites FP64 per slot, payload order) and, when
- * energies is not NULL, the running energies. */
+ * energies is not NULL, the running energies. The payload crosses the bus unchanged
+ * in one copy; the device checks it (SCEMC_ERR_NUMERIC names the first non-finite
+ * spin's replica and column, and nothing changes), rounds it to FP32 and interleaves
+ * the replicas. Replaces _from_host! (src/gpu/gpu_state.jl:81-86) for every slot. */
 int32_t scemc_batch_upload(scemc_batch* b, const double* configs, const double* energies);
+/* Page-locks (and releases) a host buffer so that uploads and downloads through it
+ * are direct DMA; a Julia caller pins the Arrays it passes to the transfer calls
+ * (what CUDA.jl's Mem.pin does for the reference's to_host!/from_host! buffers). */
+int32_t scemc_host_register(void* ptr, int64_t bytes);
+int32_t scemc_host_unregister(void* ptr);
 /* Live timing of the sweep kernels: with profiling on, each pass is bracketed by a
  * CUDA event pair on the batch stream; scemc_batch_kernel_time returns the summed
  * device time (ms) and the number of passes since profiling was switched on. */

@@ -925,12 +925,17 @@ __device__ void fast_colour(const SweepArgs& a, int col, unsigned long long* s_d
   __syncwarp();
 }
 
-// Four 256-thread blocks per SM (64 registers): a colour of the 5-chain bcc 16^3
-// workload then runs its items in one wave (measured 12 % faster than two blocks).
+// 64 registers (eight 128-thread blocks per SM): a colour of the 5-chain bcc 16^3
+// workload then runs its items in one wave. Measured on that workload: 108
+// registers (two waves) 12 % slower; 80 or 96 registers with 128-thread blocks
+// (one wave, fewer spills) 9 % and 13 % slower; 256-thread blocks 1 % slower.
 #ifndef SCEMC_FAST_MINB
-#define SCEMC_FAST_MINB 4
+#define SCEMC_FAST_MINB 8
 #endif
-#define SCEMC_FAST_BOUNDS __launch_bounds__(256, SCEMC_FAST_MINB)
+#ifndef SCEMC_FAST_THREADS
+#define SCEMC_FAST_THREADS 128
+#endif
+#define SCEMC_FAST_BOUNDS __launch_bounds__(SCEMC_FAST_THREADS, SCEMC_FAST_MINB)
 
 template <int LMAX>
 __global__ void SCEMC_FAST_BOUNDS k_fast_colour(SweepArgs a) {
@@ -1795,7 +1800,9 @@ struct scemc_ensemble {
   long long barrier_limit_ns = 2000000000ll;
   int coop_blocks = 0;  // cached co-resident grid size for the persistent form
   int coop_G = -1;
-  float4* h_stage = nullptr;  // pinned host staging of the spins (n_spins float4)
+  double* d_cfg64 = nullptr;  // device copy of a host payload (3 x n_spins FP64)
+  unsigned long long* d_bad = nullptr;  // first non-finite payload spin
+  unsigned char* h_small = nullptr;     // pinned: flag, energies in, per-slot arrays out
   // learned proposal (network not owned)
   const scemc_mlp* mlp = nullptr;
   std::vector<int32_t*> d_env;
@@ -1830,7 +1837,7 @@ struct scemc_ensemble {
   double prof_ms = 0.0;
   int64_t prof_passes = 0;
   ~scemc_ensemble() {
-    if (h_stage) cudaFreeHost(h_stage);
+    if (h_small) cudaFreeHost(h_small);
     for (auto& pr : ev_pending) {
       ev_pool.push_back(pr.first);
       ev_pool.push_back(pr.second);
@@ -1844,7 +1851,8 @@ struct scemc_ensemble {
       if (p) cudaFree(p);
     void* ps[] = {d_lat,   d_spins, d_seg,  d_energy,       d_dEfix,        d_cnt,       d_win,    d_swaps,
                   d_beta,  d_step,  d_seed, d_slot_of_rung, d_rung_of_slot, d_max_drift, d_drift,  d_eout,
-                  d_gs,    d_st,    d_partial, d_meas,      d_rprop,        d_ru,        d_rdE,    d_racc};
+                  d_gs,    d_st,    d_partial, d_meas,      d_rprop,        d_ru,        d_rdE,    d_racc,
+                  d_cfg64, d_bad};
     for (void* p : ps)
       if (p) cudaFree(p);
     if (stream) cudaStreamDestroy(stream);
@@ -2297,46 +2305,133 @@ int32_t dalloc(T** p, size_t n) {
   return SCEMC_OK;
 }
 
-bool finite3(const double* v) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]); }
+int sm_count(int dev);
 
-// Whole-table transfers through pinned staging: the host (de)interleaves the
-// replicas (spins[site * R + r]) and one contiguous copy moves the table.
-int32_t stage_upload(scemc_ensemble* E, int ti, const double* cfgs) {
-  const scemc_tables* T = E->tabs[ti];
-  const int R = E->R[ti];
-  const int64_t n = T->n_sites;
-  float4* h = E->h_stage + E->spin_off[ti];
-  for (int r = 0; r < R; ++r) {
-    const double* c = cfgs + (size_t)r * 3 * n;
-    for (int64_t s = 0; s < n; ++s) {
-      if (!finite3(c + 3 * s))
-        return fail(SCEMC_ERR_NUMERIC, "spin column " + std::to_string(s + 1) + " of replica " +
-                                           std::to_string(r + 1) + " is not finite");
-      h[s * R + r] = make_float4((float)c[3 * s], (float)c[3 * s + 1], (float)c[3 * s + 2], 0.0f);
-    }
+// Host payloads (per table, per replica 3 x n_sites FP64, the tables one after the
+// other) cross the bus unchanged, in one copy each way. Kernels check them, round
+// them to FP32 and interleave the replicas (spins[site * R + r]) on the device.
+__global__ void k_payload_check(const double* cfg, int64_t n, unsigned long long* bad) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double x = cfg[3 * i], y = cfg[3 * i + 1], z = cfg[3 * i + 2];
+    if (!(isfinite(x) && isfinite(y) && isfinite(z))) atomicMin(bad, (unsigned long long)i);
   }
-  CUDA_TRY(cudaMemcpyAsync(E->d_spins + E->spin_off[ti], h, sizeof(float4) * n * R, cudaMemcpyHostToDevice,
-                           E->stream));
+}
+
+// One table, walked in device order so that the float4 stores coalesce.
+__global__ void k_payload_in(const double* cfg, int64_t n_sites, int R, float4* spins) {
+  const int64_t tot = n_sites * R;
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < tot; j += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = j / R;
+    const double* c = cfg + 3 * ((j - s * R) * n_sites + s);
+    spins[j] = make_float4((float)c[0], (float)c[1], (float)c[2], 0.0f);
+  }
+}
+
+__global__ void k_payload_out(const float4* spins, int64_t n_sites, int R, double* cfg) {
+  const int64_t tot = n_sites * R;
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < tot; j += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = j / R;
+    const float4 v = spins[j];
+    double* c = cfg + 3 * ((j - s * R) * n_sites + s);
+    c[0] = v.x;
+    c[1] = v.y;
+    c[2] = v.z;
+  }
+}
+
+unsigned payload_blocks(const scemc_ensemble* E, int64_t n) {
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sm_count(E->device) * 16));
+}
+
+// Pinned host area for the small transfers: the non-finite flag, the energies on
+// the way in, and the per-slot arrays on the way out.
+constexpr size_t kSmallIn = 16;
+size_t small_out_offset(int n_slots) { return kSmallIn + (((size_t)8 * n_slots + 15) & ~(size_t)15); }
+size_t small_bytes(int n_slots) { return small_out_offset(n_slots) + (size_t)80 * n_slots + 64; }
+
+// Replaces every chain's spins (and, when `energies` is given, the running
+// energies) from a host payload. Nothing on the device changes when an input is
+// not finite; returns after the host buffers may be reused.
+int32_t payload_upload(scemc_ensemble* E, const double* cfgs, const double* energies) {
+  if (energies)
+    for (int i = 0; i < E->n_slots; ++i)
+      if (!std::isfinite(energies[i])) return fail(SCEMC_ERR_ARG, "energy must be finite");
+  const int64_t n = E->n_spins;
+  auto* h_bad = reinterpret_cast<unsigned long long*>(E->h_small);
+  CUDA_TRY(cudaMemsetAsync(E->d_bad, 0xff, sizeof(unsigned long long), E->stream));
+  if (n > 0) {
+    CUDA_TRY(cudaMemcpyAsync(E->d_cfg64, cfgs, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, E->stream));
+    k_payload_check<<<payload_blocks(E, n), 256, 0, E->stream>>>(E->d_cfg64, n, E->d_bad);
+    CUDA_TRY(cudaGetLastError());
+  }
+  CUDA_TRY(cudaMemcpyAsync(h_bad, E->d_bad, sizeof(unsigned long long), cudaMemcpyDeviceToHost, E->stream));
+  CUDA_TRY(cudaStreamSynchronize(E->stream));
+  if (*h_bad != ~0ull) {
+    const int64_t p = (int64_t)*h_bad;
+    size_t ti = 0;
+    while (ti + 1 < E->tabs.size() && p >= E->spin_off[ti + 1]) ++ti;
+    const int64_t local = p - E->spin_off[ti], ns = E->tabs[ti]->n_sites;
+    return fail(SCEMC_ERR_NUMERIC, "spin column " + std::to_string(local % ns + 1) + " of replica " +
+                                       std::to_string(local / ns + 1) + " is not finite");
+  }
+  for (size_t ti = 0; ti < E->tabs.size(); ++ti) {
+    const int64_t ns = E->tabs[ti]->n_sites;
+    k_payload_in<<<payload_blocks(E, ns * E->R[ti]), 256, 0, E->stream>>>(E->d_cfg64 + 3 * E->spin_off[ti], ns,
+                                                                          E->R[ti], E->d_spins + E->spin_off[ti]);
+    CUDA_TRY(cudaGetLastError());
+  }
+  if (energies) {
+    double* h_en = reinterpret_cast<double*>(E->h_small + kSmallIn);
+    std::memcpy(h_en, energies, sizeof(double) * E->n_slots);
+    CUDA_TRY(cudaMemcpyAsync(E->d_energy, h_en, sizeof(double) * E->n_slots, cudaMemcpyHostToDevice, E->stream));
+  }
   CUDA_TRY(cudaStreamSynchronize(E->stream));
   return SCEMC_OK;
 }
 
-int32_t stage_download(const scemc_ensemble* E, int ti, double* cfgs) {
-  const scemc_tables* T = E->tabs[ti];
-  const int R = E->R[ti];
-  const int64_t n = T->n_sites;
-  float4* h = E->h_stage + E->spin_off[ti];
-  CUDA_TRY(cudaMemcpyAsync(h, E->d_spins + E->spin_off[ti], sizeof(float4) * n * R, cudaMemcpyDeviceToHost,
-                           E->stream));
-  CUDA_TRY(cudaStreamSynchronize(E->stream));
-  for (int r = 0; r < R; ++r) {
-    double* c = cfgs + (size_t)r * 3 * n;
-    for (int64_t s = 0; s < n; ++s) {
-      const float4 v = h[s * R + r];
-      c[3 * s] = v.x;
-      c[3 * s + 1] = v.y;
-      c[3 * s + 2] = v.z;
+// Destinations of a download (each may be NULL).
+struct DownloadDst {
+  double* configs = nullptr;
+  double* energies = nullptr;
+  int32_t* slot_of_rung = nullptr;
+  int64_t* counters = nullptr;
+  int64_t* swaps = nullptr;
+  double* steps = nullptr;
+  double* max_drift = nullptr;
+};
+
+// Everything is read on the batch stream (after the work enqueued on it) and
+// waited for once.
+int32_t payload_download(const scemc_ensemble* E, const DownloadDst& d) {
+  const int n = E->n_slots;
+  if (d.configs && E->n_spins > 0) {
+    for (size_t ti = 0; ti < E->tabs.size(); ++ti) {
+      const int64_t ns = E->tabs[ti]->n_sites;
+      k_payload_out<<<payload_blocks(E, ns * E->R[ti]), 256, 0, E->stream>>>(
+          E->d_spins + E->spin_off[ti], ns, E->R[ti], E->d_cfg64 + 3 * E->spin_off[ti]);
+      CUDA_TRY(cudaGetLastError());
     }
+    CUDA_TRY(cudaMemcpyAsync(d.configs, E->d_cfg64, sizeof(double) * 3 * E->n_spins, cudaMemcpyDeviceToHost,
+                             E->stream));
+  }
+  struct Part {
+    void* dst;
+    const void* src;
+    size_t bytes;
+  } parts[] = {{d.energies, E->d_energy, (size_t)8 * n},      {d.slot_of_rung, E->d_slot_of_rung, (size_t)4 * n},
+               {d.counters, E->d_cnt, (size_t)32 * n},        {d.swaps, E->d_swaps, (size_t)16 * n},
+               {d.steps, E->d_step, (size_t)8 * n},           {d.max_drift, E->d_max_drift, (size_t)8 * n}};
+  unsigned char* h = E->h_small + small_out_offset(n);
+  size_t off = 0;
+  for (const Part& pt : parts) {
+    if (pt.dst) CUDA_TRY(cudaMemcpyAsync(h + off, pt.src, pt.bytes, cudaMemcpyDeviceToHost, E->stream));
+    off += (pt.bytes + 15) & ~(size_t)15;
+  }
+  CUDA_TRY(cudaStreamSynchronize(E->stream));
+  off = 0;
+  for (const Part& pt : parts) {
+    if (pt.dst) std::memcpy(pt.dst, h + off, pt.bytes);
+    off += (pt.bytes + 15) & ~(size_t)15;
   }
   return SCEMC_OK;
 }
@@ -2373,7 +2468,8 @@ int32_t create_ensemble(int32_t n_tables, const scemc_tables* const* tables, con
     if (!(steps[i] > 0) || !std::isfinite(energies[i])) return fail(SCEMC_ERR_ARG, "step must be > 0 and energy finite");
   int32_t rc;
   if ((rc = dalloc(&E->d_spins, off))) return rc;
-  CUDA_TRY(cudaHostAlloc((void**)&E->h_stage, sizeof(float4) * std::max<int64_t>(off, 1), cudaHostAllocDefault));
+  if ((rc = dalloc(&E->d_cfg64, (size_t)3 * std::max<int64_t>(off, 1))) || (rc = dalloc(&E->d_bad, 1))) return rc;
+  CUDA_TRY(cudaHostAlloc((void**)&E->h_small, small_bytes(slots), cudaHostAllocDefault));
   // lattice descriptors with per-batch geometry
   std::vector<DevLattice> lats(n_tables);
   int max_atoms = 1;
@@ -2431,11 +2527,7 @@ int32_t create_ensemble(int32_t n_tables, const scemc_tables* const* tables, con
   std::vector<double> ones(slots, 1.0);
   CUDA_TRY(cudaMemcpy(E->d_beta, ones.data(), 8 * slots, cudaMemcpyHostToDevice));
   E->rec_len = 4 + 3 * max_atoms;
-  const double* cfg = configs;
-  for (int i = 0; i < n_tables; ++i) {
-    if ((rc = stage_upload(E, i, cfg))) return rc;
-    cfg += 3 * (size_t)tables[i]->n_sites * replicas[i];
-  }
+  if ((rc = payload_upload(E, configs, nullptr))) return rc;
   *out = guard.release();
   return SCEMC_OK;
 }
@@ -2573,7 +2665,7 @@ void fast_shape(const scemc_ensemble* E, int* threads, size_t* smem) {
   const int NR = fast_rows(E->lmax);
   const size_t per_warp = fast_group_floats(std::max(E->dmax, 1), std::max(E->rmax, 1), NR) * sizeof(float);
   const size_t params = fast_param_floats(E->n_slots) * sizeof(float);
-  int t = 256;
+  int t = SCEMC_FAST_THREADS;
   size_t m = params + (size_t)(t / 32) * per_warp;
   while (m > 160 * 1024 && t > 32) {
     t /= 2;
@@ -3226,15 +3318,12 @@ int32_t scemc_download(const scemc_chain* c, double* config, double* energy, int
                        int64_t* counters) {
   int32_t rc;
   if ((rc = check_single(c, nullptr))) return rc;
-  if (config)
-    if ((rc = stage_download(c, 0, config))) return rc;
-  if (energy) CUDA_TRY(cudaMemcpy(energy, c->d_energy, 8, cudaMemcpyDeviceToHost));
+  DownloadDst d;
+  d.configs = config;
+  d.energies = energy;
+  d.counters = counters;
+  if ((rc = payload_download(c, d))) return rc;
   if (sweep_index) *sweep_index = c->sweep_index;
-  if (counters) {
-    unsigned long long v[4];
-    CUDA_TRY(cudaMemcpy(v, c->d_cnt, 32, cudaMemcpyDeviceToHost));
-    for (int i = 0; i < 4; ++i) counters[i] = (int64_t)v[i];
-  }
   return SCEMC_OK;
 }
 
@@ -3242,9 +3331,7 @@ int32_t scemc_upload(scemc_chain* c, const double* config, double energy) {
   int32_t rc;
   if ((rc = check_single(c, nullptr))) return rc;
   if (!config || !std::isfinite(energy)) return fail(SCEMC_ERR_ARG, "config NULL or energy not finite");
-  if ((rc = stage_upload(c, 0, config))) return rc;
-  CUDA_TRY(cudaMemcpy(c->d_energy, &energy, 8, cudaMemcpyHostToDevice));
-  return SCEMC_OK;
+  return payload_upload(c, config, &energy);
 }
 
 int32_t scemc_set_step(scemc_chain* c, double step) {
@@ -3449,21 +3536,21 @@ int32_t scemc_batch_stream(const scemc_batch* b, void** stream) {
   return SCEMC_OK;
 }
 
+int32_t scemc_host_register(void* ptr, int64_t bytes) {
+  if (!ptr || bytes <= 0) return fail(SCEMC_ERR_ARG, "scemc_host_register: NULL pointer or non-positive size");
+  CUDA_TRY(cudaHostRegister(ptr, (size_t)bytes, cudaHostRegisterDefault));
+  return SCEMC_OK;
+}
+
+int32_t scemc_host_unregister(void* ptr) {
+  if (!ptr) return fail(SCEMC_ERR_ARG, "scemc_host_unregister: NULL pointer");
+  CUDA_TRY(cudaHostUnregister(ptr));
+  return SCEMC_OK;
+}
+
 int32_t scemc_batch_upload(scemc_batch* b, const double* configs, const double* energies) {
   if (!b || !configs) return fail(SCEMC_ERR_ARG, "NULL argument");
-  int32_t rc;
-  const double* cfg = configs;
-  for (size_t i = 0; i < b->tabs.size(); ++i) {
-    if ((rc = stage_upload(b, (int)i, cfg))) return rc;
-    cfg += 3 * (size_t)b->tabs[i]->n_sites * b->R[i];
-  }
-  if (energies) {
-    for (int i = 0; i < b->n_slots; ++i)
-      if (!std::isfinite(energies[i])) return fail(SCEMC_ERR_ARG, "energy must be finite");
-    CUDA_TRY(cudaMemcpyAsync(b->d_energy, energies, 8 * b->n_slots, cudaMemcpyHostToDevice, b->stream));
-    CUDA_TRY(cudaStreamSynchronize(b->stream));
-  }
-  return SCEMC_OK;
+  return payload_upload(b, configs, energies);
 }
 
 int32_t scemc_batch_profile(scemc_batch* b, int32_t on) {
@@ -3492,22 +3579,15 @@ int32_t scemc_batch_launches(const scemc_batch* b, int64_t* launches) {
 int32_t scemc_batch_download(const scemc_batch* b, double* configs, double* energies, int32_t* slot_of_rung,
                              int64_t* counters, int64_t* swaps, double* steps, double* max_drift) {
   if (!b) return fail(SCEMC_ERR_ARG, "batch is NULL");
-  int32_t rc;
-  if (configs) {
-    double* cfg = configs;
-    for (size_t i = 0; i < b->tabs.size(); ++i) {
-      if ((rc = stage_download(b, (int)i, cfg))) return rc;
-      cfg += 3 * (size_t)b->tabs[i]->n_sites * b->R[i];
-    }
-  }
-  const int n = b->n_slots;
-  if (energies) CUDA_TRY(cudaMemcpy(energies, b->d_energy, 8 * n, cudaMemcpyDeviceToHost));
-  if (slot_of_rung) CUDA_TRY(cudaMemcpy(slot_of_rung, b->d_slot_of_rung, 4 * n, cudaMemcpyDeviceToHost));
-  if (counters) CUDA_TRY(cudaMemcpy(counters, b->d_cnt, 32 * n, cudaMemcpyDeviceToHost));
-  if (swaps) CUDA_TRY(cudaMemcpy(swaps, b->d_swaps, 16 * n, cudaMemcpyDeviceToHost));
-  if (steps) CUDA_TRY(cudaMemcpy(steps, b->d_step, 8 * n, cudaMemcpyDeviceToHost));
-  if (max_drift) CUDA_TRY(cudaMemcpy(max_drift, b->d_max_drift, 8 * n, cudaMemcpyDeviceToHost));
-  return SCEMC_OK;
+  DownloadDst d;
+  d.configs = configs;
+  d.energies = energies;
+  d.slot_of_rung = slot_of_rung;
+  d.counters = counters;
+  d.swaps = swaps;
+  d.steps = steps;
+  d.max_drift = max_drift;
+  return payload_download(b, d);
 }
 
 int32_t scemc_batch_reset_counters(scemc_batch* b) {

@@ -205,6 +205,34 @@ def swap_payload(a: GPUChainState, b: GPUChainState):
     check(_lib.lib().scemc_swap_payload(a.h, b.h))
 
 
+class PinnedHost:
+    """A float64 host buffer page-locked through scemc_host_register (released on
+    close or exit of a `with` block): uploads from it and downloads into it are
+    direct DMA."""
+
+    def __init__(self, n: int):
+        self.array = np.zeros(int(n))
+        check(_lib.lib().scemc_host_register(self.array.ctypes.data, self.array.nbytes))
+        self._pinned = True
+
+    def close(self):
+        if getattr(self, "_pinned", False):
+            self._pinned = False
+            check(_lib.lib().scemc_host_unregister(self.array.ctypes.data))
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class GPUBatch:
     """Replicas of one or more table sets advancing together (PT rungs, temperature
     sets, chains of uneven supercells). Slots are numbered table-major."""
@@ -229,6 +257,7 @@ class GPUBatch:
                                             C.byref(h)))
         self.h = h
         self.n_slots = nslots
+        self.n_sites_total = exp // 3  # spins of every chain
         if energies is None:
             check(_lib.lib().scemc_renormalize(self.h, None))
             self.reset_counters()
@@ -273,8 +302,14 @@ class GPUBatch:
         return s.value or 0
 
     def upload(self, configs, energies=None):
+        """Replaces every chain's spins (the payload of all chains, table-major, each
+        3 x n_sites) and optionally the running energies."""
         cfg = np.ascontiguousarray(configs, np.float64).reshape(-1)
-        en = None if energies is None else np.ascontiguousarray(energies, np.float64)
+        if cfg.size != 3 * self.n_sites_total:
+            raise ValueError("configs hold %d values, the batch %d" % (cfg.size, 3 * self.n_sites_total))
+        en = None if energies is None else np.ascontiguousarray(energies, np.float64).reshape(-1)
+        if en is not None and en.size != self.n_slots:
+            raise ValueError("one energy per slot is needed")
         check(_lib.lib().scemc_batch_upload(self.h, ptr(cfg, C.c_double), None if en is None else ptr(en, C.c_double)))
 
     def profile(self, on: bool):
@@ -333,10 +368,18 @@ class GPUBatch:
         check(_lib.lib().scemc_total_energy(self.h, int(slot), C.byref(e)))
         return e.value
 
-    def download(self):
+    def download(self, out=None):
+        """The batch state. `out`, when given, is a C-contiguous float64 buffer of
+        3 x (total spins) that receives the payload (pinned host memory makes the
+        copy a direct DMA); the returned configs are views into it."""
         n = self.n_slots
-        tot = sum(g.n_sites * r for g, r in zip(self.gHs, self.replicas))
-        cfg = np.zeros(3 * tot)
+        tot = self.n_sites_total
+        if out is None:
+            cfg = np.empty(3 * tot)
+        else:
+            cfg = out.reshape(-1)
+            if cfg.dtype != np.float64 or cfg.size != 3 * tot or not cfg.flags.c_contiguous or not cfg.flags.writeable:
+                raise ValueError("out must be a writeable C-contiguous float64 buffer of 3 x %d values" % tot)
         en = np.zeros(n)
         sor = np.zeros(n, np.int32)
         cnt = np.zeros(4 * n, np.int64)

@@ -331,6 +331,49 @@ def test_swap_payload_and_roundtrip(gpu):
     np.testing.assert_array_equal(ta.config, sa.config)
 
 
+def test_batch_payload_round_trip_and_guard(gpu):
+    """Uploads and downloads of a batch of uneven tables: the device rounds and
+    interleaves the host payload exactly like an FP32 cast, a download into a
+    pinned buffer equals the default one, and a non-finite spin is reported by its
+    replica and column with the device state left as it was."""
+    Hs = [build("bcc_body4")[0], scemc.TiledHamiltonian(2, models.config4_bcc_body4().terms, dims=(2, 3, 4))]
+    gHs = [scemc.GPUTiledHamiltonian(h) for h in Hs]
+    reps = [3, 2]
+    cfgs = [rand_cfg(h.n_sites, 40 + 7 * i + r) for i, h in enumerate(Hs) for r in range(reps[i])]
+    b = scemc.GPUBatch(gHs, reps, cfgs, list(range(1, 6)), 0.5, energies=np.zeros(5))  # no renormalisation
+    got = b.download()
+    for c, g in zip(cfgs, got["configs"]):
+        np.testing.assert_array_equal(g, c.astype(np.float32).astype(np.float64))
+    en = np.arange(5, dtype=np.float64) * 0.25 - 1.0
+    new = [rand_cfg(h.n_sites, 90 + 3 * i + r) for i, h in enumerate(Hs) for r in range(reps[i])]
+    b.upload(np.concatenate([c.reshape(-1) for c in new]), en)
+    with scemc.PinnedHost(3 * b.n_sites_total) as pin:
+        a = b.download(out=pin.array)
+        b.upload(pin.array, en)  # a pinned payload round-trips unchanged
+        a = {k: (v.copy() if isinstance(v, np.ndarray) else [c.copy() for c in v]) for k, v in
+             b.download(out=pin.array).items()}
+    d = b.download()
+    for c, x, y in zip(new, a["configs"], d["configs"]):
+        np.testing.assert_array_equal(x, c.astype(np.float32).astype(np.float64))
+        np.testing.assert_array_equal(x, y)
+    np.testing.assert_array_equal(a["energies"], en)
+    for k in ("slot_of_rung", "counters", "swaps", "steps", "max_drift"):
+        np.testing.assert_array_equal(a[k], d[k])
+    bad = np.concatenate([c.reshape(-1) for c in cfgs])
+    off = 3 * Hs[0].n_sites * reps[0] + 3 * Hs[1].n_sites  # table 2, replica 2
+    bad[off + 3 * 4 + 1] = np.inf  # its column 5
+    with pytest.raises(scemc.ScemcError, match="column 5 of replica 2"):
+        b.upload(bad, en + 1.0)
+    after = b.download()
+    for c, x in zip(new, after["configs"]):
+        np.testing.assert_array_equal(x, c.astype(np.float32).astype(np.float64))
+    np.testing.assert_array_equal(after["energies"], en)
+    with pytest.raises(_lib.ScemcArgumentError):
+        b.upload(np.concatenate([c.reshape(-1) for c in cfgs]), np.full(5, np.nan))
+    with pytest.raises(ValueError):
+        b.download(out=np.zeros(7))
+
+
 def test_guards(gpu):
     H, _ = build("chain")
     gH = scemc.GPUTiledHamiltonian(H)
