@@ -192,6 +192,8 @@ typedef struct scemc_run_params {
                          mode 1 or 3) */
   int32_t proposals;  /* 0 = auto, 1 = precompute a pass's Metropolis proposals, 2 = inline, 3 = learned
                          network (scemc_batch_set_learned; kernels 2 or 3, per-colour modes 1 or 3) */
+  int32_t rep_replicas; /* kernel 3: replicas per thread, 1 or 2; 0 = per colour launch, 1 when its
+                           one-replica threads fill at most two waves of the GPU, else 2 */
 } scemc_run_params;
 
 /* Inverse temperatures per rung (n_slots values, table-major like the slots). */

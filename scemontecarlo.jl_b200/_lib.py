@@ -45,7 +45,7 @@ class RunParams(C.Structure):
         ("exchange_interval", C.c_int64), ("adapt_interval", C.c_int64), ("adapt_target", C.c_double),
         ("renorm_interval", C.c_int64), ("measure_interval", C.c_int64), ("lanes_per_site", C.c_int32),
         ("mode", C.c_int32), ("phase_done", C.c_int64), ("phase_total", C.c_int64), ("kernel", C.c_int32),
-        ("proposals", C.c_int32),
+        ("proposals", C.c_int32), ("rep_replicas", C.c_int32),
     ]
 
 

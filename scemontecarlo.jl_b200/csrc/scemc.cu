@@ -181,6 +181,8 @@ struct SweepArgs {
   double* rec_lqr;
   uint32_t* flags;    // data-flow form: per item slot, the pass epoch its update completed (null otherwise)
   int32_t dmax, rmax;
+  int32_t rep_pf;     // replica-parallel form: prefetch every neighbour row into L1 first (few threads per colour)
+  int32_t pad_pf;
 };
 
 __device__ __forceinline__ unsigned long long globaltimer() {
@@ -983,20 +985,17 @@ __global__ void __launch_bounds__(256) k_proposals(SweepArgs a) { make_proposals
 // replicas of one site: r = g, g + G, ..., g + (P-1) G with G = ceil(R / P), so the
 // G threads of a site read each neighbour's replicas as contiguous float4 runs.
 // Every coupling word (descriptor, record, W block) a thread loads serves its P
-// replicas: the load's register writeback, not the FMA pipe, bounds a one-replica
-// thread; P = 2 at 80 registers (three 256-thread blocks per SM) measured fastest.
+// replicas. When a colour fills many waves (fcc 64^3 x 32 rungs) the load's register
+// writeback, not the FMA pipe, bounds a one-replica thread and P = 2 at 80 registers
+// measured fastest (7.7 against 9.3 ms per pass at fcc 48^3). When it fills at most
+// two waves (the PT ladders) each thread's record walk is latency-bound and P = 1
+// at 64 registers, with twice the threads, measured fastest (0.49 against 0.54 ms
+// per step).
 // Each replica keeps its NR coefficients in registers, c_t = sum_j W_j[t, :] . z_j,
 // and forms
 // dE = sum_t c_t (znew_t - zold_t) itself (no shuffles or shared-memory rows). Built
 // for large replica counts (many PT rungs of one Hamiltonian).
 // ---------------------------------------------------------------------------
-#ifndef SCEMC_REP_MINB
-#define SCEMC_REP_MINB 3
-#endif
-#ifndef SCEMC_REP_P
-#define SCEMC_REP_P 2
-#endif
-constexpr int kRepP = SCEMC_REP_P;  // replicas per thread
 
 template <int LMAX, int P>
 __device__ void rep_colour(const SweepArgs& a, int col, unsigned long long* s_dE, unsigned int* s_cnt,
@@ -1041,11 +1040,21 @@ __device__ void rep_colour(const SweepArgs& a, int col, unsigned long long* s_dE
     const int32_t* __restrict__ nbl = L.nb_list + n0;
     const float* __restrict__ ft = L.ftensor;
     // the P replicas' spins of neighbour `loc` (unused replicas read replica g)
+    const bool pf = a.rep_pf != 0;  // grid-uniform
     auto gather = [&](int loc, float4* v) {
       const float4* b = sp + (int64_t)__ldg(nbl + loc) * R + g;
 #pragma unroll
-      for (int k = 0; k < P; ++k) v[k] = __ldcg(b + (ok[k] ? k * G : 0));
+      for (int k = 0; k < P; ++k) v[k] = pf ? __ldg(b + (ok[k] ? k * G : 0)) : __ldcg(b + (ok[k] ? k * G : 0));
     };
+    if (pf) {  // every neighbour row requested at once; the record walk then hits L1
+      const int nd = (int)(cnt >> 24);
+      for (int k = 0; k < nd; ++k) {
+        const float4* b = sp + (int64_t)__ldg(nbl + k) * R + g;
+#pragma unroll
+        for (int kk = 0; kk < P; ++kk)
+          if (ok[kk]) asm volatile("prefetch.global.L1 [%0];" ::"l"(b + kk * G));
+      }
+    }
     float c[P][NR];
 #pragma unroll
     for (int k = 0; k < P; ++k)
@@ -1490,14 +1499,16 @@ __global__ void __launch_bounds__(256) k_learned_fused(SweepArgs a, LearnedNet n
   }
 }
 
-template <int LMAX>
-__global__ void __launch_bounds__(256, SCEMC_REP_MINB) k_rep_colour(SweepArgs a) {
+// P = 2 at 80 registers (three 256-thread blocks per SM); P = 1 at 64 registers
+// (four blocks per SM).
+template <int LMAX, int P>
+__global__ void __launch_bounds__(256, P == 1 ? 4 : 3) k_rep_colour(SweepArgs a) {
   extern __shared__ __align__(16) float zsm[];
   __shared__ unsigned long long s_dE[kMaxSlots];
   __shared__ unsigned int s_cnt[3 * kMaxSlots];
   zero_block(a.n_slots, s_dE, s_cnt);
   stage_params(a, zsm);
-  rep_colour<LMAX, kRepP>(a, a.colour, s_dE, s_cnt, zsm);
+  rep_colour<LMAX, P>(a, a.colour, s_dE, s_cnt, zsm);
   flush_block(a, s_dE, s_cnt);
 }
 
@@ -2648,6 +2659,7 @@ struct Launch {
   bool precompute = false;  // Metropolis proposals computed before the colour loop
   bool learned = false;     // Metropolis proposals from the learned network, per colour
   bool flow = false;        // persistent form with per-item completion flags instead of grid barriers
+  int rep_p = 0;            // replica-parallel kernel: replicas per thread (0 = per colour, by its size)
 };
 
 using FastFn = void (*)(SweepArgs);
@@ -2713,6 +2725,37 @@ int32_t prepare_learned(scemc_ensemble* E) {
   return SCEMC_OK;
 }
 
+// Threads of a replica-parallel launch of colour c with P replicas per thread.
+int64_t rep_threads(const scemc_ensemble* E, int c, int P) {
+  int64_t nt = 0;
+  const int32_t* sc = E->seg.data() + (size_t)c * (E->tabs.size() + 1);
+  for (size_t li = 0; li < E->tabs.size(); ++li)
+    nt += (int64_t)(sc[li + 1] - sc[li]) / E->R[li] * ((E->R[li] + P - 1) / P);
+  return nt;
+}
+
+// The replica-parallel form of one colour launch: replicas per thread (`forced`, or
+// 1 when the one-replica threads fill at most two waves of four 256-thread blocks per
+// SM, else 2) and whether each thread first prefetches its neighbour rows into L1
+// (at most two waves of resident threads: the record walk is then latency-bound;
+// measured 9 % faster on the PT ladders, 7 % slower at fcc 48^3 x 32).
+struct RepForm {
+  int P;
+  int64_t nt;
+  int32_t pf;
+  FastFn fn;
+};
+RepForm rep_form(const scemc_ensemble* E, int c, int forced) {
+  RepForm f;
+  const int64_t sms = sm_count(E->device);
+  f.P = forced == 1 || forced == 2 ? forced : (rep_threads(E, c, 1) <= sms * 1024 * 2 ? 1 : 2);
+  f.nt = rep_threads(E, c, f.P);
+  f.pf = f.nt <= sms * (f.P == 1 ? 1024 : 768) * 2 ? 1 : 0;
+  if (E->lmax == 1) f.fn = f.P == 1 ? k_rep_colour<1, 1> : k_rep_colour<1, 2>;
+  else f.fn = f.P == 1 ? k_rep_colour<2, 1> : k_rep_colour<2, 2>;
+  return f;
+}
+
 int32_t run_learned_pass(scemc_ensemble* E, const Launch& Lc) {
   SweepArgs a = make_args(E, -1);
   int32_t rc;
@@ -2746,14 +2789,11 @@ int32_t run_learned_pass(scemc_ensemble* E, const Launch& Lc) {
     if (Lc.rep) {
       const int threads = 256;
       const size_t smem = fast_param_floats(E->n_slots) * sizeof(float);
-      int64_t nt = 0;
-      const int32_t* sc = E->seg.data() + (size_t)c * (E->tabs.size() + 1);
-      for (size_t li = 0; li < E->tabs.size(); ++li)
-        nt += (int64_t)(sc[li + 1] - sc[li]) / E->R[li] * ((E->R[li] + kRepP - 1) / kRepP);
-      FastFn fn = E->lmax == 1 ? k_rep_colour<1> : k_rep_colour<2>;
-      CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      fn<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(cap, (nt + threads - 1) / threads)), threads, smem,
-           E->stream>>>(a);
+      const RepForm f = rep_form(E, c, Lc.rep_p);
+      a.rep_pf = f.pf;
+      CUDA_TRY(cudaFuncSetAttribute((const void*)f.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      f.fn<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(cap, (f.nt + threads - 1) / threads)), threads, smem,
+             E->stream>>>(a);
     } else {
       int threads;
       size_t smem;
@@ -2788,19 +2828,16 @@ int32_t run_pass_impl(scemc_ensemble* E, int pass, const Launch& Lc) {
       k_proposals<<<std::max(blocks, 1), 256, 0, E->stream>>>(a);
       CUDA_TRY(cudaGetLastError());
     }
-    FastFn fn = lmax == 1 ? k_rep_colour<1> : k_rep_colour<2>;
-    CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     for (int c = 0; c < E->max_colors; ++c) {
       const int n = E->seg[(size_t)c * (E->tabs.size() + 1) + E->tabs.size()];
       if (n == 0) continue;
       a.colour = c;
-      int64_t nt = 0;  // kRepP replicas per thread
-      const int32_t* sc = E->seg.data() + (size_t)c * (E->tabs.size() + 1);
-      for (size_t li = 0; li < E->tabs.size(); ++li)
-        nt += (int64_t)(sc[li + 1] - sc[li]) / E->R[li] * ((E->R[li] + kRepP - 1) / kRepP);
-      const int blocks = (int)std::min<int64_t>(cap, (nt + threads - 1) / threads);
+      const RepForm f = rep_form(E, c, Lc.rep_p);
+      CUDA_TRY(cudaFuncSetAttribute((const void*)f.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      const int blocks = (int)std::min<int64_t>(cap, (f.nt + threads - 1) / threads);
+      a.rep_pf = f.pf;
       ++E->launches;
-      fn<<<std::max(blocks, 1), threads, smem, E->stream>>>(a);
+      f.fn<<<std::max(blocks, 1), threads, smem, E->stream>>>(a);
       CUDA_TRY(cudaGetLastError());
     }
     return SCEMC_OK;
@@ -3032,8 +3069,11 @@ int auto_lanes(const scemc_ensemble* E) {
 
 // kernel: 0 auto, 1 generic, 2 row-parallel fast, 3 replica-parallel; proposals: 0 auto,
 // 1 precompute, 2 inline.
-int32_t resolve_launch(const scemc_ensemble* E, int lanes, int mode, int kernel, int proposals, Launch* out) {
+int32_t resolve_launch(const scemc_ensemble* E, int lanes, int mode, int kernel, int proposals, Launch* out,
+                       int rep_replicas = 0) {
   Launch L;
+  if (rep_replicas < 0 || rep_replicas > 2) return fail(SCEMC_ERR_ARG, "rep_replicas must be 0, 1 or 2");
+  L.rep_p = rep_replicas;
   if (mode == 0 && kernel == 0 && E->tuned) {
     mode = E->tuned_mode;
     kernel = E->tuned_kernel;
@@ -3108,7 +3148,7 @@ int32_t sweep_once(scemc_ensemble* E, int n_or, const Launch& L) {
 // device memory and the tail advances it, so one capture serves all sweeps.
 int32_t sweep_graph(scemc_ensemble* E, int n_or, const Launch& L, cudaGraphExec_t* out, int64_t* n_launch) {
   const int key[5] = {n_or, L.rep ? 2 : (L.fast ? 1 : 0), L.learned ? 2 : (L.precompute ? 1 : 0),
-                      (L.fast || L.rep) ? 0 : L.G, E->recording ? 1 : 0};
+                      L.fast ? 0 : (L.rep ? L.rep_p : L.G), E->recording ? 1 : 0};
   for (auto& g : E->graphs)
     if (std::equal(key, key + 5, g.key)) {
       *out = g.exec;
@@ -3129,8 +3169,9 @@ int32_t sweep_graph(scemc_ensemble* E, int n_or, const Launch& L, cudaGraphExec_
   }
   if (L.rep) {
     const size_t smem = fast_param_floats(E->n_slots) * sizeof(float);
-    CUDA_TRY(cudaFuncSetAttribute((const void*)(E->lmax == 1 ? k_rep_colour<1> : k_rep_colour<2>),
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    for (int c = 0; c < E->max_colors; ++c)
+      CUDA_TRY(cudaFuncSetAttribute((const void*)rep_form(E, c, L.rep_p).fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
   }
   const bool prof = E->profiling;
   E->profiling = false;  // graph launches are timed as a whole
@@ -3407,7 +3448,7 @@ int32_t scemc_batch_run_async(scemc_batch* b, const scemc_run_params* p) {
   const int64_t total = p->phase_total > 0 ? p->phase_total : p->phase_done + p->nsweeps;
   int32_t rc;
   Launch L;
-  if ((rc = resolve_launch(b, p->lanes_per_site, p->mode, p->kernel, p->proposals, &L))) return rc;
+  if ((rc = resolve_launch(b, p->lanes_per_site, p->mode, p->kernel, p->proposals, &L, p->rep_replicas))) return rc;
   if (b->sweep_index + p->nsweeps >= 0x7ffffffell - 1)
     return fail(SCEMC_ERR_EXHAUSTED, "sweep_index would exhaust the 32-bit RNG counter word");
   cudaGraphExec_t exec = nullptr;

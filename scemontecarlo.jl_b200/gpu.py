@@ -278,11 +278,11 @@ class GPUBatch:
     @staticmethod
     def params(nsweeps, or_per_metropolis=0, exchange=False, exchange_interval=1, adapt_interval=0,
                adapt_target=0.5, renorm_interval=0, measure_interval=0, lanes_per_site=0, mode=0, phase_done=0,
-               phase_total=0, kernel=0, proposals=0) -> _lib.RunParams:
+               phase_total=0, kernel=0, proposals=0, rep_replicas=0) -> _lib.RunParams:
         return _lib.RunParams(int(nsweeps), int(or_per_metropolis), int(bool(exchange)), int(exchange_interval),
                               int(adapt_interval), float(adapt_target), int(renorm_interval), int(measure_interval),
                               int(lanes_per_site), int(mode), int(phase_done), int(phase_total), int(kernel),
-                              int(proposals))
+                              int(proposals), int(rep_replicas))
 
     def run(self, nsweeps, **kw):
         """Runs `nsweeps` compound sweeps (see scemc_run_params) and waits for them."""

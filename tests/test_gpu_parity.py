@@ -166,17 +166,21 @@ def test_sweep_replay(gpu, name, lanes, mode, kernel, proposals):
 def test_fast_kernel_is_launch_shape_independent(gpu):
     """The fast kernel fixes its lane count by lmax and reduces dE with a fixed
     butterfly: per-colour vs persistent launches and precomputed vs inline proposals
-    give bitwise-identical chains, overrelaxation included."""
+    give bitwise-identical chains, overrelaxation included. The replica-parallel
+    kernel gives the same chains with one or two replicas per thread."""
     H, _ = build("bcc_l2_plaq_zeeman")
     gH = scemc.GPUTiledHamiltonian(H)
     cfg = rand_cfg(H.n_sites, 3)
-    for kernel, forms in [(2, [(1, 1), (1, 2), (2, 1), (2, 2), (3, 1), (3, 2), (4, 1), (4, 2)]),
-                          (3, [(1, 1), (1, 2), (3, 1), (3, 2)])]:
+    # kernel 3 also with one and two replicas per thread (three replicas: the second
+    # thread of a site carries one unused slot when it owns two)
+    for kernel, R, forms in [(2, 2, [(1, 1, 0), (1, 2, 0), (2, 1, 0), (2, 2, 0), (3, 1, 0), (3, 2, 0), (4, 1, 0),
+                                     (4, 2, 0)]),
+                             (3, 3, [(1, 1, 0), (1, 2, 1), (3, 1, 2), (3, 2, 1), (1, 1, 2), (3, 1, 0)])]:
         outs = []
-        for mode, prop in forms:
-            b = scemc.GPUBatch([gH], [2], [cfg, cfg], [9, 10], 0.6)
-            b.set_betas([1 / 0.002, 1 / 0.01])
-            b.run(6, or_per_metropolis=1, mode=mode, proposals=prop, kernel=kernel)
+        for mode, prop, rr in forms:
+            b = scemc.GPUBatch([gH], [R], [cfg] * R, [9, 10, 11][:R], 0.6)
+            b.set_betas([1 / 0.002, 1 / 0.01, 1 / 0.005][:R])
+            b.run(6, or_per_metropolis=1, mode=mode, proposals=prop, kernel=kernel, rep_replicas=rr)
             st = b.download()
             outs.append((np.stack(st["configs"]), st["energies"].copy(), st["counters"].copy()))
         for o in outs[1:]:
