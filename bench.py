@@ -113,7 +113,7 @@ def run_learned(args) -> int:
     X, Y = learned.collect_training_set(gH, env, w.kts, 200_000, sweeps_therm=2000, snapshots=4, spacing=50, seed=4)
     t1 = time.perf_counter()
     net = learned.ProposalNet(seed=4)
-    losses = net.train(X, Y, batch=1024, epochs=20, lr=1e-3, seed=4)
+    losses = net.train(X, Y, batch=1024, epochs=args.epochs, lr=1e-3, seed=4)
     torch.cuda.synchronize()
     t2 = time.perf_counter()
     measure = args.steps
@@ -141,7 +141,8 @@ def run_learned(args) -> int:
                        "acceptance_plain": [p.acceptance_metropolis for p in plain.points],
                        "acceptance_learned": [p.acceptance_metropolis for p in lrn.points],
                        "plain_ms_per_sweep": 1e3 * plain.extra["measure_s"] / measure,
-                       "training_rows": int(X.shape[0]), "collect_s": t1 - t0, "train_s": t2 - t1,
+                       "training_rows": int(X.shape[0]), "epochs": args.epochs, "collect_s": t1 - t0,
+                       "train_s": t2 - t1,
                        "train_loss_first_last": [float(losses[0]), float(losses[-1])],
                        "energy_plain": [float(p.stats["energy"].mean[0]) for p in plain.points],
                        "energy_learned": [float(p.stats["energy"].mean[0]) for p in lrn.points],
@@ -247,12 +248,15 @@ def main():
     ap.add_argument("--lanes", type=int, default=0, help="lanes per site (0 = autotuned)")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--therm", type=int, default=2000, help="learned workload: thermalisation sweeps per arm")
+    ap.add_argument("--epochs", type=int, default=20, help="learned workload: training epochs")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     big = args.workload in ("fcc", "pt")
     if args.steps is None:
-        args.steps = {"fcc": 20, "learned": 10000, "pt": 200}.get(args.workload, 2000)
+        # learned: plain Metropolis's tau_int is 100-200 sweeps here, so its log-binning
+        # estimate needs a few 10^4 sweeps (10^4 underestimates it by a third)
+        args.steps = {"fcc": 20, "learned": 30000, "pt": 200}.get(args.workload, 2000)
     if args.workload == "learned":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned proposal; "

@@ -997,6 +997,161 @@ __global__ void __launch_bounds__(256) k_proposals(SweepArgs a) { make_proposals
 // for large replica counts (many PT rungs of one Hamiltonian).
 // ---------------------------------------------------------------------------
 
+// The leave-one-out coefficients c[k][t] = sum_j W_j[t, :] . z_j of P replicas
+// (r = g + k G, those with ok[k]) of the site of descriptor `dsc`, from every record's
+// W block and its neighbours' Z rows. pf: the neighbour rows are prefetched into L1
+// first and read through it (else through L2).
+template <int LMAX, int P>
+__device__ __forceinline__ void rep_coeffs(const DevLattice& L, const float4* __restrict__ sp, int4 dsc, int R, int G,
+                                           int g, const bool (&ok)[P], bool pf,
+                                           float (&c)[P][(LMAX + 1) * (LMAX + 1) - 1]) {
+  constexpr int NR = (LMAX + 1) * (LMAX + 1) - 1;
+  const int n0 = dsc.y, j0 = dsc.z;
+  const uint32_t cnt = (uint32_t)dsc.w;
+  const int n_pair = (int)(cnt & 0xffu), n_trip = (int)((cnt >> 8) & 0xffu), n_quad = (int)((cnt >> 16) & 0xffu);
+  const int n_one = (dsc.x >> 31) & 1;
+  const uint2* __restrict__ fr = L.frec + j0;
+  const int32_t* __restrict__ nbl = L.nb_list + n0;
+  const float* __restrict__ ft = L.ftensor;
+  // the P replicas' spins of neighbour `loc` (unused replicas read replica g)
+  auto gather = [&](int loc, float4* v) {
+    const float4* b = sp + (int64_t)__ldg(nbl + loc) * R + g;
+#pragma unroll
+    for (int k = 0; k < P; ++k) v[k] = pf ? __ldg(b + (ok[k] ? k * G : 0)) : __ldcg(b + (ok[k] ? k * G : 0));
+  };
+  if (pf) {  // every neighbour row requested at once; the record walk then hits L1
+    const int nd = (int)(cnt >> 24);
+    for (int k = 0; k < nd; ++k) {
+      const float4* b = sp + (int64_t)__ldg(nbl + k) * R + g;
+#pragma unroll
+      for (int kk = 0; kk < P; ++kk)
+        if (ok[kk]) asm volatile("prefetch.global.L1 [%0];" ::"l"(b + kk * G));
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < P; ++k)
+#pragma unroll
+    for (int t = 0; t < NR; ++t) c[k][t] = 0.0f;
+  // merged per-neighbour pair blocks: c += W z_nb
+#pragma unroll 1
+  for (int j = 0; j < n_pair; ++j) {
+    const uint2 rec = __ldg(fr + j);
+    float4 v[P];
+    gather((int)(rec.y & 0xffu), v);
+    float z[P][NR];
+#pragma unroll
+    for (int k = 0; k < P; ++k) zrow_nr<NR>(v[k].x, v[k].y, v[k].z, z[k]);
+    const float* w = ft + (rec.x & kOffMask);
+    if constexpr (NR == 8) {
+      const float4* w4 = reinterpret_cast<const float4*>(w);
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        const float4 a0 = __ldg(w4 + 2 * t), a1 = __ldg(w4 + 2 * t + 1);
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+          float x = c[k][t];
+          x = fmaf(a0.x, z[k][0], x);
+          x = fmaf(a0.y, z[k][1], x);
+          x = fmaf(a0.z, z[k][2], x);
+          x = fmaf(a0.w, z[k][3], x);
+          x = fmaf(a1.x, z[k][4], x);
+          x = fmaf(a1.y, z[k][5], x);
+          x = fmaf(a1.z, z[k][6], x);
+          x = fmaf(a1.w, z[k][7], x);
+          c[k][t] = x;
+        }
+      }
+    } else {
+      const float4 a0 = __ldg(reinterpret_cast<const float4*>(w)), a1 = __ldg(reinterpret_cast<const float4*>(w) + 1);
+      const float a8 = __ldg(w + 8);
+      const float ww[9] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a8};
+#pragma unroll
+      for (int k = 0; k < P; ++k)
+#pragma unroll
+        for (int t = 0; t < 3; ++t)
+          c[k][t] = fmaf(ww[3 * t], z[k][0], fmaf(ww[3 * t + 1], z[k][1], fmaf(ww[3 * t + 2], z[k][2], c[k][t])));
+    }
+  }
+  // l = 1 triplets: c_t += sum_p z1_p sum_q W[t][3p + q] z2_q (rows padded to 12)
+#pragma unroll 1
+  for (int j = n_pair; j < n_pair + n_trip; ++j) {
+    const uint2 rec = __ldg(fr + j);
+    float4 v1[P], v2[P];
+    gather((int)(rec.y & 0xffu), v1);
+    gather((int)((rec.y >> 8) & 0xffu), v2);
+    float z1[P][3], z2[P][3];
+#pragma unroll
+    for (int k = 0; k < P; ++k) {
+      zrow_l1(v1[k].x, v1[k].y, v1[k].z, z1[k]);
+      zrow_l1(v2[k].x, v2[k].y, v2[k].z, z2[k]);
+    }
+    const float4* w4 = reinterpret_cast<const float4*>(ft + (rec.x & kOffMask));
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+      const float4 a0 = __ldg(w4 + 3 * t), a1 = __ldg(w4 + 3 * t + 1), a2 = __ldg(w4 + 3 * t + 2);
+      const float w[9] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a2.x};
+#pragma unroll
+      for (int k = 0; k < P; ++k) {
+        float x = c[k][t];
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {
+          const float u = fmaf(w[p * 3 + 0], z2[k][0], fmaf(w[p * 3 + 1], z2[k][1], w[p * 3 + 2] * z2[k][2]));
+          x = fmaf(z1[k][p], u, x);
+        }
+        c[k][t] = x;
+      }
+    }
+  }
+  // l = 1 quads (rows padded to 28)
+#pragma unroll 1
+  for (int j = n_pair + n_trip; j < n_pair + n_trip + n_quad; ++j) {
+    const uint2 rec = __ldg(fr + j);
+    float z1[P][3], z2[P][3], z3[P][3];
+    {
+      float4 v[P];
+      gather((int)(rec.y & 0xffu), v);
+#pragma unroll
+      for (int k = 0; k < P; ++k) zrow_l1(v[k].x, v[k].y, v[k].z, z1[k]);
+      gather((int)((rec.y >> 8) & 0xffu), v);
+#pragma unroll
+      for (int k = 0; k < P; ++k) zrow_l1(v[k].x, v[k].y, v[k].z, z2[k]);
+      gather((int)((rec.y >> 16) & 0xffu), v);
+#pragma unroll
+      for (int k = 0; k < P; ++k) zrow_l1(v[k].x, v[k].y, v[k].z, z3[k]);
+    }
+    const float4* w4 = reinterpret_cast<const float4*>(ft + (rec.x & kOffMask));
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+#pragma unroll
+      for (int p = 0; p < 3; ++p) {
+        // W[t][p][qq][:] for qq = 0..2 lives in floats 9p .. 9p + 8 of row t
+        float w[9];
+#pragma unroll
+        for (int m = 0; m < 9; ++m) w[m] = __ldg(reinterpret_cast<const float*>(w4 + 7 * t) + 9 * p + m);
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+          float t2 = 0.0f;
+#pragma unroll
+          for (int qq = 0; qq < 3; ++qq) {
+            const float t3 = fmaf(w[qq * 3], z3[k][0], fmaf(w[qq * 3 + 1], z3[k][1], w[qq * 3 + 2] * z3[k][2]));
+            t2 = fmaf(z2[k][qq], t3, t2);
+          }
+          c[k][t] = fmaf(z1[k][p], t2, c[k][t]);
+        }
+      }
+    }
+  }
+  if (n_one) {
+    const float* w = ft + (__ldg(fr + n_pair + n_trip + n_quad).x & kOffMask);
+#pragma unroll
+    for (int t = 0; t < NR; ++t) {
+      const float wt = __ldg(w + t);
+#pragma unroll
+      for (int k = 0; k < P; ++k) c[k][t] += wt;
+    }
+  }
+}
+
 template <int LMAX, int P>
 __device__ void rep_colour(const SweepArgs& a, int col, unsigned long long* s_dE, unsigned int* s_cnt,
                            const float* zsm) {
@@ -1032,152 +1187,8 @@ __device__ void rep_colour(const SweepArgs& a, int col, unsigned long long* s_dE
     bool ok[P];
 #pragma unroll
     for (int k = 0; k < P; ++k) ok[k] = g + k * G < R;
-    const int n0 = dsc.y, j0 = dsc.z;
-    const uint32_t cnt = (uint32_t)dsc.w;
-    const int n_pair = (int)(cnt & 0xffu), n_trip = (int)((cnt >> 8) & 0xffu), n_quad = (int)((cnt >> 16) & 0xffu);
-    const int n_one = (dsc.x >> 31) & 1;
-    const uint2* __restrict__ fr = L.frec + j0;
-    const int32_t* __restrict__ nbl = L.nb_list + n0;
-    const float* __restrict__ ft = L.ftensor;
-    // the P replicas' spins of neighbour `loc` (unused replicas read replica g)
-    const bool pf = a.rep_pf != 0;  // grid-uniform
-    auto gather = [&](int loc, float4* v) {
-      const float4* b = sp + (int64_t)__ldg(nbl + loc) * R + g;
-#pragma unroll
-      for (int k = 0; k < P; ++k) v[k] = pf ? __ldg(b + (ok[k] ? k * G : 0)) : __ldcg(b + (ok[k] ? k * G : 0));
-    };
-    if (pf) {  // every neighbour row requested at once; the record walk then hits L1
-      const int nd = (int)(cnt >> 24);
-      for (int k = 0; k < nd; ++k) {
-        const float4* b = sp + (int64_t)__ldg(nbl + k) * R + g;
-#pragma unroll
-        for (int kk = 0; kk < P; ++kk)
-          if (ok[kk]) asm volatile("prefetch.global.L1 [%0];" ::"l"(b + kk * G));
-      }
-    }
     float c[P][NR];
-#pragma unroll
-    for (int k = 0; k < P; ++k)
-#pragma unroll
-      for (int t = 0; t < NR; ++t) c[k][t] = 0.0f;
-    // merged per-neighbour pair blocks: c += W z_nb
-#pragma unroll 1
-    for (int j = 0; j < n_pair; ++j) {
-      const uint2 rec = __ldg(fr + j);
-      float4 v[P];
-      gather((int)(rec.y & 0xffu), v);
-      float z[P][NR];
-#pragma unroll
-      for (int k = 0; k < P; ++k) zrow_nr<NR>(v[k].x, v[k].y, v[k].z, z[k]);
-      const float* w = ft + (rec.x & kOffMask);
-      if constexpr (NR == 8) {
-        const float4* w4 = reinterpret_cast<const float4*>(w);
-#pragma unroll
-        for (int t = 0; t < 8; ++t) {
-          const float4 a0 = __ldg(w4 + 2 * t), a1 = __ldg(w4 + 2 * t + 1);
-#pragma unroll
-          for (int k = 0; k < P; ++k) {
-            float x = c[k][t];
-            x = fmaf(a0.x, z[k][0], x);
-            x = fmaf(a0.y, z[k][1], x);
-            x = fmaf(a0.z, z[k][2], x);
-            x = fmaf(a0.w, z[k][3], x);
-            x = fmaf(a1.x, z[k][4], x);
-            x = fmaf(a1.y, z[k][5], x);
-            x = fmaf(a1.z, z[k][6], x);
-            x = fmaf(a1.w, z[k][7], x);
-            c[k][t] = x;
-          }
-        }
-      } else {
-        const float4 a0 = __ldg(reinterpret_cast<const float4*>(w)), a1 = __ldg(reinterpret_cast<const float4*>(w) + 1);
-        const float a8 = __ldg(w + 8);
-        const float ww[9] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a8};
-#pragma unroll
-        for (int k = 0; k < P; ++k)
-#pragma unroll
-          for (int t = 0; t < 3; ++t)
-            c[k][t] = fmaf(ww[3 * t], z[k][0], fmaf(ww[3 * t + 1], z[k][1], fmaf(ww[3 * t + 2], z[k][2], c[k][t])));
-      }
-    }
-    // l = 1 triplets: c_t += sum_p z1_p sum_q W[t][3p + q] z2_q (rows padded to 12)
-#pragma unroll 1
-    for (int j = n_pair; j < n_pair + n_trip; ++j) {
-      const uint2 rec = __ldg(fr + j);
-      float4 v1[P], v2[P];
-      gather((int)(rec.y & 0xffu), v1);
-      gather((int)((rec.y >> 8) & 0xffu), v2);
-      float z1[P][3], z2[P][3];
-#pragma unroll
-      for (int k = 0; k < P; ++k) {
-        zrow_l1(v1[k].x, v1[k].y, v1[k].z, z1[k]);
-        zrow_l1(v2[k].x, v2[k].y, v2[k].z, z2[k]);
-      }
-      const float4* w4 = reinterpret_cast<const float4*>(ft + (rec.x & kOffMask));
-#pragma unroll
-      for (int t = 0; t < 3; ++t) {
-        const float4 a0 = __ldg(w4 + 3 * t), a1 = __ldg(w4 + 3 * t + 1), a2 = __ldg(w4 + 3 * t + 2);
-        const float w[9] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a2.x};
-#pragma unroll
-        for (int k = 0; k < P; ++k) {
-          float x = c[k][t];
-#pragma unroll
-          for (int p = 0; p < 3; ++p) {
-            const float u = fmaf(w[p * 3 + 0], z2[k][0], fmaf(w[p * 3 + 1], z2[k][1], w[p * 3 + 2] * z2[k][2]));
-            x = fmaf(z1[k][p], u, x);
-          }
-          c[k][t] = x;
-        }
-      }
-    }
-    // l = 1 quads (rows padded to 28)
-#pragma unroll 1
-    for (int j = n_pair + n_trip; j < n_pair + n_trip + n_quad; ++j) {
-      const uint2 rec = __ldg(fr + j);
-      float z1[P][3], z2[P][3], z3[P][3];
-      {
-        float4 v[P];
-        gather((int)(rec.y & 0xffu), v);
-#pragma unroll
-        for (int k = 0; k < P; ++k) zrow_l1(v[k].x, v[k].y, v[k].z, z1[k]);
-        gather((int)((rec.y >> 8) & 0xffu), v);
-#pragma unroll
-        for (int k = 0; k < P; ++k) zrow_l1(v[k].x, v[k].y, v[k].z, z2[k]);
-        gather((int)((rec.y >> 16) & 0xffu), v);
-#pragma unroll
-        for (int k = 0; k < P; ++k) zrow_l1(v[k].x, v[k].y, v[k].z, z3[k]);
-      }
-      const float4* w4 = reinterpret_cast<const float4*>(ft + (rec.x & kOffMask));
-#pragma unroll
-      for (int t = 0; t < 3; ++t) {
-#pragma unroll
-        for (int p = 0; p < 3; ++p) {
-          // W[t][p][qq][:] for qq = 0..2 lives in floats 9p .. 9p + 8 of row t
-          float w[9];
-#pragma unroll
-          for (int m = 0; m < 9; ++m) w[m] = __ldg(reinterpret_cast<const float*>(w4 + 7 * t) + 9 * p + m);
-#pragma unroll
-          for (int k = 0; k < P; ++k) {
-            float t2 = 0.0f;
-#pragma unroll
-            for (int qq = 0; qq < 3; ++qq) {
-              const float t3 = fmaf(w[qq * 3], z3[k][0], fmaf(w[qq * 3 + 1], z3[k][1], w[qq * 3 + 2] * z3[k][2]));
-              t2 = fmaf(z2[k][qq], t3, t2);
-            }
-            c[k][t] = fmaf(z1[k][p], t2, c[k][t]);
-          }
-        }
-      }
-    }
-    if (n_one) {
-      const float* w = ft + (__ldg(fr + n_pair + n_trip + n_quad).x & kOffMask);
-#pragma unroll
-      for (int t = 0; t < NR; ++t) {
-        const float wt = __ldg(w + t);
-#pragma unroll
-        for (int k = 0; k < P; ++k) c[k][t] += wt;
-      }
-    }
+    rep_coeffs<LMAX, P>(L, sp, dsc, R, G, g, ok, a.rep_pf != 0, c);
     // per replica: proposal, dE, decision, write-back
 #pragma unroll
     for (int k = 0; k < P; ++k) {
@@ -1327,7 +1338,16 @@ __device__ __forceinline__ void learned_layer(uint32_t tmem_d, const uint8_t* A,
 // Two warpgroups per CTA: both gather half of a row's environment and each runs the
 // epilogue of half the hidden columns (a warp reads TMEM lanes 32 (warp % 4) ..);
 // warpgroup 0 reads the 20 outputs and draws for its rows.
-__global__ void __launch_bounds__(256) k_learned_fused(SweepArgs a, LearnedNet net, double* lqr) {
+// MH = false: the draws, uniforms and log-density ratios go to a.prop / a.propu / lqr
+// for a sweep kernel to decide. MH = true: the Metropolis-Hastings step runs here as
+// well. Warpgroup 1 walks the records of its row's next item (the replica-parallel
+// coefficients c_t, one replica per thread) while warpgroup 0 draws, hands them over
+// in shared memory, and warpgroup 0 forms dE = sum_t c_t (z_t(new) - z_t(old)),
+// decides and writes the spin. Safe within one launch because no site of the colour
+// is a Hamiltonian neighbour or an environment site of another.
+template <int LMAX, bool MH>
+__global__ void __launch_bounds__(256, 2) k_learned_fused(SweepArgs a, LearnedNet net, double* lqr) {
+  constexpr int NR = (LMAX + 1) * (LMAX + 1) - 1;
   extern __shared__ __align__(1024) uint8_t lsm[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(lsm) + 1023) & ~(uintptr_t)1023);
   uint8_t* sW1 = base;
@@ -1336,6 +1356,11 @@ __global__ void __launch_bounds__(256) k_learned_fused(SweepArgs a, LearnedNet n
   uint8_t* sX = sW3 + 2 * (32u * 64u * 2u);
   uint8_t* sH = sX + kChunkBytes;
   float* sb = reinterpret_cast<float*>(sH + 2 * kChunkBytes);
+  // MH: per-slot accumulators after the biases (dynamic, sized by n_slots), and the
+  // rows' coefficients in the sH tile while it is free (after layer 3 has read it)
+  unsigned long long* s_dE = reinterpret_cast<unsigned long long*>(sb + 288);
+  unsigned int* s_cnt = reinterpret_cast<unsigned int*>(s_dE + a.n_slots);
+  float* sC = reinterpret_cast<float*>(sH);
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tslot;
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -1345,6 +1370,7 @@ __global__ void __launch_bounds__(256) k_learned_fused(SweepArgs a, LearnedNet n
   const int n_items = seg_c[a.n_lat];
   const int n_tiles = (n_items + kTile - 1) / kTile;
   if ((int)blockIdx.x >= n_tiles) return;
+  if (MH) zero_block(a.n_slots, s_dE, s_cnt);
   if (warp == 0) umma::tmem_alloc(&tslot, 256u);
   if (tid == 0) umma::mbar_init(&mbar, 1);
   stage_rows_kmajor(sW1, net.W1, 128, 64);
@@ -1398,8 +1424,23 @@ __global__ void __launch_bounds__(256) k_learned_fused(SweepArgs a, LearnedNet n
     if (wg) g.x[18] = __float2bfloat16_rn(g.tau);
     else g.e = sp[(int64_t)g.s * L.R + g.r];
   };
+  // MH, warpgroup 1: the coefficients of a gathered row's item
+  auto coeffs = [&](const Gather& g, float (&cc)[NR]) {
+#pragma unroll
+    for (int t = 0; t < NR; ++t) cc[t] = 0.0f;
+    if (!g.valid) return;
+    const DevLattice& L = a.lat[g.li];
+    const int4 dsc = __ldg(L.idesc + __ldg(L.color_ptr + col) + g.q);
+    const bool one[1] = {true};
+    float c1[1][NR];
+    rep_coeffs<LMAX, 1>(L, a.spins + L.spin_off, dsc, L.R, L.R, g.r, one, true, c1);
+#pragma unroll
+    for (int t = 0; t < NR; ++t) cc[t] = c1[0][t];
+  };
   Gather cur, nxt;
   gather(blockIdx.x, cur);
+  float ccur[NR];
+  if (MH && wg == 1) coeffs(cur, ccur);
   for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
     const int item = tile * kTile + row;
     const bool valid = cur.valid;
@@ -1467,10 +1508,14 @@ __global__ void __launch_bounds__(256) k_learned_fused(SweepArgs a, LearnedNet n
     if (wg == 0) {
 #pragma unroll
       for (int c0 = 0; c0 < 32; c0 += 8) umma::tmem_ld8(tmem + lane_base + (uint32_t)c0, o + c0);
+    } else if (MH) {
+#pragma unroll
+      for (int t = 0; t < NR; ++t) sC[row * NR + t] = ccur[t];
     }
     umma::fence_before();
     __syncthreads();  // every thread has read TMEM and the tiles before the next tile reuses them
     gather(tile + gridDim.x, nxt);  // the next tile's loads are in flight during this tile's draw
+    if (MH && wg == 1) coeffs(nxt, ccur);
     cur = nxt;
     if (wg != 0 || !valid || !ok) continue;
 #pragma unroll
@@ -1485,12 +1530,41 @@ __global__ void __launch_bounds__(256) k_learned_fused(SweepArgs a, LearnedNet n
     float xs[3];
     vmf::sample_f(mix, (float)philox_uniform(b0.w0, b0.w1), (float)philox_uniform(b0.w2, b0.w3),
                   (float)philox_uniform(b1.w0, b1.w1), xs);
-    const int idx = a.item_base[col] + item;
-    a.prop[idx] = make_float4(xs[0], xs[1], xs[2], 0.0f);
-    a.propu[idx] = philox_uniform(b1.w2, b1.w3);
-    lqr[idx] = (double)(vmf::log_q_f(mix, e.x, e.y, e.z) - vmf::log_q_f(mix, xs[0], xs[1], xs[2]));
+    const double u = philox_uniform(b1.w2, b1.w3);
+    const double lq = (double)(vmf::log_q_f(mix, e.x, e.y, e.z) - vmf::log_q_f(mix, xs[0], xs[1], xs[2]));
+    if (!MH) {
+      const int idx = a.item_base[col] + item;
+      a.prop[idx] = make_float4(xs[0], xs[1], xs[2], 0.0f);
+      a.propu[idx] = u;
+      lqr[idx] = lq;
+      continue;
+    }
+    float zo[NR], zn[NR];
+    zrow_nr<NR>(e.x, e.y, e.z, zo);
+    zrow_nr<NR>(xs[0], xs[1], xs[2], zn);
+    float dE = 0.0f;
+#pragma unroll
+    for (int t = 0; t < NR; ++t) dE = fmaf(sC[row * NR + t], zn[t] - zo[t], dE);
+    const double la = -a.beta[rung] * (double)dE + lq;
+    const bool acc_ok = la >= 0.0 || u < exp(la);
+    if (acc_ok) {
+      a.spins[L.spin_off + (int64_t)s * L.R + r] = make_float4(xs[0], xs[1], xs[2], 0.0f);
+      atomicAdd(s_dE + slot, (unsigned long long)llrint((double)dE * kFixScale));
+      atomicAdd(s_cnt + 3 * slot + 0, 1u);
+    }
+    if (a.rec_prop != nullptr && li == 0 && r == 0 && a.pass + 1 < kRecPasses) {
+      const int64_t qq = (int64_t)(a.pass + 1) * L.n_sites + s;
+      a.rec_prop[3 * qq + 0] = xs[0];
+      a.rec_prop[3 * qq + 1] = xs[1];
+      a.rec_prop[3 * qq + 2] = xs[2];
+      a.rec_u[qq] = u;
+      a.rec_dE[qq] = dE;
+      a.rec_acc[qq] = (uint8_t)(acc_ok ? 1 : 0);
+      if (a.rec_lqr != nullptr) a.rec_lqr[s] = lq;
+    }
   }
   if (!ok && tid == 0 && net.err) atomicExch(net.err, 1);
+  if (MH) flush_block(a, s_dE, s_cnt);
   umma::fence_before();
   __syncthreads();
   if (warp == 0) {
@@ -2716,12 +2790,22 @@ int max_colour_items(const scemc_ensemble* E) {
 
 // Learned Metropolis pass: per colour, the fused network + mixture-draw kernel, then
 // the sweep kernel on those proposals.
+// The fused learned kernel with the Metropolis-Hastings decision, and its dynamic
+// shared memory (the per-slot accumulators follow the network's tiles).
+using LearnedFn = void (*)(SweepArgs, LearnedNet, double*);
+LearnedFn learned_mh_kernel(int lmax) { return lmax == 1 ? k_learned_fused<1, true> : k_learned_fused<2, true>; }
+size_t learned_smem(const scemc_ensemble* E, bool mh) {
+  return kLearnedSmem + (mh ? (size_t)20 * E->n_slots + 16 : 0);
+}
+
 int32_t prepare_learned(scemc_ensemble* E) {
   int32_t rc;
   if ((rc = ensure_props(E))) return rc;
   if (!E->d_lqr && (rc = dalloc(&E->d_lqr, (size_t)std::max<int32_t>(E->item_base.back(), 1)))) return rc;
-  CUDA_TRY(cudaFuncSetAttribute((const void*)k_learned_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  CUDA_TRY(cudaFuncSetAttribute((const void*)k_learned_fused<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)kLearnedSmem));
+  CUDA_TRY(cudaFuncSetAttribute((const void*)learned_mh_kernel(E->lmax), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)learned_smem(E, true)));
   return SCEMC_OK;
 }
 
@@ -2780,21 +2864,19 @@ int32_t run_learned_pass(scemc_ensemble* E, const Launch& Lc) {
     a.colour = c;
     a.lqr = nullptr;
     const int tiles = (n + kTile - 1) / kTile;
+    const unsigned grid = (unsigned)std::min(tiles, 2 * sm_count(E->device));
     ++E->launches;
-    k_learned_fused<<<(unsigned)std::min(tiles, 2 * sm_count(E->device)), 256, kLearnedSmem, E->stream>>>(
-        a, net, E->d_lqr);
+    if (Lc.rep) {  // the replica-parallel decision runs inside the fused kernel
+      const auto fn = learned_mh_kernel(E->lmax);
+      fn<<<grid, 256, learned_smem(E, true), E->stream>>>(a, net, E->d_lqr);
+      CUDA_TRY(cudaGetLastError());
+      continue;
+    }
+    k_learned_fused<1, false><<<grid, 256, kLearnedSmem, E->stream>>>(a, net, E->d_lqr);
     CUDA_TRY(cudaGetLastError());
     a.lqr = E->d_lqr;
     ++E->launches;
-    if (Lc.rep) {
-      const int threads = 256;
-      const size_t smem = fast_param_floats(E->n_slots) * sizeof(float);
-      const RepForm f = rep_form(E, c, Lc.rep_p);
-      a.rep_pf = f.pf;
-      CUDA_TRY(cudaFuncSetAttribute((const void*)f.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      f.fn<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(cap, (f.nt + threads - 1) / threads)), threads, smem,
-             E->stream>>>(a);
-    } else {
+    {
       int threads;
       size_t smem;
       fast_shape(E, &threads, &smem);

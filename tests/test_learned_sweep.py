@@ -56,7 +56,10 @@ def test_learned_pass_replay(gpu, kernel):
         pre = b.download()["configs"][0].copy()
         cfg = pre.copy()
         b.record(True)
+        n0 = b.launches()
         b.run(1, kernel=kernel, proposals=3, mode=1)
+        # kernel 3 decides inside the fused network kernel: one launch per colour
+        assert b.launches() - n0 == H.n_colors * (1 if kernel == 3 else 2) + 1
         prop, u, dE32, flag = b.fetch_record(-1)
         lqr = b.fetch_record_ratio()
         assert np.all(flag != 3)
