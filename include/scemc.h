@@ -289,6 +289,17 @@ int32_t scemc_batch_download(const scemc_batch* b, double* configs, double* ener
                              int64_t* counters, int64_t* swaps, double* steps, double* max_drift);
 /* Resets the per-rung counters (acc/att metro, acc/att or, swaps) and max_drift. */
 int32_t scemc_batch_reset_counters(scemc_batch* b);
+/* Checkpoint of a batch's mutable state, for the gpu_pt lane block of a checkpoint
+ * (src/checkpoint.jl:388-425, docs/specs/checkpoint-schema.md:83-100): the FP32 spins
+ * bit for bit, running energies, rung maps, counters, swap counters, steps, device
+ * keys, betas, adaptation windows, drift and the sweep counter with the exchange
+ * parity. The keyed Philox streams have no other state, so a batch loaded with the
+ * blob continues exactly as the saved one would. The tables are not included; the
+ * blob records each table's size and replica count, and loading it into a batch of
+ * another shape fails with SCEMC_ERR_ARG. Pending measurement records are dropped. */
+int32_t scemc_batch_state_bytes(const scemc_batch* b, int64_t* bytes);
+int32_t scemc_batch_save_state(scemc_batch* b, void* buf, int64_t bytes);
+int32_t scemc_batch_load_state(scemc_batch* b, const void* buf, int64_t bytes);
 /* Measurement records written by scemc_batch_run since the last fetch: n_records
  * rows of (n_slots x record_len) FP64, indexed by RUNG, each
  * {E, mx, my, mz, sub_x1, sub_y1, sub_z1, ...} with m over active sites and the

@@ -93,6 +93,9 @@ SIGNATURES = [
     ("scemc_batch_stream", C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
     ("scemc_batch_upload", C.c_int32, [C.c_void_p, F64P, F64P]),
     ("scemc_host_register", C.c_int32, [C.c_void_p, C.c_int64]),
+    ("scemc_batch_state_bytes", C.c_int32, [C.c_void_p, I64P]),
+    ("scemc_batch_save_state", C.c_int32, [C.c_void_p, C.c_void_p, C.c_int64]),
+    ("scemc_batch_load_state", C.c_int32, [C.c_void_p, C.c_void_p, C.c_int64]),
     ("scemc_host_unregister", C.c_int32, [C.c_void_p]),
     ("scemc_batch_profile", C.c_int32, [C.c_void_p, C.c_int32]),
     ("scemc_batch_kernel_time", C.c_int32, [C.c_void_p, F64P, I64P]),

@@ -3713,6 +3713,103 @@ int32_t scemc_batch_download(const scemc_batch* b, double* configs, double* ener
   return payload_download(b, d);
 }
 
+namespace {
+// Saved-state blob: a header, then the device arrays in a fixed order, each padded to
+// 8 bytes.
+constexpr char kStateMagic[8] = {'S', 'C', 'E', 'M', 'C', 'S', 'T', '1'};
+struct StateHeader {
+  char magic[8];
+  int32_t version, n_tables, n_slots, pad;
+  int64_t n_spins, sweep_index;
+  uint64_t exchange_seed;
+};
+struct StatePart {
+  void* dev;
+  size_t bytes;
+};
+std::vector<StatePart> state_parts(const scemc_ensemble* E) {
+  const size_t n = (size_t)E->n_slots;
+  return {{E->d_spins, sizeof(float4) * (size_t)E->n_spins}, {E->d_energy, 8 * n}, {E->d_dEfix, 8 * n},
+          {E->d_cnt, 32 * n}, {E->d_win, 16 * n}, {E->d_swaps, 16 * n}, {E->d_beta, 8 * n}, {E->d_step, 8 * n},
+          {E->d_seed, 8 * n}, {E->d_slot_of_rung, 4 * n}, {E->d_rung_of_slot, 4 * n}, {E->d_max_drift, 8 * n},
+          {E->d_drift, 8 * n}, {E->d_st, sizeof(EnsState)}};
+}
+size_t state_bytes(const scemc_ensemble* E) {
+  size_t b = sizeof(StateHeader) + 8 * E->tabs.size();
+  for (const StatePart& p : state_parts(E)) b += (p.bytes + 7) & ~(size_t)7;
+  return b;
+}
+}  // namespace
+
+int32_t scemc_batch_state_bytes(const scemc_batch* b, int64_t* bytes) {
+  if (!b || !bytes) return fail(SCEMC_ERR_ARG, "NULL argument");
+  *bytes = (int64_t)state_bytes(b);
+  return SCEMC_OK;
+}
+
+int32_t scemc_batch_save_state(scemc_batch* b, void* buf, int64_t bytes) {
+  if (!b || !buf) return fail(SCEMC_ERR_ARG, "NULL argument");
+  if (bytes < (int64_t)state_bytes(b)) return fail(SCEMC_ERR_ARG, "state buffer too small");
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  auto* p = static_cast<unsigned char*>(buf);
+  StateHeader h{};
+  std::memcpy(h.magic, kStateMagic, 8);
+  h.version = 1;
+  h.n_tables = (int32_t)b->tabs.size();
+  h.n_slots = b->n_slots;
+  h.n_spins = b->n_spins;
+  h.sweep_index = b->sweep_index;
+  h.exchange_seed = b->exchange_seed;
+  std::memcpy(p, &h, sizeof h);
+  p += sizeof h;
+  for (size_t i = 0; i < b->tabs.size(); ++i) {
+    const int32_t shape[2] = {b->tabs[i]->n_sites, b->R[i]};
+    std::memcpy(p, shape, 8);
+    p += 8;
+  }
+  for (const StatePart& part : state_parts(b)) {
+    CUDA_TRY(cudaMemcpyAsync(p, part.dev, part.bytes, cudaMemcpyDeviceToHost, b->stream));
+    p += (part.bytes + 7) & ~(size_t)7;
+  }
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  return SCEMC_OK;
+}
+
+int32_t scemc_batch_load_state(scemc_batch* b, const void* buf, int64_t bytes) {
+  if (!b || !buf) return fail(SCEMC_ERR_ARG, "NULL argument");
+  if (bytes < (int64_t)(sizeof(StateHeader) + 8 * b->tabs.size()))
+    return fail(SCEMC_ERR_ARG, "state blob truncated");
+  const auto* p = static_cast<const unsigned char*>(buf);
+  StateHeader h;
+  std::memcpy(&h, p, sizeof h);
+  if (std::memcmp(h.magic, kStateMagic, 8) != 0 || h.version != 1)
+    return fail(SCEMC_ERR_ARG, "not a batch state blob (magic or version)");
+  if (h.n_tables != (int32_t)b->tabs.size() || h.n_slots != b->n_slots || h.n_spins != b->n_spins)
+    return fail(SCEMC_ERR_ARG, "state blob was saved from a batch of another shape");
+  p += sizeof h;
+  for (size_t i = 0; i < b->tabs.size(); ++i) {
+    int32_t shape[2];
+    std::memcpy(shape, p, 8);
+    if (shape[0] != b->tabs[i]->n_sites || shape[1] != b->R[i])
+      return fail(SCEMC_ERR_ARG, "state blob table " + std::to_string(i + 1) + " has another size or replica count");
+    p += 8;
+  }
+  if (bytes < (int64_t)state_bytes(b)) return fail(SCEMC_ERR_ARG, "state blob truncated");
+  if (h.sweep_index < 0 || h.sweep_index >= 0x7ffffffell) return fail(SCEMC_ERR_ARG, "state blob sweep index");
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  for (const StatePart& part : state_parts(b)) {
+    CUDA_TRY(cudaMemcpyAsync(part.dev, p, part.bytes, cudaMemcpyHostToDevice, b->stream));
+    p += (part.bytes + 7) & ~(size_t)7;
+  }
+  if (b->d_flags)  // data-flow epochs restart from the loaded sweep
+    CUDA_TRY(cudaMemsetAsync(b->d_flags, 0, sizeof(uint32_t) * std::max<int64_t>(b->n_spins, 1), b->stream));
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  b->sweep_index = h.sweep_index;
+  b->exchange_seed = h.exchange_seed;
+  b->meas_n = 0;
+  return SCEMC_OK;
+}
+
 int32_t scemc_batch_reset_counters(scemc_batch* b) {
   if (!b) return fail(SCEMC_ERR_ARG, "batch is NULL");
   const int n = b->n_slots;

@@ -312,6 +312,19 @@ class GPUBatch:
             raise ValueError("one energy per slot is needed")
         check(_lib.lib().scemc_batch_upload(self.h, ptr(cfg, C.c_double), None if en is None else ptr(en, C.c_double)))
 
+    def save_state(self) -> np.ndarray:
+        """The batch's mutable device state as a byte array (scemc_batch_save_state)."""
+        n = C.c_int64()
+        check(_lib.lib().scemc_batch_state_bytes(self.h, C.byref(n)))
+        buf = np.zeros(n.value, np.uint8)
+        check(_lib.lib().scemc_batch_save_state(self.h, buf.ctypes.data, buf.size))
+        return buf
+
+    def load_state(self, buf) -> None:
+        """Restores a state saved from a batch of the same tables and replica counts."""
+        buf = np.ascontiguousarray(buf, np.uint8)
+        check(_lib.lib().scemc_batch_load_state(self.h, buf.ctypes.data, buf.size))
+
     def profile(self, on: bool):
         check(_lib.lib().scemc_batch_profile(self.h, int(bool(on))))
 
@@ -435,7 +448,8 @@ def gpu_run_pt(gHs, *, temperature=None, kT=None, exchange: bool = True, exchang
                or_per_metropolis: int = 0, step: float = 0.6, adapt_target: float = 0.5, adapt_interval: int = 50,
                renorm_interval: int = 1000, nbins: int = 32, init=None, seed: Optional[int] = None,
                lanes_per_site: int = 0, mode: int = 0, chunk: int = 2000, kernel: int = 0, proposals: int = 0,
-               learned=None) -> PTResult:
+               learned=None, checkpoint: Optional[str] = None, checkpoint_interval: int = 0,
+               progress=None) -> PTResult:
     """Parallel tempering on the device (gpu_pt.jl:261-316 semantics; exchanges run on
     the device). `gHs` is one GPUTiledHamiltonian or a list of them: every table set
     gets its own ladder over the same kT values (chains of uneven supercells), and
@@ -447,7 +461,14 @@ def gpu_run_pt(gHs, *, temperature=None, kT=None, exchange: bool = True, exchang
 
     learned=(net, env) registers a learned proposal network (scemc.learned) with the
     batch; proposals=3 then draws every Metropolis proposal from it. The wall time
-    of the measurement phase is returned in extra["measure_s"]."""
+    of the measurement phase is returned in extra["measure_s"].
+
+    checkpoint / checkpoint_interval: every time at least checkpoint_interval sweeps
+    have run since the last write (checked at the end of each `chunk`), and at the
+    thermalisation -> measurement boundary, the run is written to `checkpoint`
+    (gpu_pt kind of src/checkpoint.jl:388-425: progress, the device state of every
+    lane, the measurement accumulators); gpu_resume continues it. progress(phase,
+    done) is called after each chunk."""
     if isinstance(gHs, GPUTiledHamiltonian):
         gHs = [gHs]
     kts = resolve_kt(temperature, kT)
@@ -463,7 +484,7 @@ def gpu_run_pt(gHs, *, temperature=None, kT=None, exchange: bool = True, exchang
     if sweeps_therm < 0 or sweeps_measure < 1 or not (1 <= measure_interval <= sweeps_measure):
         raise ValueError("bad sweep counts / measure_interval")
     if or_per_metropolis < 0 or step <= 0 or not (0 < adapt_target < 1) or adapt_interval < 1 \
-            or renorm_interval < 1 or nbins < 2:
+            or renorm_interval < 1 or nbins < 2 or chunk < 1 or checkpoint_interval < 0:
         raise ValueError("bad run parameters")
     if or_per_metropolis > 0 and not any(np.any(g.host.site_has_l1) for g in gHs):
         raise ValueError("or_per_metropolis > 0 needs an l = 1 spin channel somewhere")
@@ -484,28 +505,112 @@ def gpu_run_pt(gHs, *, temperature=None, kT=None, exchange: bool = True, exchang
     batch.set_betas(np.tile(1.0 / kts, len(gHs)))
     if learned is not None:
         batch.set_learned(*learned)
-    common = dict(or_per_metropolis=or_per_metropolis, exchange=exchange, exchange_interval=exchange_interval,
-                  renorm_interval=renorm_interval, lanes_per_site=lanes_per_site, mode=mode, kernel=kernel,
-                  proposals=proposals)
-    done = 0
-    while done < sweeps_therm:
-        n = min(chunk, sweeps_therm - done)
-        batch.run(n, adapt_interval=adapt_interval, adapt_target=adapt_target, phase_done=done,
-                  phase_total=sweeps_therm, **common)
-        done += n
-    # thermalisation -> measurement boundary: renormalise, fresh counters (gpu_pt.jl:161-179)
-    batch.renormalize()
-    batch.reset_counters()
-    planned = sweeps_measure // measure_interval
-    accs = [StandardAccumulators(g.host.n_cell_atoms, planned, nbins) for g in gHs for _ in range(R)]
+    run = dict(kts=np.asarray(kts, np.float64), exchange=bool(exchange), exchange_interval=int(exchange_interval),
+               sweeps_therm=int(sweeps_therm), sweeps_measure=int(sweeps_measure),
+               measure_interval=int(measure_interval), or_per_metropolis=int(or_per_metropolis), step=float(step),
+               adapt_target=float(adapt_target), adapt_interval=int(adapt_interval),
+               renorm_interval=int(renorm_interval), nbins=int(nbins), seed=int(seed),
+               lanes_per_site=int(lanes_per_site), mode=int(mode), chunk=int(chunk), kernel=int(kernel),
+               proposals=int(proposals), checkpoint_interval=int(checkpoint_interval))
+    ck = _Checkpointer(checkpoint, int(checkpoint_interval), gHs, run)
+    return _drive_pt(gHs, batch, run, "therm", 0, None, 0.0, ck, progress)
+
+
+CHECKPOINT_VERSION = 1
+
+
+def _tables_fingerprint(gHs) -> str:
+    """SHA-256 over every table set's host arrays (the model fingerprint a resume checks)."""
+    import hashlib
+    h = hashlib.sha256()
+    for g in gHs:
+        H = g.host
+        for name in ("site_ptr", "site_inst", "site_slot", "site_prog", "site_col", "site_col2", "sprog_ptr",
+                     "sent_w", "sent_tgt", "color_ptr", "color_sites", "site_active", "site_has_l1"):
+            a = getattr(H, name, None)
+            if a is not None:
+                h.update(name.encode())
+                h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+class _Checkpointer:
+    """Periodic writer of gpu_pt checkpoints (ck.since / ck.interval of checkpoint.jl)."""
+
+    def __init__(self, path, interval, gHs, run):
+        self.path, self.interval, self.run, self.since = path, interval, run, 0
+        self.fingerprint = _tables_fingerprint(gHs) if path else ""
+        self.shapes = np.array([[g.n_sites, g.host.n_colors] for g in gHs], np.int64)
+
+    def tick(self, n, *args):
+        if not self.path or self.interval <= 0:
+            return
+        self.since += n
+        if self.since >= self.interval:
+            self.write(*args)
+
+    def write(self, batch, phase, done, accs, measure_s):
+        if not self.path:
+            return
+        import os
+        self.since = 0
+        d = {"kind": np.array("gpu_pt"), "version": np.array([CHECKPOINT_VERSION], np.int64),
+             "fingerprint": np.array(self.fingerprint), "shapes": self.shapes,
+             "progress/phase": np.array(phase), "progress/done": np.array([done], np.int64),
+             "measure_s": np.array([measure_s]), "state": batch.save_state()}
+        for k, v in self.run.items():
+            d["run/" + k] = np.asarray(v)
+        if accs is not None:
+            for i, acc in enumerate(accs):
+                d.update(acc.state(f"lane/{i}/accs/"))
+        tmp = f"{self.path}.tmp.{os.getpid()}"
+        with open(tmp, "wb") as f:
+            np.savez(f, **d)
+        os.replace(tmp, self.path)
+
+
+def _run_common(run) -> dict:
+    return dict(or_per_metropolis=run["or_per_metropolis"], exchange=run["exchange"],
+                exchange_interval=run["exchange_interval"], renorm_interval=run["renorm_interval"],
+                lanes_per_site=run["lanes_per_site"], mode=run["mode"], kernel=run["kernel"],
+                proposals=run["proposals"])
+
+
+def _drive_pt(gHs, batch, run, phase, done, accs, measure_s, ck, progress) -> PTResult:
+    """The segment loop of gpu_run_pt from (phase, done) on; accs are the measurement
+    accumulators when phase is "measure"."""
+    kts = run["kts"]
+    R = len(kts)
+    common = _run_common(run)
+    chunk = run["chunk"]
+    if phase == "therm":
+        total = run["sweeps_therm"]
+        while done < total:
+            n = min(chunk, total - done)
+            batch.run(n, adapt_interval=run["adapt_interval"], adapt_target=run["adapt_target"], phase_done=done,
+                      phase_total=total, **common)
+            done += n
+            if done < total:
+                ck.tick(n, batch, "therm", done, None, 0.0)
+            if progress is not None:
+                progress("therm", done)
+        # thermalisation -> measurement boundary: renormalise, fresh counters (gpu_pt.jl:161-179)
+        batch.renormalize()
+        batch.reset_counters()
+        phase, done = "measure", 0
+    planned = run["sweeps_measure"] // run["measure_interval"]
+    fresh = accs is None
+    if fresh:
+        accs = [StandardAccumulators(g.host.n_cell_atoms, planned, run["nbins"]) for g in gHs for _ in range(R)]
+        ck.write(batch, "measure", 0, accs, measure_s)
     rec_off = [0]
     for g in gHs:
         rec_off.append(rec_off[-1] + R)
-    done = 0
-    t_meas = time.perf_counter()
-    while done < sweeps_measure:
-        n = min(chunk, sweeps_measure - done)
-        batch.run(n, measure_interval=measure_interval, phase_done=done, phase_total=sweeps_measure, **common)
+    total = run["sweeps_measure"]
+    while done < total:
+        n = min(chunk, total - done)
+        t0 = time.perf_counter()
+        batch.run(n, measure_interval=run["measure_interval"], phase_done=done, phase_total=total, **common)
         done += n
         rec = batch.fetch_measurements()
         for i, acc in enumerate(accs):
@@ -513,7 +618,11 @@ def gpu_run_pt(gHs, *, temperature=None, kT=None, exchange: bool = True, exchang
             A = gHs[li].host.n_cell_atoms
             if len(rec):
                 acc.push_records(rec[:, i, : 4 + 3 * A])
-    measure_s = time.perf_counter() - t_meas
+        measure_s += time.perf_counter() - t0
+        if done < total:
+            ck.tick(n, batch, "measure", done, accs, measure_s)
+        if progress is not None:
+            progress("measure", done)
     st = batch.download()
     points = []
     for i, acc in enumerate(accs):
@@ -532,6 +641,57 @@ def gpu_run_pt(gHs, *, temperature=None, kT=None, exchange: bool = True, exchang
             a, b = sw[rec_off[li] + r]
             swaps.append(b / a if a else np.nan)
     finals = [st["configs"][st["slot_of_rung"][i]] for i in range(len(accs))]
-    return PTResult(points, np.asarray(swaps), finals, seed,
+    return PTResult(points, np.asarray(swaps), finals, run["seed"],
                     extra=dict(energies=st["energies"], slot_of_rung=st["slot_of_rung"], batch=batch,
                                measure_s=measure_s))
+
+
+def gpu_resume(path: str, gHs, *, learned=None, checkpoint: Optional[str] = "", checkpoint_interval=None,
+               progress=None) -> PTResult:
+    """Continues a gpu_run_pt run from its checkpoint and returns the whole run's
+    result, bit-identical to the uninterrupted run (resume of src/checkpoint.jl for the
+    gpu_pt kind). The caller passes the same table sets (checked against the stored
+    fingerprint) and, for a learned run, the same (net, env). By default the resumed
+    run keeps writing to `path` at the stored cadence (checkpoint=None disables it;
+    checkpoint_interval overrides the cadence). The measurement wall time in
+    extra["measure_s"] adds the time before the interruption."""
+    if isinstance(gHs, GPUTiledHamiltonian):
+        gHs = [gHs]
+    with np.load(path, allow_pickle=False) as f:
+        d = {k: f[k] for k in f.files}
+    if str(d.get("kind", "")) != "gpu_pt" or int(d["version"][0]) != CHECKPOINT_VERSION:
+        raise ValueError(f"{path} is not a gpu_pt checkpoint of version {CHECKPOINT_VERSION}")
+    if str(d["fingerprint"]) != _tables_fingerprint(gHs):
+        raise ValueError("the table sets differ from the checkpointed run's (model fingerprint mismatch)")
+    run = {k[4:]: d[k] for k in d if k.startswith("run/")}
+    for k in list(run):
+        v = run[k]
+        if k == "kts":
+            run[k] = np.asarray(v, np.float64)
+        elif v.dtype == np.bool_:
+            run[k] = bool(v)
+        elif np.issubdtype(v.dtype, np.integer):
+            run[k] = int(v)
+        else:
+            run[k] = float(v)
+    kts = run["kts"]
+    R = len(kts)
+    configs = [np.tile([0.0, 0.0, 1.0], (g.n_sites, 1)) for g in gHs for _ in range(R)]
+    batch = GPUBatch(gHs, [R] * len(gHs), configs, np.arange(1, R * len(gHs) + 1, dtype=np.uint64), run["step"],
+                     energies=np.zeros(R * len(gHs)))
+    batch.load_state(d["state"])
+    if learned is not None:
+        batch.set_learned(*learned)
+    phase = str(d["progress/phase"])
+    done = int(d["progress/done"][0])
+    accs = None
+    if phase == "measure":
+        planned = run["sweeps_measure"] // run["measure_interval"]
+        accs = [StandardAccumulators(g.host.n_cell_atoms, planned, run["nbins"]) for g in gHs for _ in range(R)]
+        for i, acc in enumerate(accs):
+            acc.load_state(f"lane/{i}/accs/", d)
+    interval = int(run.get("checkpoint_interval", 0))
+    interval = interval if checkpoint_interval is None else int(checkpoint_interval)
+    run["checkpoint_interval"] = interval
+    ck = _Checkpointer(path if checkpoint == "" else checkpoint, interval, gHs, run)
+    return _drive_pt(gHs, batch, run, phase, done, accs, float(d["measure_s"][0]), ck, progress)

@@ -31,6 +31,22 @@ class LogBinner:
     def push(self, x):
         self.push_many(np.asarray(x, dtype=np.float64).reshape(1, self.ncomp))
 
+    def state(self, prefix: str) -> dict:
+        """Checkpoint arrays (the accs/<obs>/binner block of the checkpoint schema)."""
+        return {prefix + "count": self.count.copy(), prefix + "sums": self.sums.copy(),
+                prefix + "sums2": self.sums2.copy(), prefix + "pending": self.pending.copy(),
+                prefix + "pending_full": self.pending_full.copy(), prefix + "n": np.array([self.n], np.int64)}
+
+    def load_state(self, prefix: str, d) -> None:
+        self.count = np.array(d[prefix + "count"], np.int64)
+        self.sums = np.array(d[prefix + "sums"], np.float64)
+        self.sums2 = np.array(d[prefix + "sums2"], np.float64)
+        self.pending = np.array(d[prefix + "pending"], np.float64)
+        self.pending_full = np.array(d[prefix + "pending_full"], bool)
+        self.n = int(d[prefix + "n"][0])
+        if self.sums.shape != (MAX_LEVELS, self.ncomp):
+            raise ValueError("checkpointed LogBinner has another shape")
+
     def push_many(self, xs: np.ndarray):
         xs = np.asarray(xs, dtype=np.float64).reshape(-1, self.ncomp)
         if len(xs) == 0:
@@ -112,6 +128,18 @@ class BinStore:
     def bin_means(self):
         return self.means[: self.nfull].copy()
 
+    def state(self, prefix: str) -> dict:
+        """Checkpoint arrays (the accs/<obs>/store block of the checkpoint schema)."""
+        return {prefix + "means": self.means.copy(), prefix + "acc": self.acc.copy(),
+                prefix + "ints": np.array([self.bin_size, self.nbins, self.nfull, self.nacc], np.int64)}
+
+    def load_state(self, prefix: str, d) -> None:
+        bs, nb, self.nfull, self.nacc = (int(x) for x in d[prefix + "ints"])
+        if (bs, nb) != (self.bin_size, self.nbins):
+            raise ValueError("checkpointed BinStore has another bin layout")
+        self.means = np.array(d[prefix + "means"], np.float64).reshape(self.nbins, self.ncomp)
+        self.acc = np.array(d[prefix + "acc"], np.float64).reshape(self.ncomp)
+
 
 def jackknife(f, cols):
     """Leave-one-bin-out jackknife (binning.jl:198-218) -> (estimate, error)."""
@@ -173,6 +201,18 @@ class StandardAccumulators:
                       ("sublattice_m", 3 * n_cell_atoms)]
         self.binners = {n: LogBinner(c) for n, c in self.names}
         self.stores = {n: BinStore(c, bs, nbins) for n, c in self.names}
+
+    def state(self, prefix: str) -> dict:
+        d = {}
+        for n, _ in self.names:
+            d.update(self.binners[n].state(f"{prefix}{n}/binner/"))
+            d.update(self.stores[n].state(f"{prefix}{n}/store/"))
+        return d
+
+    def load_state(self, prefix: str, d) -> None:
+        for n, _ in self.names:
+            self.binners[n].load_state(f"{prefix}{n}/binner/", d)
+            self.stores[n].load_state(f"{prefix}{n}/store/", d)
 
     def push_records(self, rec: np.ndarray):
         rec = np.asarray(rec, dtype=np.float64)
