@@ -1001,10 +1001,12 @@ __global__ void __launch_bounds__(256) k_proposals(SweepArgs a) { make_proposals
 // (r = g + k G, those with ok[k]) of the site of descriptor `dsc`, from every record's
 // W block and its neighbours' Z rows. pf: the neighbour rows are prefetched into L1
 // first and read through it (else through L2).
-template <int LMAX, int P>
+// NP > 1: only the records j with j % NP == part (the one-body record with part 0),
+// for NP threads that share one site's walk.
+template <int LMAX, int P, int NP = 1>
 __device__ __forceinline__ void rep_coeffs(const DevLattice& L, const float4* __restrict__ sp, int4 dsc, int R, int G,
                                            int g, const bool (&ok)[P], bool pf,
-                                           float (&c)[P][(LMAX + 1) * (LMAX + 1) - 1]) {
+                                           float (&c)[P][(LMAX + 1) * (LMAX + 1) - 1], int part = 0) {
   constexpr int NR = (LMAX + 1) * (LMAX + 1) - 1;
   const int n0 = dsc.y, j0 = dsc.z;
   const uint32_t cnt = (uint32_t)dsc.w;
@@ -1034,7 +1036,7 @@ __device__ __forceinline__ void rep_coeffs(const DevLattice& L, const float4* __
     for (int t = 0; t < NR; ++t) c[k][t] = 0.0f;
   // merged per-neighbour pair blocks: c += W z_nb
 #pragma unroll 1
-  for (int j = 0; j < n_pair; ++j) {
+  for (int j = part; j < n_pair; j += NP) {
     const uint2 rec = __ldg(fr + j);
     float4 v[P];
     gather((int)(rec.y & 0xffu), v);
@@ -1074,7 +1076,7 @@ __device__ __forceinline__ void rep_coeffs(const DevLattice& L, const float4* __
   }
   // l = 1 triplets: c_t += sum_p z1_p sum_q W[t][3p + q] z2_q (rows padded to 12)
 #pragma unroll 1
-  for (int j = n_pair; j < n_pair + n_trip; ++j) {
+  for (int j = n_pair + part; j < n_pair + n_trip; j += NP) {
     const uint2 rec = __ldg(fr + j);
     float4 v1[P], v2[P];
     gather((int)(rec.y & 0xffu), v1);
@@ -1104,7 +1106,7 @@ __device__ __forceinline__ void rep_coeffs(const DevLattice& L, const float4* __
   }
   // l = 1 quads (rows padded to 28)
 #pragma unroll 1
-  for (int j = n_pair + n_trip; j < n_pair + n_trip + n_quad; ++j) {
+  for (int j = n_pair + n_trip + part; j < n_pair + n_trip + n_quad; j += NP) {
     const uint2 rec = __ldg(fr + j);
     float z1[P][3], z2[P][3], z3[P][3];
     {
@@ -1141,7 +1143,7 @@ __device__ __forceinline__ void rep_coeffs(const DevLattice& L, const float4* __
       }
     }
   }
-  if (n_one) {
+  if (n_one && part == 0) {
     const float* w = ft + (__ldg(fr + n_pair + n_trip + n_quad).x & kOffMask);
 #pragma unroll
     for (int t = 0; t < NR; ++t) {
@@ -1433,14 +1435,14 @@ __global__ void __launch_bounds__(256, 2) k_learned_fused(SweepArgs a, LearnedNe
     const int4 dsc = __ldg(L.idesc + __ldg(L.color_ptr + col) + g.q);
     const bool one[1] = {true};
     float c1[1][NR];
-    rep_coeffs<LMAX, 1>(L, a.spins + L.spin_off, dsc, L.R, L.R, g.r, one, true, c1);
+    rep_coeffs<LMAX, 1, 2>(L, a.spins + L.spin_off, dsc, L.R, L.R, g.r, one, true, c1, wg);
 #pragma unroll
     for (int t = 0; t < NR; ++t) cc[t] = c1[0][t];
   };
   Gather cur, nxt;
   gather(blockIdx.x, cur);
-  float ccur[NR];
-  if (MH && wg == 1) coeffs(cur, ccur);
+  float ccur[NR];  // MH: this warpgroup's half of the current tile's coefficients
+  if (MH) coeffs(cur, ccur);
   for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
     const int item = tile * kTile + row;
     const bool valid = cur.valid;
@@ -1517,7 +1519,7 @@ __global__ void __launch_bounds__(256, 2) k_learned_fused(SweepArgs a, LearnedNe
     gather(tile + gridDim.x, nxt);  // the next tile's loads are in flight during this tile's draw
     if (MH && wg == 1) coeffs(nxt, ccur);
     cur = nxt;
-    if (wg != 0 || !valid || !ok) continue;
+    auto draw_decide = [&]() {
 #pragma unroll
     for (int j = 0; j < 32; ++j) o[j] += sb[256 + j];
     const DevLattice& L = a.lat[li];
@@ -1537,14 +1539,14 @@ __global__ void __launch_bounds__(256, 2) k_learned_fused(SweepArgs a, LearnedNe
       a.prop[idx] = make_float4(xs[0], xs[1], xs[2], 0.0f);
       a.propu[idx] = u;
       lqr[idx] = lq;
-      continue;
+      return;
     }
     float zo[NR], zn[NR];
     zrow_nr<NR>(e.x, e.y, e.z, zo);
     zrow_nr<NR>(xs[0], xs[1], xs[2], zn);
     float dE = 0.0f;
 #pragma unroll
-    for (int t = 0; t < NR; ++t) dE = fmaf(sC[row * NR + t], zn[t] - zo[t], dE);
+    for (int t = 0; t < NR; ++t) dE = fmaf(ccur[t] + sC[row * NR + t], zn[t] - zo[t], dE);
     const double la = -a.beta[rung] * (double)dE + lq;
     const bool acc_ok = la >= 0.0 || u < exp(la);
     if (acc_ok) {
@@ -1562,6 +1564,9 @@ __global__ void __launch_bounds__(256, 2) k_learned_fused(SweepArgs a, LearnedNe
       a.rec_acc[qq] = (uint8_t)(acc_ok ? 1 : 0);
       if (a.rec_lqr != nullptr) a.rec_lqr[s] = lq;
     }
+    };
+    if (wg == 0 && valid && ok) draw_decide();
+    if (MH && wg == 0) coeffs(cur, ccur);  // the next tile's half, after this tile's decisions
   }
   if (!ok && tid == 0 && net.err) atomicExch(net.err, 1);
   if (MH) flush_block(a, s_dE, s_cnt);
