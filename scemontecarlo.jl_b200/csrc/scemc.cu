@@ -987,10 +987,10 @@ __global__ void __launch_bounds__(256) k_proposals(SweepArgs a) { make_proposals
 // Every coupling word (descriptor, record, W block) a thread loads serves its P
 // replicas. When a colour fills many waves (fcc 64^3 x 32 rungs) the load's register
 // writeback, not the FMA pipe, bounds a one-replica thread and P = 2 at 80 registers
-// measured fastest (7.7 against 9.3 ms per pass at fcc 48^3). When it fills at most
-// two waves (the PT ladders) each thread's record walk is latency-bound and P = 1
-// at 64 registers, with twice the threads, measured fastest (0.49 against 0.54 ms
-// per step).
+// measured fastest (7.7 against 9.3 ms per pass at fcc 48^3). When a colour is small
+// (the PT ladders) each thread's record walk is latency-bound: P = 1 at 64
+// registers with twice the threads measured 0.49 against 0.54 ms per step, and two
+// threads per item (NP = 2, rep_form) 0.41.
 // Each replica keeps its NR coefficients in registers, c_t = sum_j W_j[t, :] . z_j,
 // and forms
 // dE = sum_t c_t (znew_t - zold_t) itself (no shuffles or shared-memory rows). Built
@@ -1154,7 +1154,10 @@ __device__ __forceinline__ void rep_coeffs(const DevLattice& L, const float4* __
   }
 }
 
-template <int LMAX, int P>
+// NP = 2: two adjacent threads share an item's record walk (alternate records) and
+// add their halves with one shuffle; the even thread decides. For colours too small
+// to fill the GPU, where each thread's walk is the critical path.
+template <int LMAX, int P, int NP>
 __device__ void rep_colour(const SweepArgs& a, int col, unsigned long long* s_dE, unsigned int* s_cnt,
                            const float* zsm) {
   constexpr int NR = (LMAX + 1) * (LMAX + 1) - 1;
@@ -1168,8 +1171,9 @@ __device__ void rep_colour(const SweepArgs& a, int col, unsigned long long* s_dE
     const int R = a.lat[l].R;
     n_threads += (seg_c[l + 1] - seg_c[l]) / R * ((R + P - 1) / P);
   }
-  const int stride = gridDim.x * blockDim.x;
-  for (int tid = blockIdx.x * blockDim.x + threadIdx.x; tid < n_threads; tid += stride) {
+  const int stride = gridDim.x * blockDim.x;  // a multiple of 32: the NP threads of an item stay in one warp
+  for (int t0 = blockIdx.x * blockDim.x + threadIdx.x; t0 < n_threads * NP; t0 += stride) {
+    const int tid = t0 / NP, part = t0 % NP;
     int li = 0, base = 0, G = 1, R = 1;
     for (; li < a.n_lat; ++li) {
       R = a.lat[li].R;
@@ -1190,7 +1194,15 @@ __device__ void rep_colour(const SweepArgs& a, int col, unsigned long long* s_dE
 #pragma unroll
     for (int k = 0; k < P; ++k) ok[k] = g + k * G < R;
     float c[P][NR];
-    rep_coeffs<LMAX, P>(L, sp, dsc, R, G, g, ok, a.rep_pf != 0, c);
+    rep_coeffs<LMAX, P, NP>(L, sp, dsc, R, G, g, ok, a.rep_pf != 0, c, part);
+    if (NP == 2) {
+      const unsigned pair = 3u << (threadIdx.x & 30u);
+#pragma unroll
+      for (int k = 0; k < P; ++k)
+#pragma unroll
+        for (int t = 0; t < NR; ++t) c[k][t] += __shfl_xor_sync(pair, c[k][t], 1);
+      if (part != 0) continue;
+    }
     // per replica: proposal, dE, decision, write-back
 #pragma unroll
     for (int k = 0; k < P; ++k) {
@@ -1580,14 +1592,14 @@ __global__ void __launch_bounds__(256, 2) k_learned_fused(SweepArgs a, LearnedNe
 
 // P = 2 at 80 registers (three 256-thread blocks per SM); P = 1 at 64 registers
 // (four blocks per SM).
-template <int LMAX, int P>
+template <int LMAX, int P, int NP>
 __global__ void __launch_bounds__(256, P == 1 ? 4 : 3) k_rep_colour(SweepArgs a) {
   extern __shared__ __align__(16) float zsm[];
   __shared__ unsigned long long s_dE[kMaxSlots];
   __shared__ unsigned int s_cnt[3 * kMaxSlots];
   zero_block(a.n_slots, s_dE, s_cnt);
   stage_params(a, zsm);
-  rep_colour<LMAX, P>(a, a.colour, s_dE, s_cnt, zsm);
+  rep_colour<LMAX, P, NP>(a, a.colour, s_dE, s_cnt, zsm);
   flush_block(a, s_dE, s_cnt);
 }
 
@@ -2823,10 +2835,9 @@ int64_t rep_threads(const scemc_ensemble* E, int c, int P) {
   return nt;
 }
 
-// The replica-parallel form of one colour launch: replicas per thread (`forced`, or
-// 1 when the one-replica threads fill at most two waves of four 256-thread blocks per
-// SM, else 2) and whether each thread first prefetches its neighbour rows into L1
-// (at most two waves of resident threads: the record walk is then latency-bound;
+// The replica-parallel form of one colour launch: replicas per thread P, threads per
+// item NP, and whether each thread first prefetches its neighbour rows into L1 (at
+// most two waves of resident threads: the record walk is then latency-bound;
 // measured 9 % faster on the PT ladders, 7 % slower at fcc 48^3 x 32).
 struct RepForm {
   int P;
@@ -2837,11 +2848,24 @@ struct RepForm {
 RepForm rep_form(const scemc_ensemble* E, int c, int forced) {
   RepForm f;
   const int64_t sms = sm_count(E->device);
-  f.P = forced == 1 || forced == 2 ? forced : (rep_threads(E, c, 1) <= sms * 1024 * 2 ? 1 : 2);
-  f.nt = rep_threads(E, c, f.P);
+  const int64_t nt1 = rep_threads(E, c, 1);
+  // Small colours (twice the one-replica threads still fit one wave of four
+  // 256-thread blocks per SM): one replica per thread and two threads per item, for
+  // the most parallel walk. Larger: two replicas per thread, one thread per item.
+  // Measured (ms per sweep of 16 rungs, bcc body-4): 32^3 0.49 against 0.55 with
+  // P = 2; 40^3 (above the threshold) 0.70 with P = 2 against 0.76 with P = 1.
+  // NP depends on the colour's size only, so a forced P does not change the chains.
+  const int NP = 2 * nt1 <= sms * 1024 ? 2 : 1;
+  f.P = forced == 1 || forced == 2 ? forced : (NP == 2 ? 1 : 2);
+  f.nt = rep_threads(E, c, f.P) * NP;
   f.pf = f.nt <= sms * (f.P == 1 ? 1024 : 768) * 2 ? 1 : 0;
-  if (E->lmax == 1) f.fn = f.P == 1 ? k_rep_colour<1, 1> : k_rep_colour<1, 2>;
-  else f.fn = f.P == 1 ? k_rep_colour<2, 1> : k_rep_colour<2, 2>;
+  if (E->lmax == 1) {
+    if (f.P == 1) f.fn = NP == 2 ? k_rep_colour<1, 1, 2> : k_rep_colour<1, 1, 1>;
+    else f.fn = NP == 2 ? k_rep_colour<1, 2, 2> : k_rep_colour<1, 2, 1>;
+  } else {
+    if (f.P == 1) f.fn = NP == 2 ? k_rep_colour<2, 1, 2> : k_rep_colour<2, 1, 1>;
+    else f.fn = NP == 2 ? k_rep_colour<2, 2, 2> : k_rep_colour<2, 2, 1>;
+  }
   return f;
 }
 
