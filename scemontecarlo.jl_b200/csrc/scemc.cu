@@ -1021,8 +1021,12 @@ __device__ __forceinline__ void rep_coeffs(const DevLattice& L, const float4* __
 #pragma unroll
     for (int k = 0; k < P; ++k) v[k] = pf ? __ldg(b + (ok[k] ? k * G : 0)) : __ldcg(b + (ok[k] ? k * G : 0));
   };
-  if (pf) {  // every neighbour row requested at once; the record walk then hits L1
+  if (pf) {  // the site's records and every neighbour row requested at once; the walk then hits L1
     const int nd = (int)(cnt >> 24);
+    const int nrec = n_pair + n_trip + n_quad + n_one;
+    for (int j = 0; j < nrec; j += 16) asm volatile("prefetch.global.L1 [%0];" ::"l"(fr + j));
+    if (nrec > 0) asm volatile("prefetch.global.L1 [%0];" ::"l"(fr + nrec - 1));  // an unaligned run's last line
+#pragma unroll 4
     for (int k = 0; k < nd; ++k) {
       const float4* b = sp + (int64_t)__ldg(nbl + k) * R + g;
 #pragma unroll
