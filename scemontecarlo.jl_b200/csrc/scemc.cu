@@ -80,6 +80,11 @@ constexpr int kKindShift = 26;
 constexpr int32_t kOffMask = (1 << kKindShift) - 1;
 constexpr double kFixScale = 1099511627776.0;  // 2^40: fixed-point unit of dE sums
 constexpr int kMaxSlots = 512;
+// Layout of the per-slot readback block (byte offsets per slot count n): energy (8n),
+// slot_of_rung (4n, padded to 8n), counters (32n), swaps (16n), steps (8n),
+// max_drift (8n).
+constexpr size_t kRbEnergy = 0, kRbSlotOfRung = 8, kRbCounters = 16, kRbSwaps = 48, kRbSteps = 64,
+                 kRbMaxDrift = 72, kReadbackBytesPerSlot = 80;
 constexpr int kChunk = 1024;  // fixed reduction chunk (sites or instances)
 constexpr int kMaxCellAtoms = 64;
 constexpr int kRecPasses = 4;  // replay record: Metropolis + up to 3 overrelaxation passes
@@ -1906,6 +1911,8 @@ struct scemc_ensemble {
   long long barrier_limit_ns = 2000000000ll;
   int coop_blocks = 0;  // cached co-resident grid size for the persistent form
   int coop_G = -1;
+  unsigned char* d_readback = nullptr;  // energy, slot_of_rung, counters, swaps, steps, max_drift (one block)
+  double* d_energy_in = nullptr;        // energies of an upload, committed on the device
   double* d_cfg64 = nullptr;  // device copy of a host payload (3 x n_spins FP64)
   unsigned long long* d_bad = nullptr;  // first non-finite payload spin
   unsigned char* h_small = nullptr;     // pinned: flag, energies in, per-slot arrays out
@@ -1955,10 +1962,9 @@ struct scemc_ensemble {
       if (p) cudaFree(p);
     for (void* p : qs)
       if (p) cudaFree(p);
-    void* ps[] = {d_lat,   d_spins, d_seg,  d_energy,       d_dEfix,        d_cnt,       d_win,    d_swaps,
-                  d_beta,  d_step,  d_seed, d_slot_of_rung, d_rung_of_slot, d_max_drift, d_drift,  d_eout,
-                  d_gs,    d_st,    d_partial, d_meas,      d_rprop,        d_ru,        d_rdE,    d_racc,
-                  d_cfg64, d_bad};
+    void* ps[] = {d_lat,   d_spins,   d_seg,  d_readback, d_dEfix, d_win,   d_beta,  d_seed,
+                  d_rung_of_slot, d_drift, d_eout, d_gs, d_st, d_partial, d_meas, d_rprop, d_ru, d_rdE, d_racc,
+                  d_cfg64, d_bad,   d_energy_in};
     for (void* p : ps)
       if (p) cudaFree(p);
     if (stream) cudaStreamDestroy(stream);
@@ -2423,8 +2429,14 @@ __global__ void k_payload_check(const double* cfg, int64_t n, unsigned long long
   }
 }
 
-// One table, walked in device order so that the float4 stores coalesce.
-__global__ void k_payload_in(const double* cfg, int64_t n_sites, int R, float4* spins) {
+// One table, walked in device order so that the float4 stores coalesce. Writes
+// nothing when the check flagged a spin; block 0 of the first table's launch also
+// commits the uploaded energies.
+__global__ void k_payload_in(const double* cfg, int64_t n_sites, int R, float4* spins, const unsigned long long* bad,
+                             const double* energy_in, double* energy, int n_slots) {
+  if (*bad != ~0ull) return;
+  if (energy_in != nullptr && blockIdx.x == 0)
+    for (int i = threadIdx.x; i < n_slots; i += blockDim.x) energy[i] = energy_in[i];
   const int64_t tot = n_sites * R;
   for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < tot; j += (int64_t)gridDim.x * blockDim.x) {
     const int64_t s = j / R;
@@ -2450,14 +2462,16 @@ unsigned payload_blocks(const scemc_ensemble* E, int64_t n) {
 }
 
 // Pinned host area for the small transfers: the non-finite flag, the energies on
-// the way in, and the per-slot arrays on the way out.
+// the way in, and the per-slot readback block on the way out.
 constexpr size_t kSmallIn = 16;
 size_t small_out_offset(int n_slots) { return kSmallIn + (((size_t)8 * n_slots + 15) & ~(size_t)15); }
-size_t small_bytes(int n_slots) { return small_out_offset(n_slots) + (size_t)80 * n_slots + 64; }
+size_t small_bytes(int n_slots) { return small_out_offset(n_slots) + kReadbackBytesPerSlot * n_slots + 64; }
 
 // Replaces every chain's spins (and, when `energies` is given, the running
 // energies) from a host payload. Nothing on the device changes when an input is
-// not finite; returns after the host buffers may be reused.
+// not finite: the kernels commit only when the check found nothing, and the host
+// reads the check's result after one wait. Returns after the host buffers may be
+// reused.
 int32_t payload_upload(scemc_ensemble* E, const double* cfgs, const double* energies) {
   if (energies)
     for (int i = 0; i < E->n_slots; ++i)
@@ -2465,9 +2479,21 @@ int32_t payload_upload(scemc_ensemble* E, const double* cfgs, const double* ener
   const int64_t n = E->n_spins;
   auto* h_bad = reinterpret_cast<unsigned long long*>(E->h_small);
   CUDA_TRY(cudaMemsetAsync(E->d_bad, 0xff, sizeof(unsigned long long), E->stream));
+  if (energies) {
+    double* h_en = reinterpret_cast<double*>(E->h_small + kSmallIn);
+    std::memcpy(h_en, energies, sizeof(double) * E->n_slots);
+    CUDA_TRY(cudaMemcpyAsync(E->d_energy_in, h_en, sizeof(double) * E->n_slots, cudaMemcpyHostToDevice, E->stream));
+  }
   if (n > 0) {
     CUDA_TRY(cudaMemcpyAsync(E->d_cfg64, cfgs, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, E->stream));
     k_payload_check<<<payload_blocks(E, n), 256, 0, E->stream>>>(E->d_cfg64, n, E->d_bad);
+    CUDA_TRY(cudaGetLastError());
+  }
+  for (size_t ti = 0; ti < E->tabs.size(); ++ti) {
+    const int64_t ns = E->tabs[ti]->n_sites;
+    k_payload_in<<<payload_blocks(E, ns * E->R[ti]), 256, 0, E->stream>>>(
+        E->d_cfg64 + 3 * E->spin_off[ti], ns, E->R[ti], E->d_spins + E->spin_off[ti], E->d_bad,
+        ti == 0 && energies ? E->d_energy_in : nullptr, E->d_energy, E->n_slots);
     CUDA_TRY(cudaGetLastError());
   }
   CUDA_TRY(cudaMemcpyAsync(h_bad, E->d_bad, sizeof(unsigned long long), cudaMemcpyDeviceToHost, E->stream));
@@ -2480,18 +2506,6 @@ int32_t payload_upload(scemc_ensemble* E, const double* cfgs, const double* ener
     return fail(SCEMC_ERR_NUMERIC, "spin column " + std::to_string(local % ns + 1) + " of replica " +
                                        std::to_string(local / ns + 1) + " is not finite");
   }
-  for (size_t ti = 0; ti < E->tabs.size(); ++ti) {
-    const int64_t ns = E->tabs[ti]->n_sites;
-    k_payload_in<<<payload_blocks(E, ns * E->R[ti]), 256, 0, E->stream>>>(E->d_cfg64 + 3 * E->spin_off[ti], ns,
-                                                                          E->R[ti], E->d_spins + E->spin_off[ti]);
-    CUDA_TRY(cudaGetLastError());
-  }
-  if (energies) {
-    double* h_en = reinterpret_cast<double*>(E->h_small + kSmallIn);
-    std::memcpy(h_en, energies, sizeof(double) * E->n_slots);
-    CUDA_TRY(cudaMemcpyAsync(E->d_energy, h_en, sizeof(double) * E->n_slots, cudaMemcpyHostToDevice, E->stream));
-  }
-  CUDA_TRY(cudaStreamSynchronize(E->stream));
   return SCEMC_OK;
 }
 
@@ -2522,23 +2536,18 @@ int32_t payload_download(const scemc_ensemble* E, const DownloadDst& d) {
   }
   struct Part {
     void* dst;
-    const void* src;
-    size_t bytes;
-  } parts[] = {{d.energies, E->d_energy, (size_t)8 * n},      {d.slot_of_rung, E->d_slot_of_rung, (size_t)4 * n},
-               {d.counters, E->d_cnt, (size_t)32 * n},        {d.swaps, E->d_swaps, (size_t)16 * n},
-               {d.steps, E->d_step, (size_t)8 * n},           {d.max_drift, E->d_max_drift, (size_t)8 * n}};
+    size_t off, bytes;
+  } parts[] = {{d.energies, kRbEnergy * n, (size_t)8 * n}, {d.slot_of_rung, kRbSlotOfRung * n, (size_t)4 * n},
+               {d.counters, kRbCounters * n, (size_t)32 * n}, {d.swaps, kRbSwaps * n, (size_t)16 * n},
+               {d.steps, kRbSteps * n, (size_t)8 * n}, {d.max_drift, kRbMaxDrift * n, (size_t)8 * n}};
+  bool any = false;
+  for (const Part& pt : parts) any = any || pt.dst != nullptr;
   unsigned char* h = E->h_small + small_out_offset(n);
-  size_t off = 0;
-  for (const Part& pt : parts) {
-    if (pt.dst) CUDA_TRY(cudaMemcpyAsync(h + off, pt.src, pt.bytes, cudaMemcpyDeviceToHost, E->stream));
-    off += (pt.bytes + 15) & ~(size_t)15;
-  }
+  if (any)
+    CUDA_TRY(cudaMemcpyAsync(h, E->d_readback, kReadbackBytesPerSlot * (size_t)n, cudaMemcpyDeviceToHost, E->stream));
   CUDA_TRY(cudaStreamSynchronize(E->stream));
-  off = 0;
-  for (const Part& pt : parts) {
-    if (pt.dst) std::memcpy(pt.dst, h + off, pt.bytes);
-    off += (pt.bytes + 15) & ~(size_t)15;
-  }
+  for (const Part& pt : parts)
+    if (pt.dst) std::memcpy(pt.dst, h + pt.off, pt.bytes);
   return SCEMC_OK;
 }
 
@@ -2616,12 +2625,22 @@ int32_t create_ensemble(int32_t n_tables, const scemc_tables* const* tables, con
     E->dmax = std::max(E->dmax, tables[i]->dl.dmax);
     E->rmax = std::max(E->rmax, tables[i]->dl.rmax);
   }
-  if ((rc = dalloc(&E->d_energy, slots)) || (rc = dalloc(&E->d_dEfix, slots)) || (rc = dalloc(&E->d_cnt, 4 * slots)) ||
-      (rc = dalloc(&E->d_win, 2 * slots)) || (rc = dalloc(&E->d_swaps, 2 * slots)) ||
-      (rc = dalloc(&E->d_beta, slots)) || (rc = dalloc(&E->d_step, slots)) || (rc = dalloc(&E->d_seed, slots)) ||
-      (rc = dalloc(&E->d_slot_of_rung, slots)) || (rc = dalloc(&E->d_rung_of_slot, slots)) ||
-      (rc = dalloc(&E->d_max_drift, slots)) || (rc = dalloc(&E->d_drift, slots)) ||
-      (rc = dalloc(&E->d_eout, slots)) || (rc = dalloc(&E->d_gs, 1)) || (rc = dalloc(&E->d_st, 1)))
+  // the per-slot arrays a download returns share one allocation, read back in one copy
+  if ((rc = dalloc(&E->d_readback, kReadbackBytesPerSlot * (size_t)slots))) return rc;
+  {
+    unsigned char* rb = E->d_readback;
+    const size_t n = (size_t)slots;
+    E->d_energy = reinterpret_cast<double*>(rb + kRbEnergy * n);
+    E->d_slot_of_rung = reinterpret_cast<int32_t*>(rb + kRbSlotOfRung * n);
+    E->d_cnt = reinterpret_cast<unsigned long long*>(rb + kRbCounters * n);
+    E->d_swaps = reinterpret_cast<unsigned long long*>(rb + kRbSwaps * n);
+    E->d_step = reinterpret_cast<double*>(rb + kRbSteps * n);
+    E->d_max_drift = reinterpret_cast<double*>(rb + kRbMaxDrift * n);
+  }
+  if ((rc = dalloc(&E->d_dEfix, slots)) || (rc = dalloc(&E->d_win, 2 * slots)) || (rc = dalloc(&E->d_beta, slots)) ||
+      (rc = dalloc(&E->d_seed, slots)) || (rc = dalloc(&E->d_rung_of_slot, slots)) ||
+      (rc = dalloc(&E->d_drift, slots)) || (rc = dalloc(&E->d_energy_in, slots)) || (rc = dalloc(&E->d_eout, slots)) ||
+      (rc = dalloc(&E->d_gs, 1)) || (rc = dalloc(&E->d_st, 1)))
     return rc;
   std::vector<int32_t> ident(slots);
   for (int i = 0; i < slots; ++i) ident[i] = i;
