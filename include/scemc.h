@@ -234,19 +234,21 @@ int32_t scemc_batch_kernel_time(const scemc_batch* b, double* ms, int64_t* passe
  * 43 -> 128 -> 128 -> 20 (SiLU; BF16 weights on the tcgen05 tensor cores, FP32
  * accumulate) whose 20 outputs parameterise a 4-component von Mises-Fisher mixture
  * on S^2 (per component: logit, raw mean (3), raw concentration c; kappa =
- * softplus(c) / kT[meV] + 1e-3). Inputs per row: the 14 environment spins (x, y, z)
- * in the environment table's order, then kT in meV (43 floats).
+ * softplus(c) / kT[meV] + 1e-3). Inputs per row (n_in = 3 k + 1 floats): the k
+ * environment spins (x, y, z) in the environment table's order, then kT in meV;
+ * k = 14 (bcc nearest and next-nearest shells, n_in = 43), 18 (fcc, n_in = 55), at
+ * most 21 (n_in <= 64).
  * Parameters travel as one FP32 block of SCEMC_MLP_PARAMS floats: W1 [128][64]
- * (input columns 43..63 zero), b1 [128], W2 [128][128], b2 [128], W3 [32][128]
+ * (input columns n_in..63 zero), b1 [128], W2 [128][128], b2 [128], W3 [32][128]
  * (output rows 20..31 zero), b3 [32].
  * ------------------------------------------------------------------------- */
 #define SCEMC_MLP_PARAMS 28960
 typedef struct scemc_mlp scemc_mlp;
-int32_t scemc_mlp_create(uint64_t seed, scemc_mlp** out);
+int32_t scemc_mlp_create(uint64_t seed, int32_t n_in, scemc_mlp** out);
 int32_t scemc_mlp_destroy(scemc_mlp* m);
 int32_t scemc_mlp_get_params(const scemc_mlp* m, float* params);
 int32_t scemc_mlp_set_params(scemc_mlp* m, const float* params);
-/* out: n x 20 network outputs for the n x 43 inputs x. */
+/* out: n x 20 network outputs for the n x n_in inputs x. */
 int32_t scemc_mlp_forward(scemc_mlp* m, const float* x, int64_t n, float* out);
 /* Mean negative log-likelihood of the unit targets y (n x 3) under the mixture and
  * its gradient (SCEMC_MLP_PARAMS floats); n a multiple of 128; no update. */
@@ -267,7 +269,8 @@ int32_t scemc_energy_gradient(const scemc_tables* t, const double* config, int32
 
 /* Registers a learned proposal network with a batch (m = NULL unregisters). env:
  * for every table of the batch in order, n_sites x k 0-based site ids, the sites
- * whose spins (in that order) form a site's network input; k must be 14 and no
+ * whose spins (in that order) form a site's network input; 1 <= k <= 21 with the
+ * network's n_in = 3 k + 1, and no
  * environment site may share its site's colour. The network is not copied: it must
  * outlive the batch's learned runs. Runs with proposals = 3 then draw every
  * Metropolis proposal from the network's vMF mixture and accept it with

@@ -40,13 +40,13 @@ def sigmoid(x):
     return 1.0 / (1.0 + np.exp(-x))
 
 
-def init_params(seed: int):
+def init_params(seed: int, n_in: int = N_IN):
     """He-style initial weights (FP32 master copies, padded shapes): W1 (128, 64)
-    with input columns 43..63 zero, W2 (128, 128), W3 (32, 128) with output rows
+    with input columns n_in..63 zero, W2 (128, 128), W3 (32, 128) with output rows
     20..31 zero, biases zero. The concentration outputs start near softplus(1)."""
     rng = np.random.default_rng(seed)
     W1 = np.zeros((N_HID, N_IN_PAD))
-    W1[:, :N_IN] = rng.standard_normal((N_HID, N_IN)) * math.sqrt(2.0 / N_IN)
+    W1[:, :n_in] = rng.standard_normal((N_HID, n_in)) * math.sqrt(2.0 / n_in)
     W2 = rng.standard_normal((N_HID, N_HID)) * math.sqrt(2.0 / N_HID)
     W3 = np.zeros((N_OUT_PAD, N_HID))
     W3[:N_OUT] = rng.standard_normal((N_OUT, N_HID)) * math.sqrt(1.0 / N_HID) * 0.1
@@ -106,12 +106,13 @@ def log_q(o, tau, x):
     return lm[:, 0] + np.log(np.exp(l - lm).sum(axis=1))
 
 
-def nll_and_grad(P, X, Y, bf16: bool = False):
+def nll_and_grad(P, X, Y, bf16: bool = False, n_in: int = N_IN):
     """Mean negative log-likelihood of the unit targets Y (n, 3) and its gradient
-    for every parameter (same shapes as P); bf16 as in forward()."""
+    for every parameter (same shapes as P); bf16 as in forward(). Column n_in - 1
+    of X is kT."""
     f = forward(P, X, bf16)
     n = X.shape[0]
-    tau = np.asarray(X, np.float64)[:, N_IN - 1]  # the head reads kT unrounded
+    tau = np.asarray(X, np.float64)[:, n_in - 1]  # the head reads kT unrounded
     o = f["o"]
     logpi, mu, mn, kappa, c = head(o, tau)
     Y = np.asarray(Y, np.float64)
@@ -142,7 +143,7 @@ def nll_and_grad(P, X, Y, bf16: bool = False):
     dW1 = dz1.T @ f["X"]
     db1 = dz1.sum(axis=0)
     grads = dict(W1=dW1, b1=db1, W2=dW2, b2=db2, W3=dW3, b3=db3)
-    grads["W1"][:, N_IN:] = 0.0
+    grads["W1"][:, n_in:] = 0.0
     grads["W3"][N_OUT:] = 0.0
     grads["b3"][N_OUT:] = 0.0
     return float(-lq.mean()), grads

@@ -193,18 +193,18 @@ __global__ void k_to_bf16(const float* P, bf16* W1, bf16* W2, bf16* W2T, bf16* W
   }
 }
 
-// rows of X (n x 43 FP32, host layout) -> BF16 X [M][64] and X^T [64][M], tau, Y
+// rows of X (n x n_in FP32, host layout; kT last) -> BF16 X [M][64] and X^T [64][M], tau, Y
 __global__ void k_rows_in(const float* Xs, const float* Ys, const int32_t* idx, int64_t n_rows, int64_t M, bf16* X,
-                          bf16* XT, float* tau, float* Y) {
+                          bf16* XT, float* tau, float* Y, int n_in) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M * kInPad;
        i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t b = i / kInPad;
     const int c = (int)(i % kInPad);
     float v = 0.0f;
-    if (b < n_rows && c < kIn) {
+    if (b < n_rows && c < n_in) {
       const int64_t src = idx ? idx[b] : b;
-      v = Xs[src * kIn + c];
-      if (c == kIn - 1) tau[b] = v;
+      v = Xs[src * n_in + c];
+      if (c == n_in - 1) tau[b] = v;
       if (c < 3 && Ys) Y[b * 3 + c] = Ys[src * 3 + c];
     }
     const bf16 h = __float2bfloat16_rn(v);
@@ -237,11 +237,11 @@ __global__ void k_head_train(const float* O, const float* tau, const float* Y, i
 // one Adam step on the FP32 masters
 __global__ void k_grad_adam(float* P, float* mom, float* var, float* grad, const float* dW1, const float* dW2,
                             const float* dW3T, const bf16* dZ1T, const bf16* dZ2T, const bf16* dOT, int64_t M,
-                            float lr, float c1, float c2) {
+                            float lr, float c1, float c2, int n_in) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < kParams; i += (int64_t)gridDim.x * blockDim.x) {
     float gv = 0.0f;
     if (i < oB1) {
-      gv = ((i % kInPad) < kIn) ? dW1[i] : 0.0f;
+      gv = ((i % kInPad) < n_in) ? dW1[i] : 0.0f;
     } else if (i < oW2) {
       const bf16* r = dZ1T + (i - oB1) * M;
       for (int64_t b = 0; b < M; ++b) gv += __bfloat162float(r[b]);
@@ -363,7 +363,7 @@ int32_t step_rows(scemc_mlp* m, int64_t n, int64_t M, float lr) {
   }
   k_grad_adam<<<(unsigned)((kParams + 255) / 256), 256, 0, st>>>(m->d_master, m->d_m, m->d_v, m->d_grad, m->d_dW1,
                                                                  m->d_dW2, m->d_dW3T, m->d_dZ1T, m->d_dZ2T,
-                                                                 m->d_dOT, M, lr, c1, c2);
+                                                                 m->d_dOT, M, lr, c1, c2, m->n_in);
   LTRY(cudaGetLastError());
   if (lr > 0.0f)
     if ((rc = refresh_bf16(m))) return rc;
@@ -401,13 +401,15 @@ int32_t mlp_forward_dev(const scemc_mlp* m, const bf16* X, int64_t M, bf16* H1, 
 
 extern "C" {
 
-int32_t scemc_mlp_create(uint64_t seed, scemc_mlp** out) {
+int32_t scemc_mlp_create(uint64_t seed, int32_t n_in, scemc_mlp** out) {
   if (!out) return fail(SCEMC_ERR_ARG, "NULL argument");
   *out = nullptr;
+  if (n_in < 2 || n_in > kInPad) return fail(SCEMC_ERR_ARG, "n_in must be 2..64 (inputs, kT last)");
   int dev = 0;
   LTRY(cudaGetDevice(&dev));
   auto* m = new scemc_mlp();
   m->device = dev;
+  m->n_in = n_in;
   int32_t rc = SCEMC_OK;
   auto bail = [&](int32_t r) {
     scemc_mlp_destroy(m);
@@ -427,7 +429,7 @@ int32_t scemc_mlp_create(uint64_t seed, scemc_mlp** out) {
   std::mt19937_64 g(seed);
   std::normal_distribution<double> nd(0.0, 1.0);
   for (int r = 0; r < kHid; ++r)
-    for (int c = 0; c < kIn; ++c) P[oW1 + r * kInPad + c] = (float)(nd(g) * std::sqrt(2.0 / kIn));
+    for (int c = 0; c < n_in; ++c) P[oW1 + r * kInPad + c] = (float)(nd(g) * std::sqrt(2.0 / n_in));
   for (int i = 0; i < kHid * kHid; ++i) P[oW2 + i] = (float)(nd(g) * std::sqrt(2.0 / kHid));
   for (int o = 0; o < kOut; ++o)
     for (int h = 0; h < kHid; ++h) P[oW3 + o * kHid + h] = (float)(nd(g) * std::sqrt(1.0 / kHid) * 0.1);
@@ -477,9 +479,9 @@ int32_t scemc_mlp_forward(scemc_mlp* m, const float* x, int64_t n, float* out) {
   int32_t rc;
   if ((rc = ensure_work(m, M))) return rc;
   float* dx = nullptr;
-  LTRY(cudaMallocAsync(reinterpret_cast<void**>(&dx), (size_t)n * kIn * sizeof(float), m->stream));
-  LTRY(cudaMemcpyAsync(dx, x, (size_t)n * kIn * sizeof(float), cudaMemcpyHostToDevice, m->stream));
-  k_rows_in<<<256, 256, 0, m->stream>>>(dx, nullptr, nullptr, n, M, m->d_X, nullptr, m->d_tau, nullptr);
+  LTRY(cudaMallocAsync(reinterpret_cast<void**>(&dx), (size_t)n * m->n_in * sizeof(float), m->stream));
+  LTRY(cudaMemcpyAsync(dx, x, (size_t)n * m->n_in * sizeof(float), cudaMemcpyHostToDevice, m->stream));
+  k_rows_in<<<256, 256, 0, m->stream>>>(dx, nullptr, nullptr, n, M, m->d_X, nullptr, m->d_tau, nullptr, m->n_in);
   LTRY(cudaGetLastError());
   rc = scemc_detail::mlp_forward_dev(m, m->d_X, M, m->d_H1, m->d_H2, m->d_O, m->stream, m->d_err);
   LTRY(cudaFreeAsync(dx, m->stream));
@@ -495,11 +497,11 @@ int32_t scemc_mlp_loss_grad(scemc_mlp* m, const float* x, const float* y, int64_
   int32_t rc;
   if ((rc = ensure_work(m, n))) return rc;
   float *dx = nullptr, *dy = nullptr;
-  LTRY(cudaMallocAsync(reinterpret_cast<void**>(&dx), (size_t)n * kIn * sizeof(float), m->stream));
+  LTRY(cudaMallocAsync(reinterpret_cast<void**>(&dx), (size_t)n * m->n_in * sizeof(float), m->stream));
   LTRY(cudaMallocAsync(reinterpret_cast<void**>(&dy), (size_t)n * 3 * sizeof(float), m->stream));
-  LTRY(cudaMemcpyAsync(dx, x, (size_t)n * kIn * sizeof(float), cudaMemcpyHostToDevice, m->stream));
+  LTRY(cudaMemcpyAsync(dx, x, (size_t)n * m->n_in * sizeof(float), cudaMemcpyHostToDevice, m->stream));
   LTRY(cudaMemcpyAsync(dy, y, (size_t)n * 3 * sizeof(float), cudaMemcpyHostToDevice, m->stream));
-  k_rows_in<<<256, 256, 0, m->stream>>>(dx, dy, nullptr, n, n, m->d_X, m->d_XT, m->d_tau, m->d_Y);
+  k_rows_in<<<256, 256, 0, m->stream>>>(dx, dy, nullptr, n, n, m->d_X, m->d_XT, m->d_tau, m->d_Y, m->n_in);
   LTRY(cudaGetLastError());
   rc = step_rows(m, n, n, 0.0f);
   LTRY(cudaFreeAsync(dx, m->stream));
@@ -521,7 +523,7 @@ int32_t scemc_mlp_train(scemc_mlp* m, const float* x, const float* y, int64_t n,
   if ((rc = ensure_work(m, batch))) return rc;
   float *dx = nullptr, *dy = nullptr;
   int32_t* didx = nullptr;
-  LTRY(cudaMalloc(reinterpret_cast<void**>(&dx), (size_t)n * kIn * sizeof(float)));
+  LTRY(cudaMalloc(reinterpret_cast<void**>(&dx), (size_t)n * m->n_in * sizeof(float)));
   LTRY(cudaMalloc(reinterpret_cast<void**>(&dy), (size_t)n * 3 * sizeof(float)));
   LTRY(cudaMalloc(reinterpret_cast<void**>(&didx), (size_t)n * sizeof(int32_t)));
   auto cleanup = [&]() {
@@ -530,7 +532,7 @@ int32_t scemc_mlp_train(scemc_mlp* m, const float* x, const float* y, int64_t n,
     cudaFree(dy);
     cudaFree(didx);
   };
-  if (cudaMemcpy(dx, x, (size_t)n * kIn * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+  if (cudaMemcpy(dx, x, (size_t)n * m->n_in * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(dy, y, (size_t)n * 3 * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
     cleanup();
     return fail(SCEMC_ERR_CUDA, "dataset upload");
@@ -550,7 +552,7 @@ int32_t scemc_mlp_train(scemc_mlp* m, const float* x, const float* y, int64_t n,
     double acc = 0.0;
     for (int64_t s = 0; s < steps; ++s) {
       k_rows_in<<<256, 256, 0, m->stream>>>(dx, dy, didx + s * batch, batch, batch, m->d_X, m->d_XT, m->d_tau,
-                                            m->d_Y);
+                                            m->d_Y, m->n_in);
       if ((rc = step_rows(m, batch, batch, (float)lr))) {
         cleanup();
         return rc;

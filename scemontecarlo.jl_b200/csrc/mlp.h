@@ -7,7 +7,8 @@
 #include <stdint.h>
 
 // Parameter block (FP32 masters, padded shapes), offsets in floats:
-// W1 [128][64] (input columns 43..63 zero), b1 [128], W2 [128][128], b2 [128],
+// W1 [128][64] (input columns n_in..63 zero; n_in = 43 for 14 environment spins),
+// b1 [128], W2 [128][128], b2 [128],
 // W3 [32][128] (output rows 20..31 zero), b3 [32].
 namespace mlpl {
 constexpr int kIn = 43, kInPad = 64, kHid = 128, kOut = 20, kOutPad = 32;
@@ -17,6 +18,7 @@ constexpr int64_t oW1 = 0, oB1 = oW1 + kHid * kInPad, oW2 = oB1 + kHid, oB2 = oW
 
 struct scemc_mlp {
   int device = 0;
+  int32_t n_in = mlpl::kIn;  // inputs per row (kT last), at most kInPad
   cudaStream_t stream = nullptr;
   float* d_master = nullptr;  // kParams FP32
   float* d_m = nullptr;       // Adam moments

@@ -1415,12 +1415,18 @@ __global__ void __launch_bounds__(256, 2) k_learned_fused(SweepArgs a, LearnedNe
   // A thread's share of one tile's environment (warpgroup 0: spins 0..7 -> input
   // columns 0..23; warpgroup 1: spins 8..13 and kT -> columns 24..42), gathered for
   // the next tile while this tile draws.
+  // A row's item and, written straight into the BF16 input tile sX (free once the
+  // previous tile's layer 1 has read it), the row's input columns: warpgroup 0
+  // columns 0..23 (environment spins 0..7), warpgroup 1 columns 24..63 (spins 8..
+  // k-1, kT in meV at column 3k, zeros after it). k = L.env_k <= 21.
   struct Gather {
     int li, q, r, s;
     bool valid;
     float4 e;
     float tau;
-    alignas(16) __nv_bfloat16 x[24];
+  };
+  auto put = [&](int c, float v) {
+    *reinterpret_cast<__nv_bfloat16*>(sX + umma::kmajor_offset(row, c, 64)) = __float2bfloat16_rn(v);
   };
   auto gather = [&](int tile, Gather& g) {
     const int item = tile * kTile + row;
@@ -1428,24 +1434,33 @@ __global__ void __launch_bounds__(256, 2) k_learned_fused(SweepArgs a, LearnedNe
     g.li = g.q = g.r = g.s = 0;
     g.e = make_float4(0.f, 0.f, 1.f, 0.f);
     g.tau = 1.0f;
-#pragma unroll
-    for (int k = 0; k < 24; ++k) g.x[k] = __float2bfloat16_rn(0.0f);
+    const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+    for (int ch = wg ? 3 : 0; ch < (wg ? 8 : 3); ++ch)
+      *reinterpret_cast<uint4*>(sX + umma::kmajor_offset(row, ch * 8, 64)) = z;
     if (!g.valid) return;
     item_of(a, seg_c, item, g.li, g.q, g.r);
     const DevLattice& L = a.lat[g.li];
     g.s = L.color_sites[L.color_ptr[col] + g.q];
     const float4* sp = a.spins + L.spin_off;
-    const int32_t* env = L.env + (int64_t)g.s * L.env_k;
+    const int K = L.env_k;
+    const int32_t* env = L.env + (int64_t)g.s * K;
     g.tau = slot_kt_mev(a, L.slot0 + g.r);
-    const int k0 = wg ? 8 : 0, k1 = wg ? 14 : 8;
-    for (int k = k0; k < k1; ++k) {
-      const float4 v = __ldg(sp + (int64_t)__ldg(env + k) * L.R + g.r);
-      g.x[3 * (k - k0)] = __float2bfloat16_rn(v.x);
-      g.x[3 * (k - k0) + 1] = __float2bfloat16_rn(v.y);
-      g.x[3 * (k - k0) + 2] = __float2bfloat16_rn(v.z);
+    const int j0 = wg ? 8 : 0, j1 = wg ? K : (K < 8 ? K : 8);
+    for (int jb = j0; jb < j1; jb += 4) {  // four spins' loads in flight at a time
+      float4 v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        v[u] = jb + u < j1 ? __ldg(sp + (int64_t)__ldg(env + jb + u) * L.R + g.r) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (jb + u < j1) {
+          put(3 * (jb + u), v[u].x);
+          put(3 * (jb + u) + 1, v[u].y);
+          put(3 * (jb + u) + 2, v[u].z);
+        }
     }
-    if (wg) g.x[18] = __float2bfloat16_rn(g.tau);
-    else g.e = sp[(int64_t)g.s * L.R + g.r];
+    if ((3 * K < 24) == (wg == 0)) put(3 * K, g.tau);
+    if (!wg) g.e = sp[(int64_t)g.s * L.R + g.r];
   };
   // MH, warpgroup 1: the coefficients of a gathered row's item
   auto coeffs = [&](const Gather& g, float (&cc)[NR]) {
@@ -1470,15 +1485,6 @@ __global__ void __launch_bounds__(256, 2) k_learned_fused(SweepArgs a, LearnedNe
     const int li = cur.li, r = cur.r, s = cur.s;
     const float4 e = cur.e;
     const float tau = cur.tau;
-#pragma unroll
-    for (int kg = 0; kg < 3; ++kg)
-      *reinterpret_cast<uint4*>(sX + umma::kmajor_offset(row, (3 * wg + kg) * 8, 64)) =
-          reinterpret_cast<const uint4*>(cur.x)[kg];
-    if (wg) {
-      const uint4 z = make_uint4(0u, 0u, 0u, 0u);
-      *reinterpret_cast<uint4*>(sX + umma::kmajor_offset(row, 48, 64)) = z;
-      *reinterpret_cast<uint4*>(sX + umma::kmajor_offset(row, 56, 64)) = z;
-    }
     umma::fence_async_smem();
     umma::fence_before();
     __syncthreads();
@@ -3933,7 +3939,8 @@ int32_t scemc_batch_set_learned(scemc_batch* b, const scemc_mlp* m, const int32_
   b->graphs.clear();
   if (m) {
     if (!env) return fail(SCEMC_ERR_ARG, "env is NULL");
-    if (k != 14) return fail(SCEMC_ERR_ARG, "the network reads 14 environment spins (k = 14)");
+    if (k < 1 || k > 21 || m->n_in != 3 * k + 1)
+      return fail(SCEMC_ERR_ARG, "the network reads n_in = 3 k + 1 inputs (k environment spins and kT, k <= 21)");
     int64_t off = 0;
     for (size_t i = 0; i < b->tabs.size(); ++i) {
       const scemc_tables* T = b->tabs[i];

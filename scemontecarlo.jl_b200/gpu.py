@@ -339,15 +339,18 @@ class GPUBatch:
 
     def set_learned(self, net, env) -> None:
         """Registers a learned proposal network (scemc.learned.ProposalNet, or None to
-        unregister) with its environment table (n_sites x 14 per table, 0-based);
-        runs with proposals=3 then use it for every Metropolis proposal."""
+        unregister) with its environment table (n_sites x net.n_env per table,
+        0-based); runs with proposals=3 then use it for every Metropolis proposal."""
         if net is None:
             check(_lib.lib().scemc_batch_set_learned(self.h, None, None, 14))
             self._net = None
             return
-        env = np.ascontiguousarray(np.concatenate([np.asarray(e, np.int32).reshape(-1) for e in
-                                                   (env if isinstance(env, (list, tuple)) else [env])]), np.int32)
-        check(_lib.lib().scemc_batch_set_learned(self.h, net.h, ptr(env, C.c_int32), 14))
+        tabs = env if isinstance(env, (list, tuple)) else [env]
+        k = int(net.n_env)
+        if any(np.asarray(e).reshape(-1).size != g.n_sites * k for e, g in zip(tabs, self.gHs)):
+            raise ValueError(f"every environment table must be n_sites x {k}")
+        env = np.ascontiguousarray(np.concatenate([np.asarray(e, np.int32).reshape(-1) for e in tabs]), np.int32)
+        check(_lib.lib().scemc_batch_set_learned(self.h, net.h, ptr(env, C.c_int32), k))
         self._net = net  # the batch does not own the network: keep it alive
 
     def fetch_record_ratio(self) -> np.ndarray:

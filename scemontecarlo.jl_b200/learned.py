@@ -3,7 +3,8 @@ table (no counterpart in the reference; the acceptance it feeds is the
 reference's Metropolis test of src/updates.jl:37-64 with the Hastings factor
 q(e | env) / q(e' | env), so the stationary distribution is unchanged).
 
-The network (43 -> 128 -> 128 -> 20, SiLU) and its training run in
+The network (3 n_env + 1 -> 128 -> 128 -> 20, SiLU; 43 inputs for the 14-site
+bcc environment, 55 for the 18-site fcc one) and its training run in
 libscemc_cuda.so on the tcgen05 tensor cores; this module is the host side.
 """
 from __future__ import annotations
@@ -37,12 +38,23 @@ def pack(P: dict) -> np.ndarray:
 
 
 class ProposalNet:
-    """The learned proposal network (device resident)."""
+    """The learned proposal network (device resident) for environments of n_env spins:
+    n_in = 3 n_env + 1 inputs (the spins, then kT in meV)."""
 
-    def __init__(self, seed: int = 0):
+    def __init__(self, seed: int = 0, n_env: int = 14):
+        if not 1 <= n_env <= 21:
+            raise ValueError("n_env must be 1..21")
+        self.n_env = int(n_env)
+        self.n_in = 3 * self.n_env + 1
         h = C.c_void_p()
-        check(_lib.lib().scemc_mlp_create(int(seed) & (2 ** 64 - 1), C.byref(h)))
+        check(_lib.lib().scemc_mlp_create(int(seed) & (2 ** 64 - 1), self.n_in, C.byref(h)))
         self.h = h
+
+    def _rows(self, X) -> np.ndarray:
+        X = np.ascontiguousarray(X, np.float32)
+        if X.ndim != 2 or X.shape[1] != self.n_in:
+            raise ValueError(f"inputs must be (n, {self.n_in})")
+        return X
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -64,14 +76,14 @@ class ProposalNet:
         check(_lib.lib().scemc_mlp_set_params(self.h, ptr(flat, C.c_float)))
 
     def forward(self, X) -> np.ndarray:
-        X = np.ascontiguousarray(X, np.float32)
+        X = self._rows(X)
         n = X.shape[0]
         out = np.zeros((n, N_OUT), np.float32)
         check(_lib.lib().scemc_mlp_forward(self.h, ptr(X, C.c_float), n, ptr(out, C.c_float)))
         return out
 
     def loss_grad(self, X, Y):
-        X = np.ascontiguousarray(X, np.float32)
+        X = self._rows(X)
         Y = np.ascontiguousarray(Y, np.float32)
         loss = C.c_double()
         g = np.zeros(N_PARAMS, np.float32)
@@ -81,7 +93,7 @@ class ProposalNet:
 
     def train(self, X, Y, batch: int = 1024, epochs: int = 10, lr: float = 1e-3, seed: int = 0) -> np.ndarray:
         """Adam on shuffled minibatches; returns each epoch's mean minibatch loss."""
-        X = np.ascontiguousarray(X, np.float32)
+        X = self._rows(X)
         Y = np.ascontiguousarray(Y, np.float32)
         losses = np.zeros(max(epochs, 1))
         check(_lib.lib().scemc_mlp_train(self.h, ptr(X, C.c_float), ptr(Y, C.c_float), X.shape[0], int(batch),
@@ -134,8 +146,8 @@ def environment_table(positions: np.ndarray, dims, n_shells: int = 2, tol: float
 
 
 def environment_rows(configs, env: np.ndarray, kts_ev, sites=None) -> np.ndarray:
-    """Network inputs (n, 43) for the given sites of each configuration: the
-    environment spins in table order, then kT in meV."""
+    """Network inputs (n, 3 k + 1) for the given sites of each configuration: the
+    k environment spins in table order, then kT in meV."""
     rows = []
     for cfg, kt in zip(configs, kts_ev):
         cfg = np.asarray(cfg).reshape(-1, 3)
@@ -151,7 +163,7 @@ def collect_training_set(H, env, kts, n_rows: int, *, sweeps_therm: int = 2000, 
     device): after `sweeps_therm` adaptive-step sweeps from random spins (or from
     `init`, one configuration for every chain), `snapshots` configurations `spacing`
     sweeps apart; n_rows rows drawn evenly over kT values and snapshots.
-    Returns (X (n, 43) float32, Y (n, 3) float32): inputs and the site's own spin."""
+    Returns (X (n, 3 k + 1) float32, Y (n, 3) float32): inputs and the site's own spin."""
     from .gpu import GPUBatch, GPUTiledHamiltonian
     gH = H if isinstance(H, GPUTiledHamiltonian) else GPUTiledHamiltonian(H)
     host = gH.host

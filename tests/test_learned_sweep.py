@@ -26,22 +26,34 @@ def c4_small(n):
     return w, H, OH, env
 
 
+def fcc_small(n):
+    """The fcc l <= 2 + triangles + Zeeman model with the 18-site (12 + 6) environment."""
+    w = models.config5_fcc(n=n)
+    H = scemc.TiledHamiltonian(4, w.terms, dims=(n, n, n), magmoms=w.magmoms, field=w.field)
+    OH = O.OracleHamiltonian(4, w.terms, (n, n, n), magmoms=w.magmoms, field=w.field)
+    env = learned.environment_table(models.FCC.positions, (n, n, n))
+    return w, H, OH, env
+
+
 def env_rows(env, colors, pre, post, s_list, kt_mev):
     """Network inputs as the device saw them: an environment site of an earlier
     colour already carries this pass's decision."""
-    X = np.zeros((len(s_list), 43), np.float32)
+    k = env.shape[1]
+    X = np.zeros((len(s_list), 3 * k + 1), np.float32)
     for i, s in enumerate(s_list):
         v = [post[t] if colors[t] < colors[s] else pre[t] for t in env[s]]
-        X[i, :42] = np.asarray(v, np.float32).reshape(-1)
-        X[i, 42] = kt_mev
+        X[i, :3 * k] = np.asarray(v, np.float32).reshape(-1)
+        X[i, 3 * k] = kt_mev
     return X
 
 
-@pytest.mark.parametrize("kernel", [2, 3])
-def test_learned_pass_replay(gpu, kernel):
-    w, H, OH, env = c4_small(4)
+@pytest.mark.parametrize("lattice,kernel", [("bcc", 2), ("bcc", 3), ("fcc", 2), ("fcc", 3)])
+def test_learned_pass_replay(gpu, lattice, kernel):
+    """bcc body-4 with the 14-site environment (43 inputs) and fcc l <= 2 with the
+    18-site environment (55 inputs)."""
+    w, H, OH, env = c4_small(4) if lattice == "bcc" else fcc_small(3)
     gH = scemc.GPUTiledHamiltonian(H)
-    net = learned.ProposalNet(seed=3)
+    net = learned.ProposalNet(seed=3, n_env=env.shape[1])
     seeds = [0xABC, 0xDEF]
     kts = np.array([0.5, 1.5]) * MEV
     b = scemc.GPUBatch([gH], [2], [models.random_config(H.n_sites, 1), models.random_config(H.n_sites, 2)], seeds,
