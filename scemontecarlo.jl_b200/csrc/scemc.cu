@@ -186,8 +186,6 @@ struct SweepArgs {
   double* rec_lqr;
   uint32_t* flags;    // data-flow form: per item slot, the pass epoch its update completed (null otherwise)
   int32_t dmax, rmax;
-  int32_t rep_pf;     // replica-parallel form: prefetch every neighbour row into L1 first (few threads per colour)
-  int32_t pad_pf;
 };
 
 __device__ __forceinline__ unsigned long long globaltimer() {
@@ -1004,13 +1002,14 @@ __global__ void __launch_bounds__(256) k_proposals(SweepArgs a) { make_proposals
 
 // The leave-one-out coefficients c[k][t] = sum_j W_j[t, :] . z_j of P replicas
 // (r = g + k G, those with ok[k]) of the site of descriptor `dsc`, from every record's
-// W block and its neighbours' Z rows. pf: the neighbour rows are prefetched into L1
-// first and read through it (else through L2).
+// W block and its neighbours' Z rows. PF: the neighbour rows are prefetched into L1
+// first and read through it (else through L2); a template parameter, so the
+// many-wave form carries no per-load branch.
 // NP > 1: only the records j with j % NP == part (the one-body record with part 0),
 // for NP threads that share one site's walk.
-template <int LMAX, int P, int NP = 1>
+template <int LMAX, int P, int NP, bool PF>
 __device__ __forceinline__ void rep_coeffs(const DevLattice& L, const float4* __restrict__ sp, int4 dsc, int R, int G,
-                                           int g, const bool (&ok)[P], bool pf,
+                                           int g, const bool (&ok)[P],
                                            float (&c)[P][(LMAX + 1) * (LMAX + 1) - 1], int part = 0) {
   constexpr int NR = (LMAX + 1) * (LMAX + 1) - 1;
   const int n0 = dsc.y, j0 = dsc.z;
@@ -1024,9 +1023,9 @@ __device__ __forceinline__ void rep_coeffs(const DevLattice& L, const float4* __
   auto gather = [&](int loc, float4* v) {
     const float4* b = sp + (int64_t)__ldg(nbl + loc) * R + g;
 #pragma unroll
-    for (int k = 0; k < P; ++k) v[k] = pf ? __ldg(b + (ok[k] ? k * G : 0)) : __ldcg(b + (ok[k] ? k * G : 0));
+    for (int k = 0; k < P; ++k) v[k] = PF ? __ldg(b + (ok[k] ? k * G : 0)) : __ldcg(b + (ok[k] ? k * G : 0));
   };
-  if (pf) {  // the site's records and every neighbour row requested at once; the walk then hits L1
+  if (PF) {  // the site's records and every neighbour row requested at once; the walk then hits L1
     const int nd = (int)(cnt >> 24);
     const int nrec = n_pair + n_trip + n_quad + n_one;
     for (int j = 0; j < nrec; j += 16) asm volatile("prefetch.global.L1 [%0];" ::"l"(fr + j));
@@ -1166,7 +1165,7 @@ __device__ __forceinline__ void rep_coeffs(const DevLattice& L, const float4* __
 // NP = 2: two adjacent threads share an item's record walk (alternate records) and
 // add their halves with one shuffle; the even thread decides. For colours too small
 // to fill the GPU, where each thread's walk is the critical path.
-template <int LMAX, int P, int NP>
+template <int LMAX, int P, int NP, bool PF>
 __device__ void rep_colour(const SweepArgs& a, int col, unsigned long long* s_dE, unsigned int* s_cnt,
                            const float* zsm) {
   constexpr int NR = (LMAX + 1) * (LMAX + 1) - 1;
@@ -1203,7 +1202,7 @@ __device__ void rep_colour(const SweepArgs& a, int col, unsigned long long* s_dE
 #pragma unroll
     for (int k = 0; k < P; ++k) ok[k] = g + k * G < R;
     float c[P][NR];
-    rep_coeffs<LMAX, P, NP>(L, sp, dsc, R, G, g, ok, a.rep_pf != 0, c, part);
+    rep_coeffs<LMAX, P, NP, PF>(L, sp, dsc, R, G, g, ok, c, part);
     if (NP == 2) {
       const unsigned pair = 3u << (threadIdx.x & 30u);
 #pragma unroll
@@ -1471,7 +1470,7 @@ __global__ void __launch_bounds__(256, 2) k_learned_fused(SweepArgs a, LearnedNe
     const int4 dsc = __ldg(L.idesc + __ldg(L.color_ptr + col) + g.q);
     const bool one[1] = {true};
     float c1[1][NR];
-    rep_coeffs<LMAX, 1, 2>(L, a.spins + L.spin_off, dsc, L.R, L.R, g.r, one, true, c1, wg);
+    rep_coeffs<LMAX, 1, 2, true>(L, a.spins + L.spin_off, dsc, L.R, L.R, g.r, one, c1, wg);
 #pragma unroll
     for (int t = 0; t < NR; ++t) cc[t] = c1[0][t];
   };
@@ -1607,14 +1606,14 @@ __global__ void __launch_bounds__(256, 2) k_learned_fused(SweepArgs a, LearnedNe
 
 // P = 2 at 80 registers (three 256-thread blocks per SM); P = 1 at 64 registers
 // (four blocks per SM).
-template <int LMAX, int P, int NP>
+template <int LMAX, int P, int NP, bool PF>
 __global__ void __launch_bounds__(256, P == 1 ? 4 : 3) k_rep_colour(SweepArgs a) {
   extern __shared__ __align__(16) float zsm[];
   __shared__ unsigned long long s_dE[kMaxSlots];
   __shared__ unsigned int s_cnt[3 * kMaxSlots];
   zero_block(a.n_slots, s_dE, s_cnt);
   stage_params(a, zsm);
-  rep_colour<LMAX, P, NP>(a, a.colour, s_dE, s_cnt, zsm);
+  rep_colour<LMAX, P, NP, PF>(a, a.colour, s_dE, s_cnt, zsm);
   flush_block(a, s_dE, s_cnt);
 }
 
@@ -2888,13 +2887,17 @@ RepForm rep_form(const scemc_ensemble* E, int c, int forced) {
   f.P = forced == 1 || forced == 2 ? forced : (NP == 2 ? 1 : 2);
   f.nt = rep_threads(E, c, f.P) * NP;
   f.pf = f.nt <= sms * (f.P == 1 ? 1024 : 768) * 2 ? 1 : 0;
-  if (E->lmax == 1) {
-    if (f.P == 1) f.fn = NP == 2 ? k_rep_colour<1, 1, 2> : k_rep_colour<1, 1, 1>;
-    else f.fn = NP == 2 ? k_rep_colour<1, 2, 2> : k_rep_colour<1, 2, 1>;
-  } else {
-    if (f.P == 1) f.fn = NP == 2 ? k_rep_colour<2, 1, 2> : k_rep_colour<2, 1, 1>;
-    else f.fn = NP == 2 ? k_rep_colour<2, 2, 2> : k_rep_colour<2, 2, 1>;
-  }
+  // [lmax - 1][P - 1][NP - 1][pf]
+  static const FastFn forms[2][2][2][2] = {
+      {{{k_rep_colour<1, 1, 1, false>, k_rep_colour<1, 1, 1, true>},
+        {k_rep_colour<1, 1, 2, false>, k_rep_colour<1, 1, 2, true>}},
+       {{k_rep_colour<1, 2, 1, false>, k_rep_colour<1, 2, 1, true>},
+        {k_rep_colour<1, 2, 2, false>, k_rep_colour<1, 2, 2, true>}}},
+      {{{k_rep_colour<2, 1, 1, false>, k_rep_colour<2, 1, 1, true>},
+        {k_rep_colour<2, 1, 2, false>, k_rep_colour<2, 1, 2, true>}},
+       {{k_rep_colour<2, 2, 1, false>, k_rep_colour<2, 2, 1, true>},
+        {k_rep_colour<2, 2, 2, false>, k_rep_colour<2, 2, 2, true>}}}};
+  f.fn = forms[E->lmax == 1 ? 0 : 1][f.P - 1][NP - 1][f.pf];
   return f;
 }
 
@@ -2975,7 +2978,6 @@ int32_t run_pass_impl(scemc_ensemble* E, int pass, const Launch& Lc) {
       const RepForm f = rep_form(E, c, Lc.rep_p);
       CUDA_TRY(cudaFuncSetAttribute((const void*)f.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       const int blocks = (int)std::min<int64_t>(cap, (f.nt + threads - 1) / threads);
-      a.rep_pf = f.pf;
       ++E->launches;
       f.fn<<<std::max(blocks, 1), threads, smem, E->stream>>>(a);
       CUDA_TRY(cudaGetLastError());
