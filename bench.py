@@ -196,12 +196,14 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_rank{index}.csv"
+        # raw samples beside the bench's other outputs (SCEMC_BENCH_OUT, default ./bench_out)
+        out = pathlib.Path(os.environ.get("SCEMC_BENCH_OUT", ROOT / "bench_out"))
+        self.path = out / f"clocks_rank{index}.csv"
 
     def start(self):
         if not shutil.which("nvidia-smi"):
             return
-        self.path.parent.mkdir(exist_ok=True)
+        self.path.parent.mkdir(parents=True, exist_ok=True)
         self.fh = open(self.path, "w")
         self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
                                       "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.fh,

@@ -1,7 +1,7 @@
 """Parity of the CUDA sweep against the FP64 oracle (run on a B200: -m gpu).
 
 Every gate calls libscemc_cuda.so through the C ABI (via the package's ctypes
-API). Tolerances (the north-star parity bar):
+API). Tolerances (the parity bar of this path):
   * per-proposal dE: |dE32 - dE64| <= 1e-5 * sum|c| (sum|znew| + sum|zold|)
     (the reference's scaled form, test_gpu.jl:168,174, with 1e-5 for FP32);
   * accept/reject: identical on replay, except near-threshold ties where the
