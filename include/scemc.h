@@ -15,18 +15,18 @@
  *   - Objects are not thread-safe; one host thread per chain/batch at a time.
  *
  * Reference interfaces replaced (paths relative to the SCEMonteCarlo.jl root):
- *   scemc_tables_create        GPUTiledHamiltonian(backend, H)   src/gpu/gpu_hamiltonian.jl:438-459
- *   scemc_chain_create         GPUChainState(gH, st; seed)       src/gpu/gpu_state.jl:335-347
+ *   scemc_tables_create        GPUTiledHamiltonian(backend, H)   src/gpu/gpu_hamiltonian.jl:66-88
+ *   scemc_chain_create         GPUChainState(gH, st; seed)       src/gpu/gpu_state.jl:49-61
  *   scemc_metropolis_sweep     gpu_metropolis_sweep!             src/gpu/gpu_sweep.jl:158-190
  *   scemc_run_sweeps           gpu_run_sweeps!                   src/gpu/gpu_sweep.jl:204-218
- *   scemc_download             to_host!                          src/gpu/gpu_state.jl:357-362
- *   scemc_upload               _from_host!                       src/gpu/gpu_state.jl:367-372
+ *   scemc_download             to_host!                          src/gpu/gpu_state.jl:71-76
+ *   scemc_upload               _from_host!                       src/gpu/gpu_state.jl:81-86
  *   scemc_swap_payload         _swap_payload! (device lanes)     src/gpu/gpu_pt.jl:46-51
  *   scemc_overrelaxation_sweep overrelaxation_sweep! (CPU-only in the reference)
  *                                                                src/updates.jl:231-248
  *   scemc_total_energy         _total_energy                     src/energy.jl:55-75
  *   scemc_renormalize          _renormalize!                     src/state.jl:168-185
- *   scemc_batch_*              gpu_run_pt lanes + exchanges      src/gpu/gpu_pt.jl:82-140
+ *   scemc_batch_*              _gpu_lane_segment! + exchanges    src/gpu/gpu_pt.jl:82-140
  *   scemc_color_sites          _color_sites (table-build helper) src/hamiltonian.jl:456-499
  */
 #ifndef SCEMC_H
@@ -42,7 +42,7 @@ extern "C" {
 enum {
   SCEMC_OK = 0,
   SCEMC_ERR_ARG = 1,          /* ArgumentError / DimensionMismatch equivalents */
-  SCEMC_ERR_UNSUPPORTED = 2,  /* e.g. lmax > 6 (gpu_hamiltonian.jl:439-440) */
+  SCEMC_ERR_UNSUPPORTED = 2,  /* e.g. lmax > 6 (gpu_hamiltonian.jl:67-68) */
   SCEMC_ERR_CUDA = 3,         /* a CUDA runtime call failed */
   SCEMC_ERR_TIMEOUT = 4,      /* a bounded device wait gave up (grid barrier) */
   SCEMC_ERR_EXHAUSTED = 5,    /* 32-bit sweep counter exhausted (gpu_sweep.jl:163-164) */
@@ -109,6 +109,11 @@ int32_t scemc_tables_destroy(scemc_tables* t);
 /* Table statistics used by the roofline: mean distinct neighbours per active site
  * (d), mean adjacency entries per active site (A), and table bytes on the device. */
 int32_t scemc_tables_stats(const scemc_tables* t, double* d_mean, double* a_mean, int64_t* bytes);
+/* Mean merged records per active site that the row- and replica-parallel kernels
+ * walk (one per distinct pair neighbour, l = 1 triplet and quad, plus the body-1
+ * vector; 0 when the tables have no fast form). Each record is 8 bytes and names
+ * its neighbours by local index into the site's distinct-neighbour list. */
+int32_t scemc_tables_records(const scemc_tables* t, double* records_mean);
 
 /* GPUChainState(gH, st; seed): uploads config (3 x n_sites FP64, column-major) and
  * the chain's incremental energy; step is the Metropolis rotation scale. */
@@ -194,6 +199,11 @@ typedef struct scemc_run_params {
                          network (scemc_batch_set_learned; kernels 2 or 3, per-colour modes 1 or 3) */
   int32_t rep_replicas; /* kernel 3: replicas per thread, 1 or 2; 0 = per colour launch, 1 when its
                            one-replica threads fill at most two waves of the GPU, else 2 */
+  int32_t rep_threads_per_item; /* kernel 3: threads sharing one item's record walk, 1 or 2; 0 = per colour
+                                   launch, 2 when twice its one-replica threads fit one wave, else 1 */
+  int32_t rep_prefetch; /* kernel 3: 1 = records and neighbour rows prefetched into L1 first, 2 = not;
+                           0 = per colour launch, prefetch when its threads fill at most two waves.
+                           Prefetching changes no arithmetic: 1 and 2 give bitwise equal chains */
 } scemc_run_params;
 
 /* Inverse temperatures per rung (n_slots values, table-major like the slots). */
@@ -276,8 +286,8 @@ int32_t scemc_energy_gradient(const scemc_tables* t, const double* config, int32
  * Metropolis proposal from the network's vMF mixture and accept it with
  * probability min(1, exp(-beta dE) q(e | env) / q(e' | env)). */
 int32_t scemc_batch_set_learned(scemc_batch* b, const scemc_mlp* m, const int32_t* env, int32_t k);
-/* log q(e | env) - log q(e' | env) of the recorded learned Metropolis pass (slot 0
- * of table 0; n_sites values, 0 where no learned proposal was recorded). */
+/* log q(e | env) - log q(e' | env) of the recorded learned Metropolis pass (the
+ * recorded replica; n_sites values, 0 where no learned proposal was recorded). */
 int32_t scemc_batch_fetch_record_ratio(const scemc_batch* b, double* lqr);
 
 /* Number of kernels the batch has enqueued on its stream since creation: sweep
@@ -306,17 +316,21 @@ int32_t scemc_batch_load_state(scemc_batch* b, const void* buf, int64_t bytes);
 /* Measurement records written by scemc_batch_run since the last fetch: n_records
  * rows of (n_slots x record_len) FP64, indexed by RUNG, each
  * {E, mx, my, mz, sub_x1, sub_y1, sub_z1, ...} with m over active sites and the
- * sublattice sums per cell as in src/observables.jl:336-360. Pass rec = NULL to
+ * sublattice sums per cell as in src/observables.jl:104-143. Pass rec = NULL to
  * query the count and record_len; a fetch with rec clears the buffer. */
 int32_t scemc_batch_fetch_measurements(scemc_batch* b, double* rec, int64_t capacity, int64_t* n_records,
                                        int32_t* record_len);
 
 /* Parity recording for the replay gate: with recording on, every pass of a sweep
- * (pass -1 = Metropolis, 0..2 = overrelaxation passes) stores per site of replica
- * slot 0 the proposal (3 FP32), the accept uniform, the FP32 dE and a flag
+ * (pass -1 = Metropolis, 0..2 = overrelaxation passes) stores per site of the
+ * recorded replica (replica 0 of table 0 unless scemc_batch_record_slot chose
+ * another) the proposal (3 FP32), the accept uniform, the FP32 dE and a flag
  * (1 accepted, 0 rejected, 2 not attempted, 3 not visited). Turning it on clears
- * the record. */
+ * the record. fetch_record returns n_sites(table) values per array. */
 int32_t scemc_batch_record(scemc_batch* b, int32_t on);
+/* Chooses the recorded replica: replica `replica` (0-based, < replicas[table]) of
+ * table `table` (0-based). */
+int32_t scemc_batch_record_slot(scemc_batch* b, int32_t table, int32_t replica);
 int32_t scemc_batch_fetch_record(const scemc_batch* b, int32_t pass, float* prop, double* u, float* dE,
                                  uint8_t* acc);
 
@@ -343,12 +357,15 @@ int32_t scemc_selftest_barrier_timeout(int64_t limit_ns);
  *   energies: caller-owned device array of replicas doubles (output);
  *   stream:   cudaStream_t to enqueue on (NULL = the legacy default stream).
  * Same arithmetic as scemc_total_energy. The call enqueues two kernels and returns;
- * the energies are ready when the stream reaches that point. It calls no
+ * the energies are ready when the stream reaches that point. The device the tables
+ * were created on must be the current device (another current device returns
+ * SCEMC_ERR_ARG), and spins, energies and stream must belong to it. It calls no
  * allocator: its scratch is a fixed device array of 65536 doubles (512 KiB) that
  * every GPU loading the library holds until exit, so ceil(n_instances / 1024) x
- * replicas must not exceed 65536 (larger requests return SCEMC_ERR_ARG). The first
- * call on each device looks up that array's device address (with the device
- * current); make that first call before any stream capture. All calls share the
+ * replicas must not exceed 65536, and replicas must not exceed 65535 (larger
+ * requests return SCEMC_ERR_ARG). The first call on each device looks up that
+ * array's device address (with the device current); make that first call before
+ * any stream capture. All calls share the
  * array: calls whose kernels overlap on the GPU (for example on two streams) race
  * and must be serialised by the caller. The kernels write every partial sum they
  * read, so nothing in the array needs to start at zero. */

@@ -880,7 +880,7 @@ double renormalize(const Ham& H, Chain& ch) {  // state.jl:168-185
 }
 
 // ---------------------------------------------------------------------------
-// Binning and observables — src/binning.jl:13-218, src/observables.jl:303-467
+// Binning and observables — src/binning.jl:13-218, src/observables.jl:85-249
 // ---------------------------------------------------------------------------
 constexpr int kMinBins = 32, kMaxLevels = 62;
 
@@ -964,7 +964,7 @@ struct BinStore {  // binning.jl:138-188
   }
 };
 
-// Observable ids in the order of standard_observables (observables.jl:303-316).
+// Observable ids in the order of standard_observables (observables.jl:85-92).
 enum { OBS_E = 0, OBS_E2, OBS_M, OBS_ABSM, OBS_M2, OBS_M4, OBS_SUB, OBS_COUNT };
 
 struct Accums {
@@ -978,7 +978,7 @@ int obs_ncomp(const Ham& H, int o) {
   return 1;
 }
 
-void measure(const Ham& H, const Chain& ch, Accums& A) {  // observables.jl:336-421
+void measure(const Ham& H, const Chain& ch, Accums& A) {  // observables.jl:104-143,186-193
   double m[3] = {0, 0, 0};
   // pairwise vs sequential summation differ by ULPs only; sequential here
   for (int s = 0; s < H.n_sites; ++s)
@@ -1053,7 +1053,7 @@ void finalize(const Ham& H, const Accums& A, const Chain& ch, double kT, double*
   };
   const double n = (double)H.n_active;
   double est, err;
-  // standard_evaluables — observables.jl:378-384
+  // standard_evaluables — observables.jl:160-166
   auto ok = [](const std::vector<std::vector<double>>& c) { return c[0].size() >= 2; };
   std::vector<std::vector<double>> ce = {col(OBS_E), col(OBS_E2)};
   if (ok(ce)) {
@@ -1082,7 +1082,7 @@ void finalize(const Ham& H, const Accums& A, const Chain& ch, double kT, double*
   out[w++] = ch.max_drift;
 }
 
-Accums make_accums(const Ham& H, int64_t planned, int nbins) {  // observables.jl:398-402
+Accums make_accums(const Ham& H, int64_t planned, int nbins) {  // observables.jl:180-184
   Accums A;
   const int64_t bs = std::max<int64_t>(1, planned / nbins);
   for (int o = 0; o < OBS_COUNT; ++o) {
@@ -1281,6 +1281,17 @@ int or_keyed_sweep(void* h, double* config, double* zrows, double* dE, int32_t* 
 }
 
 double or_reduce_dE(void* h, const double* dE) { return reduce_dE(*static_cast<Ham*>(h), dE); }
+
+// One step adaptation (updates.jl:296-305) of a chain whose Metropolis counters since
+// the last adaptation are acc / att: returns the new step.
+double or_adapt_step(double step, int64_t acc, int64_t att, double target) {
+  Chain ch;
+  ch.step = step;
+  ch.acc_metro = acc;
+  ch.att_metro = att;
+  adapt_step(ch, target);
+  return ch.step;
+}
 
 int or_swap_accepts(double kt_a, double kt_b, double E_a, double E_b, double u) {  // pt.jl:92-96
   const double logw = (1.0 / kt_a - 1.0 / kt_b) * (E_a - E_b);

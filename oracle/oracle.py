@@ -64,6 +64,7 @@ def lib() -> C.CDLL:
                                          C.c_int32, C.c_int]),
             "or_reduce_dE": (C.c_double, [C.c_void_p, F64P]),
             "or_swap_accepts": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]),
+            "or_adapt_step": (C.c_double, [C.c_double, C.c_int64, C.c_int64, C.c_double]),
             "or_replay_sweep": (None, [C.c_void_p, F64P, F64P, F64P, U8P, C.c_double, F64P, F64P, U8P, F64P]),
             "or_chain_new": (C.c_void_p, [C.c_void_p, F64P, C.c_uint64, C.c_double]),
             "or_chain_free": (None, [C.c_void_p]),
@@ -152,6 +153,12 @@ def cpow(z, p):
     out = np.zeros(2)
     lib().or_cpow(z.real, z.imag, p, _p(out, C.c_double))
     return complex(out[0], out[1])
+
+
+def adapt_step(step, acc, att, target=0.5):
+    """The step after one adaptation window with acc of att Metropolis moves accepted
+    (updates.jl:296-305)."""
+    return lib().or_adapt_step(float(step), int(acc), int(att), float(target))
 
 
 def swap_accepts(kt_a, kt_b, E_a, E_b, u):

@@ -45,7 +45,8 @@ class RunParams(C.Structure):
         ("exchange_interval", C.c_int64), ("adapt_interval", C.c_int64), ("adapt_target", C.c_double),
         ("renorm_interval", C.c_int64), ("measure_interval", C.c_int64), ("lanes_per_site", C.c_int32),
         ("mode", C.c_int32), ("phase_done", C.c_int64), ("phase_total", C.c_int64), ("kernel", C.c_int32),
-        ("proposals", C.c_int32), ("rep_replicas", C.c_int32),
+        ("proposals", C.c_int32), ("rep_replicas", C.c_int32), ("rep_threads_per_item", C.c_int32),
+        ("rep_prefetch", C.c_int32),
     ]
 
 
@@ -70,6 +71,7 @@ SIGNATURES = [
     ("scemc_tables_create", C.c_int32, [C.POINTER(TablesDesc), C.POINTER(C.c_void_p)]),
     ("scemc_tables_destroy", C.c_int32, [C.c_void_p]),
     ("scemc_tables_stats", C.c_int32, [C.c_void_p, F64P, F64P, I64P]),
+    ("scemc_tables_records", C.c_int32, [C.c_void_p, F64P]),
     ("scemc_chain_create", C.c_int32, [C.c_void_p, F64P, C.c_double, C.c_uint64, C.c_double, C.POINTER(C.c_void_p)]),
     ("scemc_chain_destroy", C.c_int32, [C.c_void_p]),
     ("scemc_metropolis_sweep", C.c_int32, [C.c_void_p, C.c_void_p, C.c_double, C.c_int32, I64P]),
@@ -116,6 +118,7 @@ SIGNATURES = [
     ("scemc_batch_reset_counters", C.c_int32, [C.c_void_p]),
     ("scemc_batch_fetch_measurements", C.c_int32, [C.c_void_p, F64P, C.c_int64, I64P, I32P]),
     ("scemc_batch_record", C.c_int32, [C.c_void_p, C.c_int32]),
+    ("scemc_batch_record_slot", C.c_int32, [C.c_void_p, C.c_int32, C.c_int32]),
     ("scemc_batch_fetch_record", C.c_int32, [C.c_void_p, C.c_int32, F32P, F64P, F32P, U8P]),
     ("scemc_color_sites", C.c_int32, [C.c_int32, I32P, I32P, I32P, I32P, U8P, I32P, I32P]),
     ("scemc_selftest_barrier_timeout", C.c_int32, [C.c_int64]),

@@ -9,6 +9,7 @@ parallel and link into one shared object.
 from __future__ import annotations
 
 import concurrent.futures as cf
+import hashlib
 import os
 import pathlib
 import shutil
@@ -32,11 +33,25 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found: the CUDA toolkit is required to build libscemc_cuda.so")
 
 
+STAMP = LIB.with_name(LIB.name + ".srchash")
+
+
+def source_hash(extra=()) -> str:
+    """SHA-256 over the sources, headers and compiler flags the library is built from."""
+    h = hashlib.sha256()
+    for p in [*SRCS, *HDRS]:
+        h.update(p.name.encode())
+        h.update(p.read_bytes())
+    h.update(" ".join([*NVCC_FLAGS, *extra]).encode())
+    return h.hexdigest()
+
+
 def stale() -> bool:
-    if not LIB.exists():
+    """True unless the library exists and its stamp holds the current source hash
+    (a prebuilt library from other sources is rebuilt, whatever its mtime)."""
+    if not LIB.exists() or not STAMP.exists():
         return True
-    t = LIB.stat().st_mtime
-    return any(p.stat().st_mtime > t for p in [*SRCS, *HDRS])
+    return STAMP.read_text().strip() != source_hash()
 
 
 def _compile(src: pathlib.Path, obj: pathlib.Path, extra) -> subprocess.CompletedProcess:
@@ -45,7 +60,7 @@ def _compile(src: pathlib.Path, obj: pathlib.Path, extra) -> subprocess.Complete
 
 
 def build(force: bool = False, verbose: bool = False, extra=(), out: pathlib.Path | None = None) -> pathlib.Path:
-    """Compile libscemc_cuda.so if it is missing or older than its sources."""
+    """Compile libscemc_cuda.so if it is missing or was built from other sources."""
     out = out or LIB
     if out == LIB and not force and not stale():
         return LIB
@@ -65,6 +80,8 @@ def build(force: bool = False, verbose: bool = False, extra=(), out: pathlib.Pat
     if link.returncode != 0:
         raise RuntimeError("link failed:\n" + link.stdout + link.stderr)
     os.replace(tmp, out)
+    if out == LIB:
+        STAMP.write_text(source_hash(extra) + "\n")
     return out
 
 

@@ -173,7 +173,8 @@ struct SweepArgs {
   long long barrier_limit_ns;
   unsigned long long bar_base;  // arrival count at launch (persistent form)
   const EnsState* st;           // device sweep counter (read by every launch, so graphs stay valid)
-  // replay recording (slot 0 of lattice 0), may be null
+  // replay recording (replica rec_r of lattice rec_li), may be null
+  int32_t rec_li, rec_r, rec_cap;  // rec_cap: sites per recorded pass
   float* rec_prop;
   double* rec_u;
   float* rec_dE;
@@ -521,8 +522,8 @@ __device__ void sweep_colour(const SweepArgs& a, int col, unsigned long long* s_
     } else if (acc) {
       atomicAdd(s_cnt + 3 * slot + 0, 1u);
     }
-    if (a.rec_prop != nullptr && li == 0 && r == 0 && a.pass + 1 < kRecPasses) {
-      const int64_t q = (int64_t)(a.pass + 1) * L.n_sites + s;
+    if (a.rec_prop != nullptr && li == a.rec_li && r == a.rec_r && a.pass + 1 < kRecPasses) {
+      const int64_t q = (int64_t)(a.pass + 1) * a.rec_cap + s;
       a.rec_prop[3 * q + 0] = px;
       a.rec_prop[3 * q + 1] = py;
       a.rec_prop[3 * q + 2] = pz;
@@ -895,8 +896,8 @@ __device__ void fast_colour(const SweepArgs& a, int col, unsigned long long* s_d
     } else if (acc_ok) {
       atomicAdd(s_cnt + 3 * slot + 0, 1u);
     }
-    if (a.rec_prop != nullptr && li == 0 && r == 0 && a.pass + 1 < kRecPasses) {
-      const int64_t qq = (int64_t)(a.pass + 1) * L.n_sites + s;
+    if (a.rec_prop != nullptr && li == a.rec_li && r == a.rec_r && a.pass + 1 < kRecPasses) {
+      const int64_t qq = (int64_t)(a.pass + 1) * a.rec_cap + s;
       a.rec_prop[3 * qq + 0] = px;
       a.rec_prop[3 * qq + 1] = py;
       a.rec_prop[3 * qq + 2] = pz;
@@ -1276,8 +1277,8 @@ __device__ void rep_colour(const SweepArgs& a, int col, unsigned long long* s_dE
       } else if (acc_ok) {
         atomicAdd(s_cnt + 3 * slot + 0, 1u);
       }
-      if (a.rec_prop != nullptr && li == 0 && r == 0 && a.pass + 1 < kRecPasses) {
-        const int64_t qq = (int64_t)(a.pass + 1) * L.n_sites + s;
+      if (a.rec_prop != nullptr && li == a.rec_li && r == a.rec_r && a.pass + 1 < kRecPasses) {
+        const int64_t qq = (int64_t)(a.pass + 1) * a.rec_cap + s;
         a.rec_prop[3 * qq + 0] = px;
         a.rec_prop[3 * qq + 1] = py;
         a.rec_prop[3 * qq + 2] = pz;
@@ -1580,8 +1581,8 @@ __global__ void __launch_bounds__(256, 2) k_learned_fused(SweepArgs a, LearnedNe
       atomicAdd(s_dE + slot, (unsigned long long)llrint((double)dE * kFixScale));
       atomicAdd(s_cnt + 3 * slot + 0, 1u);
     }
-    if (a.rec_prop != nullptr && li == 0 && r == 0 && a.pass + 1 < kRecPasses) {
-      const int64_t qq = (int64_t)(a.pass + 1) * L.n_sites + s;
+    if (a.rec_prop != nullptr && li == a.rec_li && r == a.rec_r && a.pass + 1 < kRecPasses) {
+      const int64_t qq = (int64_t)(a.pass + 1) * a.rec_cap + s;
       a.rec_prop[3 * qq + 0] = xs[0];
       a.rec_prop[3 * qq + 1] = xs[1];
       a.rec_prop[3 * qq + 2] = xs[2];
@@ -1772,7 +1773,7 @@ __global__ void k_normalize(const DevLattice* lat, int li, float4* spins) {
   }
 }
 
-// ---- measurements (observables.jl:303-360) -----------------------------------
+// ---- measurements (observables.jl:85-143) -----------------------------------
 
 // Partial sums per (chunk, replica): {m_x, m_y, m_z} over active sites and the
 // sublattice sums {x_a, y_a, z_a}; record layout per slot: 3 + 3*n_cell_atoms.
@@ -1907,8 +1908,10 @@ struct scemc_ensemble {
   double* d_meas = nullptr;
   int64_t meas_cap = 0, meas_n = 0;
   int32_t rec_len = 0;
-  // replay record
+  // replay record (replica rec_r of table rec_li; buffers sized for the largest table)
   bool recording = false;
+  int32_t rec_li = 0, rec_r = 0;
+  int32_t rec_cap = 0;  // sites the record buffers hold
   float* d_rprop = nullptr;
   double* d_ru = nullptr;
   float* d_rdE = nullptr;
@@ -1942,7 +1945,7 @@ struct scemc_ensemble {
   int tuned_mode = 2, tuned_proposals = 0, tuned_lanes = 0, tuned_kernel = 0;
   // captured compound-sweep graphs keyed by {n_or, fast, precompute, G, recording}
   struct GraphEntry {
-    int key[5];
+    int key[7];
     cudaGraphExec_t exec;
     int64_t launches;  // kernel nodes in the graph
   };
@@ -2727,6 +2730,9 @@ SweepArgs make_args(scemc_ensemble* E, int pass) {
   a.gs = E->d_gs;
   a.barrier_limit_ns = E->barrier_limit_ns;
   if (E->recording) {
+    a.rec_li = E->rec_li;
+    a.rec_r = E->rec_r;
+    a.rec_cap = E->rec_cap;
     a.rec_prop = E->d_rprop;
     a.rec_u = E->d_ru;
     a.rec_dE = E->d_rdE;
@@ -2779,6 +2785,8 @@ struct Launch {
   bool learned = false;     // Metropolis proposals from the learned network, per colour
   bool flow = false;        // persistent form with per-item completion flags instead of grid barriers
   int rep_p = 0;            // replica-parallel kernel: replicas per thread (0 = per colour, by its size)
+  int rep_np = 0;           // replica-parallel kernel: threads per item (0 = per colour, by its size)
+  int rep_pf = 0;           // replica-parallel kernel: 1 prefetch, 2 no prefetch (0 = per colour, by its size)
 };
 
 using FastFn = void (*)(SweepArgs);
@@ -2873,7 +2881,7 @@ struct RepForm {
   int32_t pf;
   FastFn fn;
 };
-RepForm rep_form(const scemc_ensemble* E, int c, int forced) {
+RepForm rep_form(const scemc_ensemble* E, int c, int forced, int forced_np = 0, int forced_pf = 0) {
   RepForm f;
   const int64_t sms = sm_count(E->device);
   const int64_t nt1 = rep_threads(E, c, 1);
@@ -2883,10 +2891,10 @@ RepForm rep_form(const scemc_ensemble* E, int c, int forced) {
   // Measured (ms per sweep of 16 rungs, bcc body-4): 32^3 0.49 against 0.55 with
   // P = 2; 40^3 (above the threshold) 0.70 with P = 2 against 0.76 with P = 1.
   // NP depends on the colour's size only, so a forced P does not change the chains.
-  const int NP = 2 * nt1 <= sms * 1024 ? 2 : 1;
+  const int NP = forced_np == 1 || forced_np == 2 ? forced_np : (2 * nt1 <= sms * 1024 ? 2 : 1);
   f.P = forced == 1 || forced == 2 ? forced : (NP == 2 ? 1 : 2);
   f.nt = rep_threads(E, c, f.P) * NP;
-  f.pf = f.nt <= sms * (f.P == 1 ? 1024 : 768) * 2 ? 1 : 0;
+  f.pf = forced_pf == 1 ? 1 : forced_pf == 2 ? 0 : (f.nt <= sms * (f.P == 1 ? 1024 : 768) * 2 ? 1 : 0);
   // [lmax - 1][P - 1][NP - 1][pf]
   static const FastFn forms[2][2][2][2] = {
       {{{k_rep_colour<1, 1, 1, false>, k_rep_colour<1, 1, 1, true>},
@@ -2975,7 +2983,7 @@ int32_t run_pass_impl(scemc_ensemble* E, int pass, const Launch& Lc) {
       const int n = E->seg[(size_t)c * (E->tabs.size() + 1) + E->tabs.size()];
       if (n == 0) continue;
       a.colour = c;
-      const RepForm f = rep_form(E, c, Lc.rep_p);
+      const RepForm f = rep_form(E, c, Lc.rep_p, Lc.rep_np, Lc.rep_pf);
       CUDA_TRY(cudaFuncSetAttribute((const void*)f.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       const int blocks = (int)std::min<int64_t>(cap, (f.nt + threads - 1) / threads);
       ++E->launches;
@@ -3212,10 +3220,14 @@ int auto_lanes(const scemc_ensemble* E) {
 // kernel: 0 auto, 1 generic, 2 row-parallel fast, 3 replica-parallel; proposals: 0 auto,
 // 1 precompute, 2 inline.
 int32_t resolve_launch(const scemc_ensemble* E, int lanes, int mode, int kernel, int proposals, Launch* out,
-                       int rep_replicas = 0) {
+                       int rep_replicas = 0, int rep_np = 0, int rep_pf = 0) {
   Launch L;
   if (rep_replicas < 0 || rep_replicas > 2) return fail(SCEMC_ERR_ARG, "rep_replicas must be 0, 1 or 2");
+  if (rep_np < 0 || rep_np > 2) return fail(SCEMC_ERR_ARG, "rep_threads_per_item must be 0, 1 or 2");
+  if (rep_pf < 0 || rep_pf > 2) return fail(SCEMC_ERR_ARG, "rep_prefetch must be 0, 1 or 2");
   L.rep_p = rep_replicas;
+  L.rep_np = rep_np;
+  L.rep_pf = rep_pf;
   if (mode == 0 && kernel == 0 && E->tuned) {
     mode = E->tuned_mode;
     kernel = E->tuned_kernel;
@@ -3289,10 +3301,11 @@ int32_t sweep_once(scemc_ensemble* E, int n_or, const Launch& L) {
 // configuration, replayed every sweep). Every launch reads the sweep counter from
 // device memory and the tail advances it, so one capture serves all sweeps.
 int32_t sweep_graph(scemc_ensemble* E, int n_or, const Launch& L, cudaGraphExec_t* out, int64_t* n_launch) {
-  const int key[5] = {n_or, L.rep ? 2 : (L.fast ? 1 : 0), L.learned ? 2 : (L.precompute ? 1 : 0),
-                      L.fast ? 0 : (L.rep ? L.rep_p : L.G), E->recording ? 1 : 0};
+  const int key[7] = {n_or, L.rep ? 2 : (L.fast ? 1 : 0), L.learned ? 2 : (L.precompute ? 1 : 0),
+                      L.fast ? 0 : (L.rep ? L.rep_p : L.G), E->recording ? 1 : 0, L.rep ? L.rep_np : 0,
+                      L.rep ? L.rep_pf : 0};
   for (auto& g : E->graphs)
-    if (std::equal(key, key + 5, g.key)) {
+    if (std::equal(key, key + 7, g.key)) {
       *out = g.exec;
       *n_launch = g.launches;
       return SCEMC_OK;
@@ -3312,7 +3325,7 @@ int32_t sweep_graph(scemc_ensemble* E, int n_or, const Launch& L, cudaGraphExec_
   if (L.rep) {
     const size_t smem = fast_param_floats(E->n_slots) * sizeof(float);
     for (int c = 0; c < E->max_colors; ++c)
-      CUDA_TRY(cudaFuncSetAttribute((const void*)rep_form(E, c, L.rep_p).fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      CUDA_TRY(cudaFuncSetAttribute((const void*)rep_form(E, c, L.rep_p, L.rep_np, L.rep_pf).fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem));
   }
   const bool prof = E->profiling;
@@ -3336,7 +3349,7 @@ int32_t sweep_graph(scemc_ensemble* E, int n_or, const Launch& L, cudaGraphExec_
   cudaGraphDestroy(graph);
   if (ie != cudaSuccess) return fail(SCEMC_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
   scemc_ensemble::GraphEntry g;
-  std::copy(key, key + 5, g.key);
+  std::copy(key, key + 7, g.key);
   g.exec = exec;
   g.launches = captured;
   E->graphs.push_back(g);
@@ -3388,6 +3401,12 @@ int32_t scemc_tables_stats(const scemc_tables* t, double* d_mean, double* a_mean
   if (d_mean) *d_mean = t->d_mean;
   if (a_mean) *a_mean = t->a_mean;
   if (bytes) *bytes = t->bytes;
+  return SCEMC_OK;
+}
+
+int32_t scemc_tables_records(const scemc_tables* t, double* records_mean) {
+  if (!t || !records_mean) return fail(SCEMC_ERR_ARG, "NULL argument");
+  *records_mean = t->n_active ? (double)t->fast_records / t->n_active : 0.0;
   return SCEMC_OK;
 }
 
@@ -3590,7 +3609,9 @@ int32_t scemc_batch_run_async(scemc_batch* b, const scemc_run_params* p) {
   const int64_t total = p->phase_total > 0 ? p->phase_total : p->phase_done + p->nsweeps;
   int32_t rc;
   Launch L;
-  if ((rc = resolve_launch(b, p->lanes_per_site, p->mode, p->kernel, p->proposals, &L, p->rep_replicas))) return rc;
+  if ((rc = resolve_launch(b, p->lanes_per_site, p->mode, p->kernel, p->proposals, &L, p->rep_replicas, p->rep_threads_per_item,
+                           p->rep_prefetch)))
+    return rc;
   if (b->sweep_index + p->nsweeps >= 0x7ffffffell - 1)
     return fail(SCEMC_ERR_EXHAUSTED, "sweep_index would exhaust the 32-bit RNG counter word");
   cudaGraphExec_t exec = nullptr;
@@ -3899,15 +3920,29 @@ int32_t scemc_batch_record(scemc_batch* b, int32_t on) {
   b->recording = on != 0;
   for (auto& g : b->graphs) cudaGraphExecDestroy(g.exec);
   b->graphs.clear();
-  const size_t n = (size_t)b->tabs[0]->n_sites * kRecPasses;
+  int32_t cap = 0;
+  for (const scemc_tables* T : b->tabs) cap = std::max(cap, T->n_sites);
+  const size_t n = (size_t)cap * kRecPasses;
   if (b->recording && !b->d_rprop) {
     int32_t rc;
     if ((rc = dalloc(&b->d_rprop, 3 * n)) || (rc = dalloc(&b->d_ru, n)) || (rc = dalloc(&b->d_rdE, n)) ||
-        (rc = dalloc(&b->d_racc, n)) || (rc = dalloc(&b->d_rlqr, (size_t)b->tabs[0]->n_sites)))
+        (rc = dalloc(&b->d_racc, n)) || (rc = dalloc(&b->d_rlqr, (size_t)cap)))
       return rc;
+    b->rec_cap = cap;
   }
-  if (b->recording) CUDA_TRY(cudaMemset(b->d_rlqr, 0, sizeof(double) * b->tabs[0]->n_sites));
+  if (b->recording) CUDA_TRY(cudaMemset(b->d_rlqr, 0, sizeof(double) * cap));
   if (b->recording) CUDA_TRY(cudaMemset(b->d_racc, 3, n));  // 3 = site not visited
+  return SCEMC_OK;
+}
+
+int32_t scemc_batch_record_slot(scemc_batch* b, int32_t table, int32_t replica) {
+  if (!b) return fail(SCEMC_ERR_ARG, "batch is NULL");
+  if (table < 0 || table >= (int32_t)b->tabs.size()) return fail(SCEMC_ERR_ARG, "record table out of range");
+  if (replica < 0 || replica >= b->R[table]) return fail(SCEMC_ERR_ARG, "record replica out of range");
+  b->rec_li = table;
+  b->rec_r = replica;
+  for (auto& g : b->graphs) cudaGraphExecDestroy(g.exec);  // captured launches carry the old slot
+  b->graphs.clear();
   return SCEMC_OK;
 }
 
@@ -3915,7 +3950,7 @@ int32_t scemc_batch_fetch_record(const scemc_batch* b, int32_t pass, float* prop
                                  uint8_t* acc) {
   if (!b || !b->d_rprop) return fail(SCEMC_ERR_ARG, "recording was never enabled");
   if (pass < -1 || pass + 1 >= kRecPasses) return fail(SCEMC_ERR_ARG, "pass outside -1..2");
-  const size_t n = (size_t)b->tabs[0]->n_sites, o = (size_t)(pass + 1) * n;
+  const size_t n = (size_t)b->tabs[b->rec_li]->n_sites, o = (size_t)(pass + 1) * (size_t)b->rec_cap;
   if (prop) CUDA_TRY(cudaMemcpy(prop, b->d_rprop + 3 * o, 12 * n, cudaMemcpyDeviceToHost));
   if (u) CUDA_TRY(cudaMemcpy(u, b->d_ru + o, 8 * n, cudaMemcpyDeviceToHost));
   if (dE) CUDA_TRY(cudaMemcpy(dE, b->d_rdE + o, 4 * n, cudaMemcpyDeviceToHost));
@@ -3925,7 +3960,7 @@ int32_t scemc_batch_fetch_record(const scemc_batch* b, int32_t pass, float* prop
 
 int32_t scemc_batch_fetch_record_ratio(const scemc_batch* b, double* lqr) {
   if (!b || !b->d_rlqr || !lqr) return fail(SCEMC_ERR_ARG, "recording was never enabled");
-  CUDA_TRY(cudaMemcpy(lqr, b->d_rlqr, sizeof(double) * b->tabs[0]->n_sites, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(lqr, b->d_rlqr, sizeof(double) * b->tabs[b->rec_li]->n_sites, cudaMemcpyDeviceToHost));
   return SCEMC_OK;
 }
 
@@ -4205,8 +4240,15 @@ extern "C" int32_t scemc_total_energy_static(const scemc_tables* t, const void* 
     return fail(SCEMC_ERR_ARG, "scemc_total_energy_static: ceil(n_instances/1024) x replicas = " +
                                    std::to_string(n_chunks * replicas) + " exceeds the fixed scratch of " +
                                    std::to_string(kStaticScratch) + " partial sums");
+  // one grid row per replica: the y dimension of a launch grid stops at 65535
+  if (replicas > 65535) return fail(SCEMC_ERR_ARG, "scemc_total_energy_static: replicas must be <= 65535");
   int dev = 0;
   CUDA_TRY(cudaGetDevice(&dev));
+  // the kernels read the tables' device pointers: they must run on the tables' device
+  if (dev != t->device)
+    return fail(SCEMC_ERR_ARG, "scemc_total_energy_static: the current device is " + std::to_string(dev) +
+                                   " but the tables live on device " + std::to_string(t->device) +
+                                   "; make that device current");
   if (dev < 0 || dev >= kMaxDevices) return fail(SCEMC_ERR_ARG, "device index out of range");
   double* scratch = nullptr;
   {

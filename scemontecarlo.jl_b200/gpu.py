@@ -1,11 +1,11 @@
 """The reference's device-path API over libscemc_cuda.so.
 
 Names, argument meaning and error behaviour follow src/gpu/*.jl:
-  GPUTiledHamiltonian  gpu_hamiltonian.jl:433-460
-  GPUChainState        gpu_state.jl:305-347
+  GPUTiledHamiltonian  gpu_hamiltonian.jl:61-88
+  GPUChainState        gpu_state.jl:19-61
   gpu_metropolis_sweep gpu_sweep.jl:158-190
   gpu_run_sweeps       gpu_sweep.jl:204-218
-  to_host / from_host  gpu_state.jl:357-372
+  to_host / from_host  gpu_state.jl:71-86
   swap_payload         gpu_pt.jl:46-51
   gpu_run_pt           gpu_pt.jl:261-316
 plus the device overrelaxation sweep (the reference has it on the CPU only,
@@ -58,6 +58,12 @@ class GPUTiledHamiltonian:
         dm, am, by = C.c_double(), C.c_double(), C.c_int64()
         check(_lib.lib().scemc_tables_stats(self.h, C.byref(dm), C.byref(am), C.byref(by)))
         return dm.value, am.value, by.value
+
+    def records_per_site(self) -> float:
+        """Mean merged records per active site that the fast kernels walk."""
+        r = C.c_double()
+        check(_lib.lib().scemc_tables_records(self.h, C.byref(r)))
+        return r.value
 
 
 @dataclass
@@ -142,7 +148,7 @@ class GPUChainState:
         return float(d[0])
 
 
-def gpu_metropolis_sweep(gst: GPUChainState, gH: GPUTiledHamiltonian, beta: float, workgroupsize: int = 32) -> int:
+def gpu_metropolis_sweep(gst: GPUChainState, gH: GPUTiledHamiltonian, beta: float, workgroupsize: int = 128) -> int:
     """One device Metropolis sweep; returns the number of accepted moves."""
     if not _ispow2(int(workgroupsize)):
         raise ValueError(f"workgroupsize must be a power of two (got {workgroupsize})")
@@ -152,7 +158,7 @@ def gpu_metropolis_sweep(gst: GPUChainState, gH: GPUTiledHamiltonian, beta: floa
 
 
 def gpu_overrelaxation_sweep(gst: GPUChainState, gH: GPUTiledHamiltonian, beta: float,
-                             workgroupsize: int = 32):
+                             workgroupsize: int = 128):
     """One device overrelaxation sweep; returns (accepted, attempted)."""
     if not _ispow2(int(workgroupsize)):
         raise ValueError(f"workgroupsize must be a power of two (got {workgroupsize})")
@@ -190,7 +196,7 @@ def gpu_energy_gradient(gH: GPUTiledHamiltonian, config) -> np.ndarray:
 
 
 def gpu_run_sweeps(gst: GPUChainState, gH: GPUTiledHamiltonian, st: ChainState, beta: float, nsweeps: int,
-                   renorm_interval: int = 1000, workgroupsize: int = 32) -> GPUChainState:
+                   renorm_interval: int = 1000, workgroupsize: int = 128) -> GPUChainState:
     """nsweeps device Metropolis sweeps with a device renormalisation + FP64 recompute
     every renorm_interval sweeps (<= 0 disables); downloads the state into st."""
     if not _ispow2(int(workgroupsize)):
@@ -278,11 +284,12 @@ class GPUBatch:
     @staticmethod
     def params(nsweeps, or_per_metropolis=0, exchange=False, exchange_interval=1, adapt_interval=0,
                adapt_target=0.5, renorm_interval=0, measure_interval=0, lanes_per_site=0, mode=0, phase_done=0,
-               phase_total=0, kernel=0, proposals=0, rep_replicas=0) -> _lib.RunParams:
+               phase_total=0, kernel=0, proposals=0, rep_replicas=0, rep_threads_per_item=0,
+               rep_prefetch=0) -> _lib.RunParams:
         return _lib.RunParams(int(nsweeps), int(or_per_metropolis), int(bool(exchange)), int(exchange_interval),
                               int(adapt_interval), float(adapt_target), int(renorm_interval), int(measure_interval),
                               int(lanes_per_site), int(mode), int(phase_done), int(phase_total), int(kernel),
-                              int(proposals), int(rep_replicas))
+                              int(proposals), int(rep_replicas), int(rep_threads_per_item), int(rep_prefetch))
 
     def run(self, nsweeps, **kw):
         """Runs `nsweeps` compound sweeps (see scemc_run_params) and waits for them."""
@@ -355,7 +362,7 @@ class GPUBatch:
 
     def fetch_record_ratio(self) -> np.ndarray:
         """log q(e|env) - log q(e'|env) of the recorded learned Metropolis pass."""
-        out = np.zeros(self.gHs[0].n_sites)
+        out = np.zeros(self.gHs[getattr(self, "_rec_table", 0)].n_sites)
         check(_lib.lib().scemc_batch_fetch_record_ratio(self.h, ptr(out, C.c_double)))
         return out
 
@@ -425,10 +432,15 @@ class GPUBatch:
     def record(self, on: bool):
         check(_lib.lib().scemc_batch_record(self.h, int(bool(on))))
 
+    def record_slot(self, table: int = 0, replica: int = 0):
+        """Chooses the recorded replica (0-based replica of 0-based table)."""
+        check(_lib.lib().scemc_batch_record_slot(self.h, int(table), int(replica)))
+        self._rec_table = int(table)
+
     def fetch_record(self, pass_: int = -1):
-        """Recorded (proposal, u, dE32, flag) of slot 0 for pass -1 (Metropolis) or
-        overrelaxation pass k."""
-        n = self.gHs[0].n_sites
+        """Recorded (proposal, u, dE32, flag) of the recorded replica for pass -1
+        (Metropolis) or overrelaxation pass k."""
+        n = self.gHs[getattr(self, "_rec_table", 0)].n_sites
         prop = np.zeros(3 * n, np.float32)
         u = np.zeros(n)
         dE = np.zeros(n, np.float32)

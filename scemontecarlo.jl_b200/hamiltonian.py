@@ -57,7 +57,7 @@ def _lm0(l: int, m: int) -> int:
 
 
 def resolve_kt(temperature=None, kT=None) -> np.ndarray:
-    """src/units.jl:507-528: exactly one of kelvin `temperature` or `kT`."""
+    """src/units.jl:40-61: exactly one of kelvin `temperature` or `kT`."""
     if (temperature is None) == (kT is None):
         raise ValueError("provide exactly one of `temperature` (kelvin) or `kT` (k_B·T, model energy units)")
     if kT is not None:

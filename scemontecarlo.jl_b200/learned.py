@@ -194,6 +194,58 @@ def collect_training_set(H, env, kts, n_rows: int, *, sweeps_therm: int = 2000, 
     return X, Y
 
 
+def fibonacci_sphere(n: int) -> np.ndarray:
+    """n nearly uniform unit vectors (golden-angle spiral), (n, 3)."""
+    i = np.arange(n) + 0.5
+    z = 1.0 - 2.0 * i / n
+    r = np.sqrt(np.maximum(0.0, 1.0 - z * z))
+    ph = np.pi * (3.0 - np.sqrt(5.0)) * i
+    return np.stack([r * np.cos(ph), r * np.sin(ph), z], axis=1)
+
+
+def ordered_energies(gH, directions) -> np.ndarray:
+    """FP64 energy per site of the uniform states e_s = n for each direction n (one
+    device batch, one replica per direction; the library's energy recompute)."""
+    from .gpu import GPUBatch
+    d = np.asarray(directions, np.float64).reshape(-1, 3)
+    d = d / np.linalg.norm(d, axis=1, keepdims=True)
+    ns = gH.n_sites
+    out = []
+    for i in range(0, len(d), 512):  # a batch holds at most 512 replica slots
+        part = d[i:i + 512]
+        cfgs = [np.broadcast_to(v, (ns, 3)) for v in part]
+        b = GPUBatch([gH], [len(part)], cfgs, np.arange(1, len(part) + 1), 0.6)
+        out.append(b.download()["energies"] / gH.host.n_active)
+    return np.concatenate(out)
+
+
+def easy_axis(gH, n_dirs: int = 4096, rounds: int = 3) -> np.ndarray:
+    """The direction n that minimises the energy of the uniform state e_s = n: the
+    orientation a ferromagnetically ordered chain relaxes to when anisotropic terms
+    (l = 1 body-3/body-4 products with random coefficients) pick an easy axis. A
+    chain started ordered along another axis has to rotate its whole magnetisation,
+    which local moves do slowly on large lattices; starting along n removes that
+    transient. Grid search on a Fibonacci sphere, then `rounds` refinements on
+    shrinking caps around the best direction. gH should be a small lattice of the
+    same model (the uniform state's energy per site does not depend on its size)."""
+    dirs = fibonacci_sphere(n_dirs)
+    e = ordered_energies(gH, dirs)
+    best = dirs[int(np.argmin(e))]
+    width = 2.0 / np.sqrt(n_dirs)
+    for _ in range(rounds):
+        t1 = np.cross(best, [1.0, 0.0, 0.0] if abs(best[0]) < 0.9 else [0.0, 1.0, 0.0])
+        t1 /= np.linalg.norm(t1)
+        t2 = np.cross(best, t1)
+        g = np.linspace(-width, width, 21)
+        a, c = np.meshgrid(g, g)
+        cand = best + a.reshape(-1, 1) * t1 + c.reshape(-1, 1) * t2
+        cand /= np.linalg.norm(cand, axis=1, keepdims=True)
+        e = ordered_energies(gH, cand)
+        best = cand[int(np.argmin(e))]
+        width /= 8.0
+    return best
+
+
 def ess_per_second(result) -> tuple:
     """(ESS/s, per-point ESS, per-point max tau_int) of a PT/run_mc result:
     ESS = n_meas / (1 + 2 max(tau_int(E), tau_int(|m|))) summed over the points

@@ -27,7 +27,7 @@ Z3 = (0, 0, 0)
 # reference test fixtures (test/unit/fixtures.jl, test/unit/test_energy.jl)
 # ---------------------------------------------------------------------------
 def chain_terms(J: float):
-    """Both directed members of the +x bond of a 1-atom chain (fixtures.jl:94-103)."""
+    """Both directed members of the +x bond of a 1-atom chain (test/unit/fixtures.jl:94-103)."""
     folded = np.eye(3)
     raw = J / (2 * N1 ** 2 * FOUR_PI)
     return [MultipoleTerm(raw, [1, 1], [Z3, (1, 0, 0)], [1, 1], folded.copy()),
@@ -35,7 +35,7 @@ def chain_terms(J: float):
 
 
 def threebody_terms(J: float):
-    """3-body chain cluster (0, +x, +2x) (fixtures.jl:109-117); triplet fast path."""
+    """3-body chain cluster (0, +x, +2x) (test/unit/fixtures.jl:109-117); triplet fast path."""
     f = np.zeros((3, 3, 3))
     f[1, 1, 1] = 1.0
     f[0, 2, 0] = 0.7
@@ -44,7 +44,7 @@ def threebody_terms(J: float):
 
 
 def fourbody_terms(J: float):
-    """4-body chain cluster (0, +x, +2x, +3x) (fixtures.jl:122-131); general path."""
+    """4-body chain cluster (0, +x, +2x, +3x) (test/unit/fixtures.jl:122-131); general path."""
     f = np.zeros((3, 3, 3, 3))
     f[1, 1, 1, 1] = 1.0
     f[0, 2, 1, 0] = 0.6
@@ -55,7 +55,7 @@ def fourbody_terms(J: float):
 def dimer_terms(J: float = -0.02):
     """Isotropic l = 1 pair between atoms 1 and 2 of a 4-atom cell; atoms 3 and 4 are
     untouched (inactive). Energy J e1 . e2 per cell (the fitted dimer of
-    fixtures.jl:27-31, restated as a hand-built term)."""
+    test/unit/fixtures.jl:27-31, restated as a hand-built term)."""
     return [MultipoleTerm(J / 3.0, [1, 2], [Z3, Z3], [1, 1], np.eye(3))]
 
 
@@ -65,7 +65,7 @@ def dimer(dims=(1, 1, 1), J: float = -0.02, **kw) -> TiledHamiltonian:
 
 def biquadratic_terms(seed: int, scale: float = 0.05):
     """Anisotropic l <= 2 pair between the two atoms of a 2-atom cell: one template
-    per (l1, l2) in {1,2}^2 with N(0, scale) entries (fixtures.jl:55-61 restated)."""
+    per (l1, l2) in {1,2}^2 with N(0, scale) entries (test/unit/fixtures.jl:55-61 restated)."""
     rng = np.random.default_rng(seed)
     out = []
     for l1, l2 in itertools.product((1, 2), (1, 2)):

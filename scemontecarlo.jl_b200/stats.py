@@ -1,6 +1,6 @@
 """Host-side statistics of a run: streaming log-binning, bin stores, jackknife and
 the standard observables/evaluables (src/binning.jl:13-218,
-src/observables.jl:303-467), fed by the measurement records the device writes
+src/observables.jl:85-249), fed by the measurement records the device writes
 (one row per measurement and rung: E, m over active sites, sublattice sums).
 """
 from __future__ import annotations
@@ -191,7 +191,7 @@ class PTResult:
 
 
 class StandardAccumulators:
-    """The standard observables of one rung (observables.jl:303-316) accumulated
+    """The standard observables of one rung (observables.jl:85-92) accumulated
     from device records {E, m_x, m_y, m_z, sub_x1, sub_y1, sub_z1, ...}."""
 
     def __init__(self, n_cell_atoms: int, planned: int, nbins: int = 32):
@@ -226,7 +226,7 @@ class StandardAccumulators:
             self.stores[n].push_many(vals[n])
 
     def finalize(self, kT: float, n_active: int) -> dict:
-        """_finalize_stats (observables.jl:425-467) with the standard evaluables."""
+        """_finalize_stats (observables.jl:207-249) with the standard evaluables."""
         stats = {}
         for n, _ in self.names:
             b = self.binners[n]

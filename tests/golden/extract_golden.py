@@ -1,6 +1,6 @@
 """Extracts the known-answer vectors that SCEMonteCarlo.jl's own test suite holds
-for the sweep path into philox_kat.json (run once, in a container where the
-reference is checked out; the tests read only the JSON).
+for the sweep path into philox_kat.json (run once, with the path of a checkout of
+the reference as its argument; the tests read only the JSON).
 
 Source: test/unit/test_gpu.jl:49-59 — the Random123 philox4x32-10 known answers
 the reference gates its keyed RNG on — and the open-interval edge words of
@@ -11,7 +11,9 @@ import pathlib
 import re
 import sys
 
-REF = pathlib.Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+if len(sys.argv) != 2:
+    sys.exit("usage: python extract_golden.py <SCEMonteCarlo.jl checkout>")
+REF = pathlib.Path(sys.argv[1])
 src = (REF / "test" / "unit" / "test_gpu.jl").read_text()
 hexes = r"\((0x[0-9a-f]+), (0x[0-9a-f]+), (0x[0-9a-f]+), (0x[0-9a-f]+)\)"
 pat = re.compile(r"MC\._philox4x32\(" + hexes + r",\s*\((0x[0-9a-f]+), (0x[0-9a-f]+)\)\)\s*==\s*" + hexes)

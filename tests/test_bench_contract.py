@@ -1,5 +1,6 @@
 """The bench's reference arm on CPU: one JSON line with the fields the measurement
-contract needs (the CPU port of the reference sweep, timed on the host cores)."""
+contract needs (the CPU port of the reference sweep, timed on the host cores), and
+the bench's committed DRAM-traffic record."""
 import json
 import pathlib
 import subprocess
@@ -21,4 +22,13 @@ def test_reference_arm_prints_one_contract_line():
     assert d["impl"] == "reference" and d["metric"] == "spin-updates/s" and d["unit"] == "attempts/s"
     assert d["value"] > 0 and d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
-    assert d["config"]["workload"].startswith("bcc16")
+    # the default workload is the large frustrated configuration, and the reference arm
+    # runs the oracle's port alone: the CUDA library is never mapped into that process
+    assert d["config"]["workload"].startswith("fcc64") and d["config"]["sites_per_chain"] == 4 * 64 ** 3
+    assert d["config"]["libscemc_cuda_loaded"] is False
+
+
+def test_dram_traffic_record_names_the_default_workload():
+    d = json.loads((ROOT / "profiles" / "dram_traffic.json").read_text())
+    rec = d["fcc64_l2_tri_zeeman_32rungs_metropolis+OR+exchange"]
+    assert 100 < rec["bytes_per_attempt"] < 5000 and rec["source"]

@@ -64,8 +64,10 @@ def f32_normalised(v):
     return (v / np.sqrt((v[0] * v[0] + v[1] * v[1]) + v[2] * v[2])).astype(np.float32)
 
 
-def check_pass(OH, cfg, rec, beta, kind, seed=None, sweep=None, step=None, orpass=0):
-    """Replays one recorded pass; returns (#ties, #attempted). cfg updated in place."""
+def check_pass(OH, cfg, rec, beta, kind, seed=None, sweep=None, step=None, orpass=0, sample=None):
+    """Replays one recorded pass; returns (#ties, #attempted). cfg updated in place.
+    dE and the decisions are checked at every site; the proposals at every site, or
+    at `sample` random sites of a large lattice (the check is a Python loop)."""
     prop, u, dE32, flag = rec
     pre = cfg.copy()
     dev_acc = (flag == 1).astype(np.uint8)
@@ -89,8 +91,12 @@ def check_pass(OH, cfg, rec, beta, kind, seed=None, sweep=None, step=None, orpas
     mism = att & ((flag == 1) != oacc)
     assert not (mism & ~tie).any(), np.nonzero(mism & ~tie)[0][:5]
     n_sites = len(flag)
+    pick = np.arange(n_sites)
+    if sample is not None and sample < n_sites:
+        pick = np.sort(np.random.default_rng(sweep).choice(n_sites, sample, replace=False))
     if kind == "metro":
-        for s in np.nonzero(active)[0]:
+        for s in np.nonzero(active[pick])[0]:
+            s = pick[s]
             b0 = O.philox_block(seed, int(s) + 1, sweep, 0)
             if O.philox_uniform(b0[0], b0[1]) < 0.2:
                 exp = (-pre[s]).astype(np.float32)
@@ -99,7 +105,8 @@ def check_pass(OH, cfg, rec, beta, kind, seed=None, sweep=None, step=None, orpas
                 exp = f32_normalised(e2)
             assert np.max(np.abs(prop[s] - exp)) <= F32_ULP, (s, prop[s], exp)
     else:
-        for s in np.nonzero(visited)[0]:
+        for s in np.nonzero(visited[pick])[0]:
+            s = pick[s]
             h = np.array([c[s, 3], c[s, 1], c[s, 2]])
             hn = np.linalg.norm(h)
             if flag[s] == 2:
@@ -161,6 +168,143 @@ def test_sweep_replay(gpu, name, lanes, mode, kernel, proposals):
         # the running (FP32 dE, fixed-point summed) energy tracks the recompute
         assert abs(post["energies"][0] - E_or) <= 1e-5 * max(1.0, abs(E_or))
     assert ties <= max(1, att // 100)
+
+
+# Every instance k_rep_colour<LMAX, P, NP, PF> of the replica-parallel kernel, forced
+# through the run parameters: P replicas per thread, NP threads per item, PF prefetch
+# (1 on, 2 off). Three replicas, so a P = 2 thread (G = 2) owns replicas 0 and 2 and
+# replica 2 is its second lane; the recorded replica is that lane (P = 2) or the
+# replica of the second thread of a site (P = 1).
+REP_FORMS = [(P, NP, PF) for P in (1, 2) for NP in (1, 2) for PF in (1, 2)]
+
+
+@pytest.mark.parametrize("name", ["bcc_body4", "fcc_l2_tri_zeeman"])
+@pytest.mark.parametrize("P,NP,PF", REP_FORMS, ids=[f"P{p}-NP{n}-PF{f}" for p, n, f in REP_FORMS])
+def test_rep_colour_every_instance_replays(gpu, name, P, NP, PF):
+    H, OH = build(name)
+    gH = scemc.GPUTiledHamiltonian(H)
+    R, step = 3, 0.6
+    seeds = [0xA11CE + 17 * i for i in range(R)]
+    betas = [1 / 0.05, 1 / 0.03, 1 / 0.08]
+    rec = 2 if P == 2 else 1
+    b = scemc.GPUBatch([gH], [R], [rand_cfg(H.n_sites, 40 + i) for i in range(R)], seeds, step)
+    b.set_betas(betas)
+    b.record_slot(0, rec)
+    n_or = 2 if H.site_has_l1.any() else 0
+    ties = att = 0
+    for sw in range(1, 4):
+        cfg = b.download()["configs"][rec].copy()
+        b.record(True)
+        b.run(1, or_per_metropolis=n_or, kernel=3, mode=1 + 2 * (sw == 3), proposals=1 + (sw % 2),
+              rep_replicas=P, rep_threads_per_item=NP, rep_prefetch=PF)
+        t, a, _ = check_pass(OH, cfg, b.fetch_record(-1), betas[rec], "metro", seed=seeds[rec], sweep=sw, step=step)
+        ties, att = ties + t, att + a
+        for k in range(n_or):
+            t, a, _ = check_pass(OH, cfg, b.fetch_record(k), betas[rec], "or", seed=seeds[rec], sweep=sw, orpass=k)
+            ties, att = ties + t, att + a
+        post = b.download()
+        np.testing.assert_array_equal(post["configs"][rec], cfg)
+        E_or = OH.total_energy(post["configs"][rec])
+        assert abs(b.total_energy(rec) - E_or) <= 1e-10 * max(1.0, abs(E_or))
+        assert abs(post["energies"][rec] - E_or) <= 1e-5 * max(1.0, abs(E_or))
+    assert ties <= max(1, att // 100)
+
+
+@pytest.mark.parametrize("P,NP", [(1, 1), (1, 2), (2, 1), (2, 2)])
+def test_rep_prefetch_changes_no_arithmetic(gpu, P, NP):
+    """Prefetching the records and neighbour rows into L1 changes no arithmetic: the
+    two forms give bitwise equal chains, overrelaxation included."""
+    H, _ = build("fcc_l2_tri_zeeman")
+    gH = scemc.GPUTiledHamiltonian(H)
+    cfgs = [rand_cfg(H.n_sites, 60 + i) for i in range(3)]
+    outs = []
+    for PF in (1, 2):
+        b = scemc.GPUBatch([gH], [3], cfgs, [5, 6, 7], 0.6)
+        b.set_betas([1 / 0.05, 1 / 0.03, 1 / 0.08])
+        b.run(5, or_per_metropolis=1, kernel=3, mode=1, rep_replicas=P, rep_threads_per_item=NP, rep_prefetch=PF)
+        st = b.download()
+        outs.append((np.stack(st["configs"]), st["energies"].copy(), st["counters"].copy()))
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+    assert np.array_equal(outs[0][2], outs[1][2])
+
+
+def test_rep_forms_refuse_bad_values(gpu):
+    H, _ = build("bcc_body4")
+    b = scemc.GPUBatch([scemc.GPUTiledHamiltonian(H)], [2], [rand_cfg(H.n_sites, 1)] * 2, [1, 2], 0.6)
+    with pytest.raises(_lib.ScemcArgumentError):
+        b.run(1, kernel=3, mode=1, rep_threads_per_item=3)
+    with pytest.raises(_lib.ScemcArgumentError):
+        b.run(1, kernel=3, mode=1, rep_prefetch=-1)
+    with pytest.raises(_lib.ScemcArgumentError):
+        b.record_slot(0, 2)
+    with pytest.raises(_lib.ScemcArgumentError):
+        b.record_slot(1, 0)
+
+
+def test_fcc64_32_rungs_replays_at_full_size(gpu):
+    """The large frustrated configuration at its own size (fcc 64^3 x 4 sites, 32
+    rungs, kT geometric in [0.05, 2.0] meV), through the launch form the library
+    picks by itself: its colours fill many waves, so k_rep_colour runs with two
+    replicas per thread, one thread per item and no prefetch. Rung 0 (the first lane
+    of a thread) and rung 17 (the second lane of thread 1) are recorded over a
+    Metropolis and an overrelaxation pass and replayed through the FP64 oracle
+    (dE and the decisions at every site, the proposals at 3000 sampled sites)."""
+    w = models.config5_fcc(n=64, replicas=32)
+    H = w.hamiltonians()[0]
+    OH = O.OracleHamiltonian(4, w.terms, (64, 64, 64), magmoms=w.magmoms, field=w.field)
+    gH = scemc.GPUTiledHamiltonian(H)
+    R, step = 32, 0.6
+    seeds = [0x5EED0 + 3 * r for r in range(R)]
+    betas = 1.0 / w.kts
+    base = rand_cfg(H.n_sites, 77)
+    cfgs = [np.roll(base, 7 * r, axis=0) for r in range(R)]
+    b = scemc.GPUBatch([gH], [R], cfgs, seeds, step)
+    b.set_betas(betas)
+    ties = att = 0
+    for sw, rec in ((1, 0), (2, 17)):
+        b.record_slot(0, rec)
+        cfg = b.download()["configs"][rec].copy()
+        b.record(True)
+        b.run(1, or_per_metropolis=1, kernel=3, mode=1)
+        t, a, _ = check_pass(OH, cfg, b.fetch_record(-1), betas[rec], "metro", seed=seeds[rec], sweep=sw,
+                             step=step, sample=3000)
+        ties, att = ties + t, att + a
+        t, a, _ = check_pass(OH, cfg, b.fetch_record(0), betas[rec], "or", seed=seeds[rec], sweep=sw, orpass=0,
+                             sample=3000)
+        ties, att = ties + t, att + a
+        np.testing.assert_array_equal(b.download()["configs"][rec], cfg)
+        E_or = OH.total_energy(cfg)
+        assert abs(b.total_energy(rec) - E_or) <= 1e-10 * max(1.0, abs(E_or))
+    assert att > 3 * H.n_sites
+    assert ties <= max(1, att // 100)
+
+
+def test_step_adaptation_follows_the_oracle(gpu):
+    """Device step adaptation (k_tail) against the oracle's _adapt_step! law
+    (updates.jl:296-305): every adapt_interval sweeps of a thermalisation phase, the
+    step of each rung becomes clamp(step exp((a - target) / 2), 1e-3, pi) with a the
+    Metropolis acceptance of that window. The windows are read back from the counters
+    and the whole per-rung step trajectory is recomputed by the oracle."""
+    H, _ = build("bcc_l2_plaq_zeeman")
+    gH = scemc.GPUTiledHamiltonian(H)
+    R, interval, target = 4, 10, 0.5
+    kts = np.array([0.02, 0.2, 2.0, 20.0]) * 1e-3  # from near-frozen to hot: the step shrinks and grows
+    steps0 = np.array([0.6, 0.6, 2.0, 3.0])
+    b = scemc.GPUBatch([gH], [R], [rand_cfg(H.n_sites, 90 + r) for r in range(R)], [11, 12, 13, 14], steps0)
+    b.set_betas(1.0 / kts)
+    expect = steps0.copy()
+    hit_clamp = False
+    for win in range(12):
+        before = b.download()["counters"].copy()
+        b.run(interval, adapt_interval=interval, adapt_target=target, phase_done=win * interval,
+              phase_total=12 * interval, kernel=1, mode=2)
+        st = b.download()
+        d = st["counters"] - before
+        for r in range(R):
+            expect[r] = O.adapt_step(expect[r], d[r, 0], d[r, 1], target)
+            hit_clamp |= expect[r] in (1e-3, math.pi)
+        np.testing.assert_allclose(st["steps"], expect, rtol=1e-14, atol=0)
+    assert hit_clamp or np.ptp(expect) > 0.5
 
 
 def test_fast_kernel_is_launch_shape_independent(gpu):
@@ -389,7 +533,7 @@ def test_guards(gpu):
     bad = np.full((H.n_sites, 3), np.nan)
     with pytest.raises(scemc.ScemcError):
         scemc.GPUChainState(gH, bad, seed=1, energy=0.0)
-    # lmax > 6 refused at table upload (gpu_hamiltonian.jl:439-440)
+    # lmax > 6 refused at table upload (gpu_hamiltonian.jl:67-68)
     f = np.zeros((15, 3))
     f[0, 0] = 1.0
     H7 = scemc.TiledHamiltonian(1, [scemc.MultipoleTerm(1.0, [1, 1], [(0, 0, 0), (1, 0, 0)], [7, 1], f)],

@@ -316,6 +316,17 @@ def test_swap_rule_sign():
     assert not O.swap_accepts(0.1, 0.2, -2.0, -1.0, w * 1.001)
 
 
+def test_adapt_step_law():
+    """_adapt_step! (updates.jl:296-305): step <- clamp(step exp((a - target) / 2), 1e-3,
+    pi) with a the window's Metropolis acceptance; no attempts, no change."""
+    assert O.adapt_step(0.6, 50, 100, 0.5) == 0.6
+    assert O.adapt_step(0.6, 100, 100, 0.5) == pytest.approx(0.6 * math.exp(0.25), rel=1e-15)
+    assert O.adapt_step(0.6, 10, 100, 0.3) == pytest.approx(0.6 * math.exp(-0.1), rel=1e-15)
+    assert O.adapt_step(3.1, 100, 100, 0.5) == math.pi
+    assert O.adapt_step(1.1e-3, 0, 100, 0.5) == 1e-3
+    assert O.adapt_step(0.6, 0, 0, 0.5) == 0.6
+
+
 def test_logbinner_tau_of_ar1():
     rng = np.random.default_rng(1)
     rho, n = 0.8, 1 << 17
