@@ -194,7 +194,10 @@ typedef struct scemc_run_params {
   int64_t phase_total;
   int32_t kernel;     /* 0 = auto, 1 = generic record walk, 2 = row-parallel fast kernel (one warp per
                          item), 3 = replica-parallel kernel (one thread per item; per-colour launches,
-                         mode 1 or 3) */
+                         mode 1 or 3), 4 = chain-resident cluster kernel (one thread-block cluster per
+                         replica slot holds the replica's spins in shared memory; the row-parallel
+                         arithmetic, bit for bit; one launch per compound sweep, mode 1 or 3; needs
+                         n_sites x 16 bytes plus scratch within one block's shared memory) */
   int32_t proposals;  /* 0 = auto, 1 = precompute a pass's Metropolis proposals, 2 = inline, 3 = learned
                          network (scemc_batch_set_learned; kernels 2 or 3, per-colour modes 1 or 3) */
   int32_t rep_replicas; /* kernel 3: replicas per thread, 1 or 2; 0 = per colour launch, 1 when its
@@ -341,6 +344,13 @@ int32_t scemc_batch_fetch_record(const scemc_batch* b, int32_t pass, float* prop
 int32_t scemc_color_sites(int32_t n_sites, const int32_t* site_ptr, const int32_t* site_inst,
                           const int32_t* inst_ptr, const int32_t* inst_sites, const uint8_t* site_active,
                           int32_t* colors_out, int32_t* n_colors);
+
+/* L2 read bandwidth (GB/s) of a `bytes`-sized device buffer (1 to 96 MiB, small
+ * enough to stay in the 126 MB L2) read `reps` times in one launch through L2-only
+ * loads; best of five timed launches on the current device. A measurement helper for
+ * the roofline of sweeps whose working set fits in L2 (no counterpart in the
+ * reference). */
+int32_t scemc_l2_probe(int64_t bytes, int32_t reps, double* gbs);
 
 /* Failure-detection self test: runs the persistent kernel's grid barrier with one
  * block that never arrives, bounded by limit_ns; returns SCEMC_ERR_TIMEOUT when the

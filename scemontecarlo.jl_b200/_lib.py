@@ -122,6 +122,7 @@ SIGNATURES = [
     ("scemc_batch_fetch_record", C.c_int32, [C.c_void_p, C.c_int32, F32P, F64P, F32P, U8P]),
     ("scemc_color_sites", C.c_int32, [C.c_int32, I32P, I32P, I32P, I32P, U8P, I32P, I32P]),
     ("scemc_selftest_barrier_timeout", C.c_int32, [C.c_int64]),
+    ("scemc_l2_probe", C.c_int32, [C.c_int64, C.c_int32, F64P]),
     ("scemc_total_energy_static", C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
 ]
 

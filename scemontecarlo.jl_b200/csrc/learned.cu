@@ -71,7 +71,8 @@ struct GemmArgs {
 
 constexpr int kKC = 64;  // K columns staged per chunk
 
-__device__ __forceinline__ float silu_f(float z) { return z / (1.0f + __expf(-z)); }
+// the sweep's fused kernel uses the same form (fast division; 0 for z below about -87)
+__device__ __forceinline__ float silu_f(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 __device__ __forceinline__ float dsilu_f(float z) {
   const float s = 1.0f / (1.0f + __expf(-z));
   return s * (1.0f + z * (1.0f - s));

@@ -34,6 +34,7 @@
 #include "umma.cuh"
 #include "vmf.cuh"
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -581,6 +582,20 @@ __global__ void __launch_bounds__(256) k_sweep_persistent(SweepArgs a) {
   flush_block(a, s_dE, s_cnt);
 }
 
+// L2 read-bandwidth probe: each block reads a contiguous share of buf, `reps` times,
+// with L2-only loads; the sum keeps the loads alive.
+__global__ void __launch_bounds__(256) k_l2_probe(const float4* __restrict__ buf, int64_t n4, int reps, float* sink) {
+  const int64_t per = (n4 + gridDim.x - 1) / gridDim.x;
+  const int64_t i0 = (int64_t)blockIdx.x * per, i1 = i0 + per < n4 ? i0 + per : n4;
+  float acc = 0.0f;
+  for (int k = 0; k < reps; ++k)
+    for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+      const float4 v = __ldcg(buf + i);
+      acc += (v.x + v.y) + (v.z + v.w);
+    }
+  if (acc == 1234.5f) sink[blockIdx.x] = acc;  // never true for a zeroed buffer; the loads stay
+}
+
 // Barrier self-test: nblocks_expected = gridDim.x + 1 can never be reached.
 __global__ void k_barrier_selftest(GridSync* gs, long long limit_ns) {
   grid_barrier(gs, 0ull, 0, gridDim.x + 1, limit_ns);
@@ -681,6 +696,158 @@ __device__ void make_proposals(const SweepArgs& a) {
   }
 }
 
+// The coefficient rows of one item from its records (rb) and its neighbours' Z rows
+// (zb): row lane `row` sums its W rows over the records of slice `slice`; the
+// slices are added with a fixed butterfly, so every lane of a row ends with c_row.
+template <int NR, int G, int S>
+__device__ __forceinline__ float fast_walk(const uint2* rb, const float* zb, const float* __restrict__ ft,
+                                           int n_pair, int n_trip, int n_quad, int n_one, int row, int slice) {
+  float acc = 0.0f, acc2 = 0.0f;
+  // pairs: each row lane dots its W row with the neighbour's Z row
+  if (row < NR) {
+#pragma unroll 4
+    for (int j = slice; j < n_pair; j += S) {
+      const uint2 fr = rb[j];
+      const float* z = zb + (fr.y & 0xffu) * NR;
+      const float* w = ft + (fr.x & kOffMask) + row * NR;
+      if (NR == 8) {
+        const float4 w0 = __ldg(reinterpret_cast<const float4*>(w));
+        const float4 w1 = __ldg(reinterpret_cast<const float4*>(w) + 1);
+        const float4 z0 = *reinterpret_cast<const float4*>(z);
+        const float4 z1 = *reinterpret_cast<const float4*>(z + 4);
+        acc = fmaf(w0.x, z0.x, acc);
+        acc2 = fmaf(w0.y, z0.y, acc2);
+        acc = fmaf(w0.z, z0.z, acc);
+        acc2 = fmaf(w0.w, z0.w, acc2);
+        acc = fmaf(w1.x, z1.x, acc);
+        acc2 = fmaf(w1.y, z1.y, acc2);
+        acc = fmaf(w1.z, z1.z, acc);
+        acc2 = fmaf(w1.w, z1.w, acc2);
+      } else {
+#pragma unroll
+        for (int m = 0; m < NR; ++m) acc = fmaf(__ldg(w + m), z[m], acc);
+      }
+    }
+  }
+  // l = 1 triplets and quads: rows 1..3 only
+  if (row < 3) {
+    for (int j = n_pair + slice; j < n_pair + n_trip; j += S) {
+      const uint2 fr = rb[j];
+      const float* z1 = zb + (fr.y & 0xffu) * NR;
+      const float* z2 = zb + ((fr.y >> 8) & 0xffu) * NR;
+      const float4* w4 = reinterpret_cast<const float4*>(ft + (fr.x & kOffMask) + row * 12);
+      const float4 a0 = __ldg(w4), a1 = __ldg(w4 + 1), a2 = __ldg(w4 + 2);
+      const float w[9] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a2.x};
+#pragma unroll
+      for (int p = 0; p < 3; ++p) {
+        const float t = fmaf(w[p * 3 + 0], z2[0], fmaf(w[p * 3 + 1], z2[1], w[p * 3 + 2] * z2[2]));
+        acc = fmaf(z1[p], t, acc);
+      }
+    }
+    for (int j = n_pair + n_trip + slice; j < n_pair + n_trip + n_quad; j += S) {
+      const uint2 fr = rb[j];
+      const float* z1 = zb + (fr.y & 0xffu) * NR;
+      const float* z2 = zb + ((fr.y >> 8) & 0xffu) * NR;
+      const float* z3 = zb + ((fr.y >> 16) & 0xffu) * NR;
+      const float4* w4 = reinterpret_cast<const float4*>(ft + (fr.x & kOffMask) + row * 28);
+      float w[28];
+#pragma unroll
+      for (int k = 0; k < 7; ++k) {
+        const float4 v = __ldg(w4 + k);
+        w[4 * k] = v.x, w[4 * k + 1] = v.y, w[4 * k + 2] = v.z, w[4 * k + 3] = v.w;
+      }
+      const float z3a = z3[0], z3b = z3[1], z3c = z3[2];
+#pragma unroll
+      for (int p = 0; p < 3; ++p) {
+        float t2 = 0.0f;
+#pragma unroll
+        for (int qq = 0; qq < 3; ++qq) {
+          const int o = (p * 3 + qq) * 3;
+          const float t3 = fmaf(w[o], z3a, fmaf(w[o + 1], z3b, w[o + 2] * z3c));
+          t2 = fmaf(z2[qq], t3, t2);
+        }
+        acc = fmaf(z1[p], t2, acc);
+      }
+    }
+  }
+  if (n_one && slice == 0 && row < NR) {
+    const uint2 fr = rb[n_pair + n_trip + n_quad];
+    acc += __ldg(ft + (fr.x & kOffMask) + row);
+  }
+  acc += acc2;
+#pragma unroll
+  for (int o = G; o < 32; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  return acc;
+}
+
+struct FastMove {
+  float px, py, pz, dE;
+  double u;
+  bool attempted, acc_ok;
+};
+
+// The move of one item from its coefficient rows (acc, one row per row lane): the
+// proposal (Metropolis: precomputed or drawn from the keyed stream; overrelaxation:
+// reflection about the l = 1 field h = (c4, c2, c3)), dE = sum_t c_t (znew_t - zold_t)
+// summed over the row lanes with a fixed butterfly, and the decision (Metropolis, or
+// Metropolis-Hastings with the learned density ratio lq). Every lane gets the result.
+template <int NR, int G>
+__device__ __forceinline__ FastMove fast_decide(float acc, float4 e, int row, int pass, bool have_prop, float4 p4,
+                                                double u_pre, bool mh, double lq, double beta,
+                                                unsigned long long seed, double step, uint32_t site1,
+                                                uint32_t sweep1) {
+  const bool do_or = pass >= 0;
+  float px, py, pz;
+  double u;
+  bool attempted = true;
+  if (!do_or) {
+    if (have_prop) {
+      px = p4.x, py = p4.y, pz = p4.z;
+      u = u_pre;
+    } else {
+      u = keyed_proposal(seed, site1, sweep1, e.x, e.y, e.z, step, px, py, pz);
+    }
+  } else {
+    // reflection about h = (c4, c2, c3): rows 3, 1, 2 live in lanes 2, 0, 1
+    const double h0 = __shfl_sync(0xffffffffu, acc, 2);
+    const double h1 = __shfl_sync(0xffffffffu, acc, 0);
+    const double h2 = __shfl_sync(0xffffffffu, acc, 1);
+    const double hn = sqrt((h0 * h0 + h1 * h1) + h2 * h2);
+    if (hn < 1e-12) {
+      attempted = false;
+      px = e.x, py = e.y, pz = e.z;
+    } else {
+      const double a0 = h0 / hn, a1 = h1 / hn, a2 = h2 / hn;
+      const double d2 = 2.0 * (((double)e.x * a0 + (double)e.y * a1) + (double)e.z * a2);
+      const double r0 = d2 * a0 - e.x, r1 = d2 * a1 - e.y, r2 = d2 * a2 - e.z;
+      const double rn = sqrt((r0 * r0 + r1 * r1) + r2 * r2);
+      px = (float)(r0 / rn);
+      py = (float)(r1 / rn);
+      pz = (float)(r2 / rn);
+    }
+    const Blk bk = philox_block(seed, site1, sweep1, (uint32_t)pass, kTagOR);
+    u = philox_uniform(bk.w0, bk.w1);
+  }
+  float zo[NR], zn[NR];
+  zrow_nr<NR>(e.x, e.y, e.z, zo);
+  zrow_nr<NR>(px, py, pz, zn);
+  float term = 0.0f;
+  if (row < NR && acc != 0.0f) term = acc * (pick<NR>(zn, row) - pick<NR>(zo, row));
+#pragma unroll
+  for (int o = G / 2; o >= 1; o >>= 1) term += __shfl_xor_sync(0xffffffffu, term, o);
+  const float dE = attempted ? term : 0.0f;
+  bool acc_ok;
+  if (!do_or && mh) {  // Metropolis-Hastings with the learned proposal's density ratio
+    const double la = -beta * (double)dE + lq;
+    acc_ok = la >= 0.0 || u < exp(la);
+  } else {
+    acc_ok = attempted && (dE <= 0.0f || u < exp(-beta * (double)dE));
+  }
+  FastMove m;
+  m.px = px, m.py = py, m.pz = pz, m.dE = dE, m.u = u, m.attempted = attempted, m.acc_ok = acc_ok;
+  return m;
+}
+
 template <int LMAX, bool PERSIST>
 __device__ void fast_colour(const SweepArgs& a, int col, unsigned long long* s_dE, unsigned int* s_cnt,
                             float* zsm, FastPre& pre, int next_col) {
@@ -761,129 +928,14 @@ __device__ void fast_colour(const SweepArgs& a, int col, unsigned long long* s_d
       }
     }
     __syncwarp();
-    float acc = 0.0f, acc2 = 0.0f;
-    // pairs: each row lane dots its W row with the neighbour's Z row
-    if (row < NR) {
-#pragma unroll 4
-      for (int j = slice; j < n_pair; j += S) {
-        const uint2 fr = rb[j];
-        const float* z = zb + (fr.y & 0xffu) * NR;
-        const float* w = L.ftensor + (fr.x & kOffMask) + row * NR;
-        if (NR == 8) {
-          const float4 w0 = __ldg(reinterpret_cast<const float4*>(w));
-          const float4 w1 = __ldg(reinterpret_cast<const float4*>(w) + 1);
-          const float4 z0 = *reinterpret_cast<const float4*>(z);
-          const float4 z1 = *reinterpret_cast<const float4*>(z + 4);
-          acc = fmaf(w0.x, z0.x, acc);
-          acc2 = fmaf(w0.y, z0.y, acc2);
-          acc = fmaf(w0.z, z0.z, acc);
-          acc2 = fmaf(w0.w, z0.w, acc2);
-          acc = fmaf(w1.x, z1.x, acc);
-          acc2 = fmaf(w1.y, z1.y, acc2);
-          acc = fmaf(w1.z, z1.z, acc);
-          acc2 = fmaf(w1.w, z1.w, acc2);
-        } else {
-#pragma unroll
-          for (int m = 0; m < NR; ++m) acc = fmaf(__ldg(w + m), z[m], acc);
-        }
-      }
-    }
-    // l = 1 triplets and quads: rows 1..3 only
-    if (row < 3) {
-      for (int j = n_pair + slice; j < n_pair + n_trip; j += S) {
-        const uint2 fr = rb[j];
-        const float* z1 = zb + (fr.y & 0xffu) * NR;
-        const float* z2 = zb + ((fr.y >> 8) & 0xffu) * NR;
-        const float4* w4 = reinterpret_cast<const float4*>(L.ftensor + (fr.x & kOffMask) + row * 12);
-        const float4 a0 = __ldg(w4), a1 = __ldg(w4 + 1), a2 = __ldg(w4 + 2);
-        const float w[9] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a2.x};
-#pragma unroll
-        for (int p = 0; p < 3; ++p) {
-          const float t = fmaf(w[p * 3 + 0], z2[0], fmaf(w[p * 3 + 1], z2[1], w[p * 3 + 2] * z2[2]));
-          acc = fmaf(z1[p], t, acc);
-        }
-      }
-      for (int j = n_pair + n_trip + slice; j < n_pair + n_trip + n_quad; j += S) {
-        const uint2 fr = rb[j];
-        const float* z1 = zb + (fr.y & 0xffu) * NR;
-        const float* z2 = zb + ((fr.y >> 8) & 0xffu) * NR;
-        const float* z3 = zb + ((fr.y >> 16) & 0xffu) * NR;
-        const float4* w4 = reinterpret_cast<const float4*>(L.ftensor + (fr.x & kOffMask) + row * 28);
-        float w[28];
-#pragma unroll
-        for (int k = 0; k < 7; ++k) {
-          const float4 v = __ldg(w4 + k);
-          w[4 * k] = v.x, w[4 * k + 1] = v.y, w[4 * k + 2] = v.z, w[4 * k + 3] = v.w;
-        }
-        const float z3a = z3[0], z3b = z3[1], z3c = z3[2];
-#pragma unroll
-        for (int p = 0; p < 3; ++p) {
-          float t2 = 0.0f;
-#pragma unroll
-          for (int qq = 0; qq < 3; ++qq) {
-            const int o = (p * 3 + qq) * 3;
-            const float t3 = fmaf(w[o], z3a, fmaf(w[o + 1], z3b, w[o + 2] * z3c));
-            t2 = fmaf(z2[qq], t3, t2);
-          }
-          acc = fmaf(z1[p], t2, acc);
-        }
-      }
-    }
-    if (n_one && slice == 0 && row < NR) {
-      const uint2 fr = rb[n_pair + n_trip + n_quad];
-      acc += __ldg(L.ftensor + (fr.x & kOffMask) + row);
-    }
-    acc += acc2;
-#pragma unroll
-    for (int o = G; o < 32; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    const float acc = fast_walk<NR, G, S>(rb, zb, L.ftensor, n_pair, n_trip, n_quad, n_one, row, slice);
     __syncwarp();  // rb / zb are rewritten for the next item
-    const double beta = p_beta[slot];
-    float px, py, pz;
-    double u;
-    bool attempted = true;
-    if (!do_or) {
-      if (a.prop != nullptr) {
-        px = p4.x, py = p4.y, pz = p4.z;
-        u = u_pre;
-      } else {
-        u = keyed_proposal(p_seed[slot], (uint32_t)(s + 1), a.st->sweep + 1u, e.x, e.y, e.z, p_step[slot], px, py, pz);
-      }
-    } else {
-      // reflection about h = (c4, c2, c3): rows 3, 1, 2 live in lanes 2, 0, 1
-      const double h0 = __shfl_sync(0xffffffffu, acc, 2);
-      const double h1 = __shfl_sync(0xffffffffu, acc, 0);
-      const double h2 = __shfl_sync(0xffffffffu, acc, 1);
-      const double hn = sqrt((h0 * h0 + h1 * h1) + h2 * h2);
-      if (hn < 1e-12) {
-        attempted = false;
-        px = e.x, py = e.y, pz = e.z;
-      } else {
-        const double a0 = h0 / hn, a1 = h1 / hn, a2 = h2 / hn;
-        const double d2 = 2.0 * (((double)e.x * a0 + (double)e.y * a1) + (double)e.z * a2);
-        const double r0 = d2 * a0 - e.x, r1 = d2 * a1 - e.y, r2 = d2 * a2 - e.z;
-        const double rn = sqrt((r0 * r0 + r1 * r1) + r2 * r2);
-        px = (float)(r0 / rn);
-        py = (float)(r1 / rn);
-        pz = (float)(r2 / rn);
-      }
-      const Blk bk = philox_block(p_seed[slot], (uint32_t)(s + 1), a.st->sweep + 1u, (uint32_t)a.pass, kTagOR);
-      u = philox_uniform(bk.w0, bk.w1);
-    }
-    float zo[NR], zn[NR];
-    zrow_nr<NR>(e.x, e.y, e.z, zo);
-    zrow_nr<NR>(px, py, pz, zn);
-    float term = 0.0f;
-    if (row < NR && acc != 0.0f) term = acc * (pick<NR>(zn, row) - pick<NR>(zo, row));
-#pragma unroll
-    for (int o = G / 2; o >= 1; o >>= 1) term += __shfl_xor_sync(0xffffffffu, term, o);
-    const float dE = attempted ? term : 0.0f;
-    bool acc_ok;
-    if (!do_or && a.lqr != nullptr) {  // Metropolis-Hastings with the learned proposal's density ratio
-      const double la = -beta * (double)dE + lq;
-      acc_ok = la >= 0.0 || u < exp(la);
-    } else {
-      acc_ok = attempted && (dE <= 0.0f || u < exp(-beta * (double)dE));
-    }
+    const FastMove mv = fast_decide<NR, G>(acc, e, row, a.pass, !do_or && a.prop != nullptr, p4, u_pre,
+                                           a.lqr != nullptr, lq, p_beta[slot], p_seed[slot], p_step[slot],
+                                           (uint32_t)(s + 1), a.st->sweep + 1u);
+    const float px = mv.px, py = mv.py, pz = mv.pz, dE = mv.dE;
+    const double u = mv.u;
+    const bool attempted = mv.attempted, acc_ok = mv.acc_ok;
     if (lane != 0) continue;
     if (acc_ok) {
       a.spins[L.spin_off + (int64_t)s * R + r] = make_float4(px, py, pz, 0.0f);
@@ -983,6 +1035,165 @@ __global__ void SCEMC_FAST_BOUNDS k_fast_persistent(SweepArgs a) {
 }
 
 __global__ void __launch_bounds__(256) k_proposals(SweepArgs a) { make_proposals<false>(a); }
+
+// ---------------------------------------------------------------------------
+// Chain-resident cluster sweep (row-parallel arithmetic, one launch per compound
+// sweep). For chains small enough that one replica's spins fit in shared memory
+// (16 bytes a site), a thread-block cluster owns one replica slot and every CTA of
+// the cluster holds a full copy of that replica's spins. Each colour is split over
+// the cluster's warps (one warp per site, the row-parallel record walk of
+// fast_walk / fast_decide reading the neighbours from the local copy); an accepted
+// spin is written into every CTA's copy through distributed shared memory, and the
+// hardware cluster barrier separates the colours, so a colour costs a barrier
+// instead of a kernel boundary and its neighbour reads never leave the SM. The
+// cluster's CTAs are co-scheduled by construction, and every thread of every CTA
+// takes the same barriers, so no wait can be left hanging. The chain's spins are
+// loaded at the start and written back at the end of the compound sweep (one
+// Metropolis pass, then n_or overrelaxation passes); arithmetic and decisions are
+// those of k_fast_colour, bit for bit.
+// ---------------------------------------------------------------------------
+constexpr int kClusterThreads = 512;
+
+__host__ __device__ __forceinline__ size_t cluster_smem_bytes(int n_sites, int dmax, int rmax, int nr) {
+  return (size_t)n_sites * 16 + (size_t)(kClusterThreads / 32) * fast_group_floats(dmax, rmax, nr) * 4;
+}
+
+template <int LMAX>
+__global__ void __launch_bounds__(kClusterThreads, 1) k_chain_cluster(SweepArgs a, int n_or) {
+  namespace cg = cooperative_groups;
+  constexpr int NR = (LMAX + 1) * (LMAX + 1) - 1;
+  constexpr int G = NR <= 4 ? 4 : 8;
+  constexpr int S = 32 / G;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int crank = (int)cluster.block_rank();
+  const int csize = (int)cluster.num_blocks();
+  const int slot = blockIdx.x / csize;  // one cluster per replica slot
+  int li = 0;
+  while (li + 1 < a.n_lat && slot >= a.lat[li + 1].slot0) ++li;
+  const DevLattice& L = a.lat[li];
+  const int R = L.R, r = slot - L.slot0, ns = L.n_sites;
+  const int rung = a.rung_of_slot[slot];
+  const double beta = a.beta[rung], step = a.step[rung];
+  const unsigned long long seed = a.seed[rung];
+  extern __shared__ __align__(16) float zsm[];
+  float4* sspin = reinterpret_cast<float4*>(zsm);
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int row = lane % G, slice = lane / G;
+  const int wpb = blockDim.x >> 5;
+  const size_t per_warp = fast_group_floats(a.dmax, a.rmax, NR);
+  float* wbase = zsm + (size_t)ns * 4 + (size_t)wib * per_warp;
+  uint2* rb = reinterpret_cast<uint2*>(wbase);
+  int* nbid = reinterpret_cast<int*>(wbase + fast_rec_floats(a.rmax));
+  float* zb = wbase + fast_rec_floats(a.rmax) + fast_nbid_words(a.dmax);
+  __shared__ unsigned long long s_dE;
+  __shared__ unsigned int s_cnt[3];
+  if (threadIdx.x == 0) s_dE = 0ull, s_cnt[0] = s_cnt[1] = s_cnt[2] = 0u;
+  float4* __restrict__ gsp = a.spins + L.spin_off;
+  for (int s = threadIdx.x; s < ns; s += blockDim.x) sspin[s] = __ldcg(gsp + (int64_t)s * R + r);
+  cluster.sync();  // every copy is complete before any CTA writes into another's
+  const uint32_t sweep1 = a.st->sweep + 1u;
+  // The static tables of a warp's first item of a colour (descriptor, records,
+  // neighbour ids) are read before the barrier that ends the previous colour, so
+  // their latency overlaps the wait; the spins are read after it.
+  int pre_q = -1;
+  int4 pre_dsc = make_int4(0, 0, 0, 0);
+  auto load_tables = [&](int4 dsc) {
+    const uint32_t cnt = (uint32_t)dsc.w;
+    const int nrec = (int)(cnt & 0xffu) + (int)((cnt >> 8) & 0xffu) + (int)((cnt >> 16) & 0xffu) + ((dsc.x >> 31) & 1);
+    for (int k = lane; k < nrec; k += 32) rb[k] = __ldg(L.frec + dsc.z + k);
+    for (int k = lane; k < (int)(cnt >> 24); k += 32) nbid[k] = __ldg(L.nb_list + dsc.y + k);
+  };
+  auto prefetch = [&](int pass, int col) {
+    pre_q = -1;
+    if (col >= a.max_colors) return;
+    const int32_t* seg_c = a.seg + (size_t)col * (a.n_lat + 1);
+    const int q = crank * wpb + wib;
+    if (q >= (seg_c[li + 1] - seg_c[li]) / R) return;
+    pre_dsc = __ldg(L.idesc + __ldg(L.color_ptr + col) + q);
+    if (pass >= 0 && !(pre_dsc.x & (1 << 30))) return;  // skipped by the overrelaxation pass
+    load_tables(pre_dsc);
+    pre_q = q;
+  };
+  prefetch(-1, 0);
+  for (int pass = -1; pass < n_or; ++pass) {
+    const bool do_or = pass >= 0;
+    for (int col = 0; col < a.max_colors; ++col) {
+      const int32_t* seg_c = a.seg + (size_t)col * (a.n_lat + 1);
+      const int nq = (seg_c[li + 1] - seg_c[li]) / R;
+      for (int q = crank * wpb + wib; q < nq; q += csize * wpb) {  // warp-uniform
+        const bool have = q == pre_q;
+        const int4 dsc = have ? pre_dsc : __ldg(L.idesc + __ldg(L.color_ptr + col) + q);
+        const int site = dsc.x & 0x3fffffff;
+        if (do_or && !(dsc.x & (1 << 30))) continue;  // no l = 1 channel
+        const float4 e = sspin[site];
+        float4 p4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        double u_pre = 0.0;
+        const bool have_prop = !do_or && a.prop != nullptr;
+        if (have_prop) {
+          const int idx = a.item_base[col] + seg_c[li] + q * R + r;
+          p4 = a.prop[idx];
+          u_pre = a.propu[idx];
+        }
+        const uint32_t cnt = (uint32_t)dsc.w;
+        const int nd = (int)(cnt >> 24);
+        const int n_pair = (int)(cnt & 0xffu), n_trip = (int)((cnt >> 8) & 0xffu), n_quad = (int)((cnt >> 16) & 0xffu);
+        const int n_one = (dsc.x >> 31) & 1;
+        if (!have) {
+          load_tables(dsc);
+          __syncwarp();
+        }
+        pre_q = -1;
+        for (int k = lane; k < nd; k += 32) {
+          const float4 v = sspin[nbid[k]];
+          zrow_nr<NR>(v.x, v.y, v.z, zb + k * NR);
+        }
+        __syncwarp();
+        const float acc = fast_walk<NR, G, S>(rb, zb, L.ftensor, n_pair, n_trip, n_quad, n_one, row, slice);
+        __syncwarp();  // rb / nbid / zb are rewritten for the next item
+        const FastMove mv = fast_decide<NR, G>(acc, e, row, pass, have_prop, p4, u_pre, false, 0.0, beta, seed, step,
+                                               (uint32_t)(site + 1), sweep1);
+        if (mv.acc_ok && lane < csize) {  // the new spin into every CTA's copy
+          float4* dst = cluster.map_shared_rank(sspin + site, (unsigned)lane);
+          *dst = make_float4(mv.px, mv.py, mv.pz, 0.0f);
+        }
+        if (lane != 0) continue;
+        if (mv.acc_ok) atomicAdd(&s_dE, (unsigned long long)llrint((double)mv.dE * kFixScale));
+        if (do_or) {
+          if (mv.attempted) atomicAdd(s_cnt + 2, 1u);
+          if (mv.acc_ok) atomicAdd(s_cnt + 1, 1u);
+        } else if (mv.acc_ok) {
+          atomicAdd(s_cnt + 0, 1u);
+        }
+        if (a.rec_prop != nullptr && li == a.rec_li && r == a.rec_r && pass + 1 < kRecPasses) {
+          const int64_t qq = (int64_t)(pass + 1) * a.rec_cap + site;
+          a.rec_prop[3 * qq + 0] = mv.px;
+          a.rec_prop[3 * qq + 1] = mv.py;
+          a.rec_prop[3 * qq + 2] = mv.pz;
+          a.rec_u[qq] = mv.u;
+          a.rec_dE[qq] = mv.dE;
+          a.rec_acc[qq] = (uint8_t)(mv.acc_ok ? 1 : (mv.attempted ? 0 : 2));
+        }
+      }
+      __syncwarp();
+      if (col + 1 < a.max_colors) prefetch(pass, col + 1);
+      else if (pass + 1 < n_or) prefetch(pass + 1, 0);
+      __syncwarp();
+      cluster.sync();  // this colour's spins are in every copy before the next colour reads them
+    }
+  }
+  // every copy is identical: each CTA writes back its share of the sites
+  const int per = (ns + csize - 1) / csize;
+  const int s0 = crank * per, s1 = min(ns, s0 + per);
+  for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) gsp[(int64_t)s * R + r] = sspin[s];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (s_dE) atomicAdd(a.dE_fix + slot, s_dE);
+    if (s_cnt[0]) atomicAdd(a.cnt + 4 * rung + 0, (unsigned long long)s_cnt[0]);
+    if (s_cnt[1]) atomicAdd(a.cnt + 4 * rung + 2, (unsigned long long)s_cnt[1]);
+    if (s_cnt[2]) atomicAdd(a.cnt + 4 * rung + 3, (unsigned long long)s_cnt[2]);
+  }
+}
+
 
 // ---------------------------------------------------------------------------
 // Replica-parallel sweep (same tables as the row-parallel kernel). A thread owns P
@@ -1368,6 +1579,11 @@ __device__ __forceinline__ void learned_layer(uint32_t tmem_d, const uint8_t* A,
 // in shared memory, and warpgroup 0 forms dE = sum_t c_t (z_t(new) - z_t(old)),
 // decides and writes the spin. Safe within one launch because no site of the colour
 // is a Hamiltonian neighbour or an environment site of another.
+// SiLU z / (1 + e^-z) with the fast division (the training path in learned.cu uses the
+// same form, so the sweep and the training forward agree): for z below about -87,
+// e^-z is infinite and the quotient is 0, the function's limit.
+__device__ __forceinline__ float silu_fast(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
+
 template <int LMAX, bool MH>
 __global__ void __launch_bounds__(256, 2) k_learned_fused(SweepArgs a, LearnedNet net, double* lqr) {
   constexpr int NR = (LMAX + 1) * (LMAX + 1) - 1;
@@ -1500,7 +1716,7 @@ __global__ void __launch_bounds__(256, 2) k_learned_fused(SweepArgs a, LearnedNe
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
         const float z = v[i] + sb[c0 + i];
-        h[i] = __float2bfloat16_rn(z / (1.0f + __expf(-z)));
+        h[i] = __float2bfloat16_rn(silu_fast(z));
       }
       *reinterpret_cast<uint4*>(sH + (c0 >> 6) * kChunkBytes + umma::kmajor_offset(row, c0 & 63, 64)) =
           *reinterpret_cast<const uint4*>(h);
@@ -1520,7 +1736,7 @@ __global__ void __launch_bounds__(256, 2) k_learned_fused(SweepArgs a, LearnedNe
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
         const float z = v[i] + sb[128 + c0 + i];
-        h[i] = __float2bfloat16_rn(z / (1.0f + __expf(-z)));
+        h[i] = __float2bfloat16_rn(silu_fast(z));
       }
       *reinterpret_cast<uint4*>(sH + (c0 >> 6) * kChunkBytes + umma::kmajor_offset(row, c0 & 63, 64)) =
           *reinterpret_cast<const uint4*>(h);
@@ -1607,8 +1823,11 @@ __global__ void __launch_bounds__(256, 2) k_learned_fused(SweepArgs a, LearnedNe
 
 // P = 2 at 80 registers (three 256-thread blocks per SM); P = 1 at 64 registers
 // (four blocks per SM).
+#ifndef SCEMC_REP_MINB_P2
+#define SCEMC_REP_MINB_P2 3
+#endif
 template <int LMAX, int P, int NP, bool PF>
-__global__ void __launch_bounds__(256, P == 1 ? 4 : 3) k_rep_colour(SweepArgs a) {
+__global__ void __launch_bounds__(256, P == 1 ? 4 : SCEMC_REP_MINB_P2) k_rep_colour(SweepArgs a) {
   extern __shared__ __align__(16) float zsm[];
   __shared__ unsigned long long s_dE[kMaxSlots];
   __shared__ unsigned int s_cnt[3 * kMaxSlots];
@@ -1938,6 +2157,9 @@ struct scemc_ensemble {
   float4* d_prop = nullptr;
   double* d_propu = nullptr;
   int coop_key[4] = {-1, -1, -1, -1};
+  // chain-resident cluster kernel: cluster size and dynamic shared memory (0 = not prepared)
+  int cluster_cs = 0;
+  size_t cluster_smem = 0;
   unsigned long long bar_base = 0;  // host mirror of GridSync::arrived after the enqueued launches
   int graph_passes_per_launch = 0;
   // autotuned launch form (used when mode, proposals, lanes are 0)
@@ -2352,14 +2574,23 @@ int32_t compile_tables(const scemc_tables_desc* d, scemc_tables* T) {
   if ((r = upload(T->allocs, rebase(d->inst_sites, d->n_inst_sites), &L.inst_sites))) return r;
   std::vector<int32_t> cp = rebase(d->color_ptr, d->n_colors + 1);
   if ((r = upload(T->allocs, cp, &L.color_ptr))) return r;
-  // Sites of a colour in sublattice order (stable): translation-equivalent sites share
-  // their coupling blocks, so the threads of one warp, which carry two neighbouring
-  // items of a colour, read the same block. The order inside a colour does not change
-  // any result (its sites are updated independently and keyed by site).
+  // Sites of a colour in tiles of SCEMC_ORDER_TILE_CELLS consecutive cells, and in
+  // sublattice order inside a tile (stable): translation-equivalent sites share their
+  // coupling blocks, so the threads of one warp, which carry two neighbouring items of
+  // a colour, read the same block, and the items in flight together gather from one
+  // region of the lattice. The order inside a colour does not change any result (its
+  // sites are updated independently and keyed by site; measured bitwise equal). Tiles
+  // of 4096 cells measured 3 % faster than one tile at fcc 48^3 x 32 rungs (13.78
+  // against 14.23 ms per compound sweep; site order 14.52).
   std::vector<int32_t> cs = rebase(d->color_sites, d->n_active);
+#ifndef SCEMC_ORDER_TILE_CELLS
+#define SCEMC_ORDER_TILE_CELLS 4096  // 0: one tile (the whole lattice)
+#endif
   for (int32_t c = 0; c < d->n_colors; ++c)
     std::stable_sort(cs.begin() + cp[c], cs.begin() + cp[c + 1], [&](int32_t x, int32_t y) {
-      return x % d->n_cell_atoms < y % d->n_cell_atoms;
+      const int32_t na = d->n_cell_atoms, tc = SCEMC_ORDER_TILE_CELLS;
+      if (tc > 0 && x / (na * tc) != y / (na * tc)) return x / (na * tc) < y / (na * tc);
+      return x % na < y % na;
     });
   if ((r = upload(T->allocs, cs, &L.color_sites))) return r;
   if ((r = upload(T->allocs, has_l1, &L.has_l1))) return r;
@@ -2787,6 +3018,7 @@ struct Launch {
   int rep_p = 0;            // replica-parallel kernel: replicas per thread (0 = per colour, by its size)
   int rep_np = 0;           // replica-parallel kernel: threads per item (0 = per colour, by its size)
   int rep_pf = 0;           // replica-parallel kernel: 1 prefetch, 2 no prefetch (0 = per colour, by its size)
+  bool cluster = false;     // chain-resident cluster kernel: one launch per compound sweep
 };
 
 using FastFn = void (*)(SweepArgs);
@@ -3205,6 +3437,123 @@ int32_t check_error(scemc_ensemble* E) {
   return SCEMC_OK;
 }
 
+// The chain-resident cluster kernel applies when the batch has the fast tables and
+// one replica's spins plus the per-warp scratch fit in one CTA's shared memory.
+int32_t cluster_fits(const scemc_ensemble* E) {
+  if (!E->fast)
+    return fail(SCEMC_ERR_ARG, "the cluster kernel (kernel 4) needs the fast tables (lmax 1 or 2 dense programs)");
+  int optin = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, E->device));
+  const int nr = fast_rows(E->lmax);
+  for (const scemc_tables* T : E->tabs)
+    if (cluster_smem_bytes(T->n_sites, std::max(E->dmax, 1), std::max(E->rmax, 1), nr) > (size_t)optin)
+      return fail(SCEMC_ERR_ARG, "the cluster kernel (kernel 4) needs one replica's spins (" +
+                                     std::to_string(T->n_sites) + " sites x 16 bytes) and its scratch in " +
+                                     std::to_string(optin) + " bytes of shared memory");
+  return SCEMC_OK;
+}
+
+// Cluster size of the chain-resident kernel: enough CTAs that a colour of one replica
+// gives every warp about one site, at most 16 (the non-portable limit), and a size
+// the device can co-schedule with this kernel's shared memory.
+int cluster_size(scemc_ensemble* E, size_t smem) {
+  const void* fn = E->lmax == 1 ? (const void*)k_chain_cluster<1> : (const void*)k_chain_cluster<2>;
+  int items = 1;
+  for (int c = 0; c < E->max_colors; ++c)
+    for (size_t li = 0; li < E->tabs.size(); ++li) {
+      const int32_t* sc = E->seg.data() + (size_t)c * (E->tabs.size() + 1);
+      items = std::max(items, (sc[li + 1] - sc[li]) / E->R[li]);
+    }
+  const int warps = kClusterThreads / 32;
+  int want = 1;
+  while (want < 16 && want * warps < items) want <<= 1;
+  for (int cs = want; cs >= 1; cs >>= 1) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)cs);
+    cfg.blockDim = dim3(kClusterThreads);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, fn, &cfg) == cudaSuccess && n > 0) return cs;
+    cudaGetLastError();
+  }
+  return 0;
+}
+
+// One compound sweep (Metropolis + n_or overrelaxation passes) of every replica slot
+// through the chain-resident cluster kernel: one cluster per slot.
+// Function attributes and cluster size of the chain-resident kernel (once per batch,
+// outside any stream capture).
+int32_t prepare_cluster(scemc_ensemble* E) {
+  if (E->cluster_cs > 0) return SCEMC_OK;
+  int32_t max_ns = 1;
+  for (const scemc_tables* T : E->tabs) max_ns = std::max(max_ns, T->n_sites);
+  const size_t smem = cluster_smem_bytes(max_ns, std::max(E->dmax, 1), std::max(E->rmax, 1), fast_rows(E->lmax));
+  const void* fn = E->lmax == 1 ? (const void*)k_chain_cluster<1> : (const void*)k_chain_cluster<2>;
+  CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  const int cs = cluster_size(E, smem);
+  if (cs < 1) return fail(SCEMC_ERR_CUDA, "no thread-block cluster of the chain-resident kernel fits the device");
+  E->cluster_cs = cs;
+  E->cluster_smem = smem;
+  return SCEMC_OK;
+}
+
+int32_t run_cluster_sweep(scemc_ensemble* E, int n_or, const Launch& Lc) {
+  SweepArgs a = make_args(E, -1);
+  a.dmax = std::max(E->dmax, 1);
+  a.rmax = std::max(E->rmax, 1);
+  a.item_base = E->d_item_base;
+  int32_t rc;
+  if (Lc.precompute) {
+    if ((rc = ensure_props(E))) return rc;
+    a.prop = E->d_prop;
+    a.propu = E->d_propu;
+  }
+  if ((rc = prepare_cluster(E))) return rc;
+  const int cs = E->cluster_cs;
+  const size_t smem = E->cluster_smem;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (E->profiling) {
+    ev0 = take_event(E);
+    ev1 = take_event(E);
+    CUDA_TRY(cudaEventRecord(ev0, E->stream));
+  }
+  if (a.prop) {
+    const int blocks = (int)std::min<int64_t>(sm_count(E->device) * 16, ((int64_t)E->item_base.back() + 255) / 256);
+    ++E->launches;
+    k_proposals<<<std::max(blocks, 1), 256, 0, E->stream>>>(a);
+    CUDA_TRY(cudaGetLastError());
+  }
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)(cs * E->n_slots));
+  cfg.blockDim = dim3(kClusterThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = E->stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)cs;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  ++E->launches;
+  if (E->lmax == 1) CUDA_TRY(cudaLaunchKernelEx(&cfg, k_chain_cluster<1>, a, n_or));
+  else CUDA_TRY(cudaLaunchKernelEx(&cfg, k_chain_cluster<2>, a, n_or));
+  if (E->profiling) {
+    CUDA_TRY(cudaEventRecord(ev1, E->stream));
+    E->ev_pending.emplace_back(ev0, ev1);
+    E->graph_passes_per_launch = 1 + n_or;
+  }
+  return SCEMC_OK;
+}
+
 int auto_lanes(const scemc_ensemble* E) {
   // Items per colour vs. ~16 resident warps per SM: give each item more lanes when
   // a colour class alone cannot fill the device.
@@ -3238,8 +3587,14 @@ int32_t resolve_launch(const scemc_ensemble* E, int lanes, int mode, int kernel,
   if (mode < 0 || mode > 4) return fail(SCEMC_ERR_ARG, "mode must be 0..4");
   if (mode == 4 && (!E->fast || kernel == 1 || kernel == 3 || proposals == 3))
     return fail(SCEMC_ERR_ARG, "the data-flow form (mode 4) runs the row-parallel kernel with plain proposals");
-  if (kernel < 0 || kernel > 3 || proposals < 0 || proposals > 3)
-    return fail(SCEMC_ERR_ARG, "kernel must be 0..3 and proposals 0..3");
+  if (kernel < 0 || kernel > 4 || proposals < 0 || proposals > 3)
+    return fail(SCEMC_ERR_ARG, "kernel must be 0..4 and proposals 0..3");
+  if (kernel == 4) {
+    int32_t rc;
+    if ((rc = cluster_fits(E))) return rc;
+    if (proposals == 3) return fail(SCEMC_ERR_ARG, "the cluster kernel (kernel 4) runs plain Metropolis proposals");
+    if (mode == 2 || mode == 4) return fail(SCEMC_ERR_ARG, "the cluster kernel (kernel 4) runs with mode 1 or 3");
+  }
   if (proposals == 3) {
     if (!E->mlp) return fail(SCEMC_ERR_ARG, "learned proposals need scemc_batch_set_learned first");
     if (!E->fast) return fail(SCEMC_ERR_ARG, "learned proposals need the fast tables (lmax 1 or 2 dense programs)");
@@ -3260,10 +3615,11 @@ int32_t resolve_launch(const scemc_ensemble* E, int lanes, int mode, int kernel,
   for (int r : E->R) min_r = std::min(min_r, r);
   const bool rep_auto = E->fast && mode != 2 && min_r >= 16 &&
                         (int64_t)max_colour_items(E) >= (int64_t)sm_count(E->device) * 256;
+  L.cluster = kernel == 4;
   L.rep = kernel == 3 || (kernel == 0 && rep_auto);
-  L.fast = !L.rep && (kernel == 2 || (kernel == 0 && E->fast));
+  L.fast = !L.rep && (kernel == 2 || kernel == 4 || (kernel == 0 && E->fast));
   L.learned = proposals == 3;
-  L.mode = mode == 0 ? ((L.rep || L.learned) ? 1 : 2) : mode;
+  L.mode = mode == 0 ? ((L.rep || L.learned || L.cluster) ? 1 : 2) : mode;
   if (L.mode == 3) {
     L.graph = true;
     L.mode = 1;
@@ -3277,6 +3633,8 @@ int32_t resolve_launch(const scemc_ensemble* E, int lanes, int mode, int kernel,
   L.G = lanes ? norm_lanes(lanes) : auto_lanes(E);
   if (L.learned) {
     L.precompute = false;
+  } else if (L.cluster) {  // precomputed by default: the keyed draw's FP64 trigonometry stays off the colour steps
+    L.precompute = proposals != 2;
   } else if (L.fast) {
     const int64_t groups = (int64_t)max_colour_items(E) * 32;
     L.precompute = proposals == 1 || (proposals == 0 && groups < (int64_t)sm_count(E->device) * 2048);
@@ -3291,6 +3649,7 @@ int32_t sweep_once(scemc_ensemble* E, int n_or, const Launch& L) {
   if (E->sweep_index >= 0x7ffffffell - 1)
     return fail(SCEMC_ERR_EXHAUSTED, "sweep_index exhausted the 32-bit RNG counter word");
   int32_t rc;
+  if (L.cluster) return run_cluster_sweep(E, n_or, L);
   if ((rc = run_pass(E, -1, L))) return rc;
   for (int k = 0; k < n_or; ++k)
     if ((rc = run_pass(E, k, L))) return rc;
@@ -3301,7 +3660,7 @@ int32_t sweep_once(scemc_ensemble* E, int n_or, const Launch& L) {
 // configuration, replayed every sweep). Every launch reads the sweep counter from
 // device memory and the tail advances it, so one capture serves all sweeps.
 int32_t sweep_graph(scemc_ensemble* E, int n_or, const Launch& L, cudaGraphExec_t* out, int64_t* n_launch) {
-  const int key[7] = {n_or, L.rep ? 2 : (L.fast ? 1 : 0), L.learned ? 2 : (L.precompute ? 1 : 0),
+  const int key[7] = {n_or, L.cluster ? 3 : (L.rep ? 2 : (L.fast ? 1 : 0)), L.learned ? 2 : (L.precompute ? 1 : 0),
                       L.fast ? 0 : (L.rep ? L.rep_p : L.G), E->recording ? 1 : 0, L.rep ? L.rep_np : 0,
                       L.rep ? L.rep_pf : 0};
   for (auto& g : E->graphs)
@@ -3315,6 +3674,8 @@ int32_t sweep_graph(scemc_ensemble* E, int n_or, const Launch& L, cudaGraphExec_
     if ((rc = ensure_props(E))) return rc;
   if (L.learned)
     if ((rc = prepare_learned(E))) return rc;
+  if (L.cluster)  // attributes and the cluster size are settled outside the capture
+    if ((rc = prepare_cluster(E))) return rc;
   if (L.fast) {  // attributes are set outside the capture
     int threads;
     size_t smem;
@@ -3666,6 +4027,8 @@ int32_t scemc_batch_autotune(scemc_batch* b, int32_t or_per_metropolis, int32_t 
       for (int q : {1, 2}) cands.push_back({m, q, 0, 2});
     cands.push_back({4, 2, 0, 2});
     for (int q : {1, 2}) cands.push_back({3, q, 0, 3});
+    if (cluster_fits(b) == SCEMC_OK)
+      for (int q : {1, 2}) cands.push_back({3, q, 0, 4});
   } else {
     for (int m : {2, 3})
       for (int g : {1, 4, 8, 32}) cands.push_back({m, 0, g, 1});
@@ -4035,6 +4398,44 @@ int32_t scemc_color_sites(int32_t n_sites, const int32_t* site_ptr, const int32_
     colors_out[s - 1] = c;
   }
   *n_colors = ncol;
+  return SCEMC_OK;
+}
+
+// L2 read bandwidth (GB/s) of a buffer small enough to stay in L2: every block reads
+// its share of the buffer `reps` times through L2 (ld.global.cg: L1 bypassed) in one
+// launch; the best of five timed launches after a warm-up. The roofline denominator
+// of sweeps whose working set fits in L2.
+int32_t scemc_l2_probe(int64_t bytes, int32_t reps, double* gbs) {
+  if (bytes < (1 << 20) || bytes > ((int64_t)96 << 20) || reps < 1 || !gbs)
+    return fail(SCEMC_ERR_ARG, "scemc_l2_probe: bytes in [1 MiB, 96 MiB], reps >= 1");
+  const int64_t n4 = bytes / 16;
+  float4* buf = nullptr;
+  float* sink = nullptr;
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  const int blocks = sm_count(dev) * 4;
+  CUDA_TRY(cudaMalloc(&buf, (size_t)n4 * 16));
+  CUDA_TRY(cudaMalloc(&sink, sizeof(float) * blocks));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e = cudaMemset(buf, 0, (size_t)n4 * 16);
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  float best = 1e30f;
+  for (int t = 0; t < 6 && e == cudaSuccess; ++t) {
+    cudaEventRecord(e0);
+    k_l2_probe<<<blocks, 256>>>(buf, n4, reps, sink);
+    cudaEventRecord(e1);
+    e = cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (t > 0) best = std::min(best, ms);
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(buf);
+  cudaFree(sink);
+  if (e != cudaSuccess) return fail(SCEMC_ERR_CUDA, std::string("scemc_l2_probe: ") + cudaGetErrorString(e));
+  *gbs = (double)n4 * 16.0 * reps / (best * 1e-3) / 1e9;
   return SCEMC_OK;
 }
 

@@ -137,7 +137,8 @@ REPLAY_CASES = [(m, 4, 2, 1, 0) for m in MODELS] + [(m, 0, 2, 0, 1) for m in FAS
     ("bcc_l2_plaq_zeeman", 0, 3, 0, 1), ("fcc_l2_tri_zeeman", 0, 3, 0, 2), ("biquadratic", 4, 3, 1, 0),
     ("mixed", 8, 3, 0, 0),
 ] + [(m, 0, 1, 3, 2) for m in FAST] + [("bcc_l2_plaq_zeeman", 0, 3, 3, 1), ("fcc_l2_tri_zeeman", 0, 3, 3, 2)] + [
-    (m, 0, 4, 2, 2) for m in FAST]
+    (m, 0, 4, 2, 2) for m in FAST] + [(m, 0, 1, 4, 2) for m in FAST] + [
+    ("bcc_l2_plaq_zeeman", 0, 3, 4, 1), ("fcc_l2_tri_zeeman", 0, 1, 4, 1), ("bcc_body4", 0, 3, 4, 2)]
 
 
 @pytest.mark.parametrize("name,lanes,mode,kernel,proposals", REPLAY_CASES,
@@ -332,14 +333,56 @@ def test_fast_kernel_is_launch_shape_independent(gpu):
             assert np.array_equal(o[2], outs[0][2])
 
 
+def test_cluster_kernel_equals_row_parallel_kernel(gpu):
+    """The chain-resident cluster kernel (kernel 4: one thread-block cluster per
+    replica slot, the replica's spins in every CTA's shared memory, colours separated
+    by the cluster barrier) runs the row-parallel arithmetic: its chains are bitwise
+    those of the row-parallel kernel, for several replicas and for a batch of two
+    lattices of different sizes, with per-sweep launches and in a CUDA graph, with
+    precomputed and inline proposals, overrelaxation included."""
+    w = models.config2_bcc_l2(n=3)
+    Hs = [scemc.TiledHamiltonian(2, w.terms, dims=(d, d, d), magmoms=w.magmoms, field=w.field) for d in (3, 4)]
+    gHs = [scemc.GPUTiledHamiltonian(H) for H in Hs]
+    cfgs = [rand_cfg(H.n_sites, 30 + i) for i, H in enumerate(Hs) for _ in range(3)]
+    betas = np.tile(1 / np.array([0.2e-3, 1e-3, 2e-3]), 2)
+    outs = []
+    for kernel, mode, prop in [(2, 1, 1), (4, 1, 1), (4, 1, 2), (4, 3, 1), (4, 3, 2)]:
+        b = scemc.GPUBatch(gHs, [3, 3], cfgs, [70 + i for i in range(6)], 0.6)
+        b.set_betas(betas)
+        b.run(7, or_per_metropolis=2, kernel=kernel, mode=mode, proposals=prop)
+        st = b.download()
+        outs.append((np.concatenate([c.reshape(-1) for c in st["configs"]]), st["energies"].copy(),
+                     st["counters"].copy()))
+    for o in outs[1:]:
+        np.testing.assert_array_equal(o[0], outs[0][0])
+        np.testing.assert_array_equal(o[1], outs[0][1])
+        np.testing.assert_array_equal(o[2], outs[0][2])
+
+
+def test_cluster_kernel_refusals(gpu):
+    H, _ = build("bcc_l2_plaq_zeeman")
+    b = scemc.GPUBatch([scemc.GPUTiledHamiltonian(H)], [1], [rand_cfg(H.n_sites, 1)], [1], 0.6)
+    with pytest.raises(_lib.ScemcArgumentError):
+        b.run(1, kernel=4, mode=2)
+    Hm, _ = build("mixed")  # no fast tables
+    bm = scemc.GPUBatch([scemc.GPUTiledHamiltonian(Hm)], [1], [rand_cfg(Hm.n_sites, 1)], [1], 0.6)
+    with pytest.raises(_lib.ScemcArgumentError):
+        bm.run(1, kernel=4)
+    w = models.config2_bcc_l2(n=24)  # 27,648 sites x 16 bytes: more than one block's shared memory
+    Hb = w.hamiltonians()[0]
+    bb = scemc.GPUBatch([scemc.GPUTiledHamiltonian(Hb)], [1], [rand_cfg(Hb.n_sites, 1)], [1], 0.6)
+    with pytest.raises(_lib.ScemcArgumentError, match="shared memory"):
+        bb.run(1, kernel=4)
+
+
 def test_autotune_keeps_a_valid_launch_form(gpu):
     H, _ = build("bcc_l2_plaq_zeeman")
     gH = scemc.GPUTiledHamiltonian(H)
     b = scemc.GPUBatch([gH], [3], [rand_cfg(H.n_sites, i) for i in range(3)], [1, 2, 3], 0.6)
     b.set_betas([1 / 0.002, 1 / 0.004, 1 / 0.008])
     t = b.autotune(or_per_metropolis=1, sweeps_per_trial=3)
-    assert t["mode"] in (2, 3) and t["proposals"] in (1, 2) and t["kernel"] in (2, 3) and t["ms_per_sweep"] > 0
-    if t["kernel"] == 3:
+    assert t["mode"] in (2, 3, 4) and t["proposals"] in (1, 2) and t["kernel"] in (2, 3, 4) and t["ms_per_sweep"] > 0
+    if t["kernel"] in (3, 4):
         assert t["mode"] == 3
     before = b.download()["counters"].copy()
     b.run(4, or_per_metropolis=1)  # mode 0 now uses the tuned form

@@ -106,6 +106,89 @@ def test_learned_pass_replay(gpu, lattice, kernel):
     assert ties <= max(1, att // 100)
 
 
+def test_learned_fcc_pass_and_or_replay_at_many_wave_size(gpu):
+    """The learned + overrelaxation form of the large frustrated configuration at a
+    size whose colours fill many waves (fcc 48^3 x 4 sites, 32 rungs, kT geometric in
+    [0.05, 2.0] meV, 18-site environment): one learned Metropolis-Hastings pass (the
+    fused network + decision kernel) and one overrelaxation pass through the forms the
+    library picks (two replicas per thread, one thread per item, no prefetch), recorded
+    on rung 17 (the second lane of thread 1) and replayed through the oracles: dE and
+    the decisions at every site, the draws and the density ratio at 2000 sampled sites,
+    the overrelaxation reflection at every site."""
+    n = 48
+    w = models.config5_fcc(n=n, replicas=32)
+    H = w.hamiltonians()[0]
+    OH = O.OracleHamiltonian(4, w.terms, (n, n, n), magmoms=w.magmoms, field=w.field)
+    env = learned.environment_table(models.FCC.positions, (n, n, n))
+    gH = scemc.GPUTiledHamiltonian(H)
+    net = learned.ProposalNet(seed=3, n_env=env.shape[1])
+    R, rec = 32, 17
+    seeds = [0xF00D + 5 * r for r in range(R)]
+    base = models.random_config(H.n_sites, 5)
+    b = scemc.GPUBatch([gH], [R], [np.roll(base, 11 * r, axis=0) for r in range(R)], seeds, 0.6)
+    b.set_betas(1.0 / w.kts)
+    b.set_learned(net, env)
+    b.record_slot(0, rec)
+    beta = 1.0 / w.kts[rec]
+    kt_mev = np.float32(1e3 / beta)
+    colors = np.asarray(H.colors)
+    pre = b.download()["configs"][rec].copy()
+    cfg = pre.copy()
+    b.record(True)
+    b.run(1, kernel=3, proposals=3, mode=1, or_per_metropolis=1)
+    # learned Metropolis-Hastings pass
+    prop, u, dE32, flag = b.fetch_record(-1)
+    lqr = b.fetch_record_ratio()
+    assert np.all(flag != 3)
+    dE64, scale, _, _ = OH.replay_sweep(cfg, prop.astype(np.float64), u, (flag == 1).astype(np.uint8), beta)
+    mid = cfg.copy()
+    tol = 1e-5 * scale + 1e-30
+    assert np.all(np.abs(dE32.astype(np.float64) - dE64) <= tol)
+    la = -beta * dE64 + lqr
+    oacc = (la >= 0) | (u < np.exp(np.minimum(la, 0.0)))
+    tie = (np.abs(la - np.log(u)) <= beta * tol) | (np.abs(la) <= beta * tol)
+    mism = (flag == 1) != oacc
+    assert not (mism & ~tie).any(), np.nonzero(mism & ~tie)[0][:5]
+    ties = int((mism & tie).sum())
+    sites = np.sort(np.random.default_rng(7).choice(H.n_sites, 2000, replace=False))
+    X = env_rows(env, colors, pre, mid, sites, kt_mev)
+    out = np.zeros((len(sites), 32))
+    out[:, :20] = net.forward(X)
+    for i, s in enumerate(sites):
+        b0 = O.philox_block(seeds[rec], int(s) + 1, 1, 0, tag=4)
+        b1 = O.philox_block(seeds[rec], int(s) + 1, 1, 1, tag=4)
+        x, _ = LO.sample(out[i], float(kt_mev), O.philox_uniform(b0[0], b0[1]), O.philox_uniform(b0[2], b0[3]),
+                         O.philox_uniform(b1[0], b1[1]))
+        assert np.max(np.abs(prop[s] - x.astype(np.float32))) <= 3e-5, (s, prop[s], x)
+        assert u[s] == O.philox_uniform(b1[2], b1[3])
+    tau = np.full(len(sites), float(kt_mev))
+    lq_ref = LO.log_q(out, tau, pre[sites]) - LO.log_q(out, tau, prop[sites].astype(np.float64))
+    np.testing.assert_allclose(lqr[sites], lq_ref, rtol=0, atol=2e-4)
+    # overrelaxation pass on the state the learned pass left
+    prop, u, dE32, flag = b.fetch_record(0)
+    pre_or = cfg.copy()
+    dE64, scale, oacc, c = OH.replay_sweep(cfg, prop.astype(np.float64), u, (flag == 1).astype(np.uint8), beta,
+                                           want_c=True)
+    att = (flag == 0) | (flag == 1)
+    tol = 1e-5 * scale + 1e-30
+    assert np.all(np.abs(dE32[att].astype(np.float64) - dE64[att]) <= tol[att])
+    with np.errstate(divide="ignore"):
+        thr = -np.log(u) / beta
+    tie = (np.abs(dE64 - thr) <= tol) | (np.abs(dE64) <= tol)
+    mism = att & ((flag == 1) != oacc)
+    assert not (mism & ~tie).any(), np.nonzero(mism & ~tie)[0][:5]
+    ties += int((mism & tie).sum())
+    h = c[:, [3, 1, 2]]
+    a = h / np.linalg.norm(h, axis=1, keepdims=True)
+    refl = 2.0 * np.sum(pre_or * a, axis=1, keepdims=True) * a - pre_or
+    refl /= np.linalg.norm(refl, axis=1, keepdims=True)
+    assert np.max(np.abs(prop[att] - refl[att])) <= 1e-4
+    np.testing.assert_array_equal(b.download()["configs"][rec], cfg)
+    E_or = OH.total_energy(cfg)
+    assert abs(b.total_energy(rec) - E_or) <= 1e-10 * max(1.0, abs(E_or))
+    assert ties <= max(1, 2 * H.n_sites // 100)
+
+
 def langevin(x):
     return 1.0 / math.tanh(x) - 1.0 / x
 
