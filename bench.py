@@ -41,6 +41,12 @@ metric is tau_int-corrected independent samples per second, ESS/s = sum over
 chains of n_meas / (1 + 2 max(tau_int(E), tau_int(|m|))) over the measurement wall
 time; the line reports the learned value with the plain one and their ratio.
 
+--workload l2body3 (not one of the five benchmark configurations): bcc 16^3 with l <= 2
+pairs to shell 2 and (NN, NN, NNN) triangles with every member l in {1, 2} (the
+body-3-heavy regime of the reference's fitted models), 5 chains, Metropolis + OR; L2
+flushed before every step. Compare the default (merged dense body-3 records) with
+--kernel 1 (the generic walk of the reference's sparse programs).
+
 --workload fcc_learned (the large frustrated configuration as specified): the fcc
 workload with the learned proposal. The network (18-site environment, 55 inputs) is
 trained on 200k environments from plain chains at the 32 kT values; then Metropolis
@@ -49,7 +55,7 @@ thermalisation and --steps (default 4000) measured compound sweeps of the 32 run
 The metric is tau_int-corrected samples/s, as for --workload learned.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl scemc|reference]
-                  [--workload fcc|bcc16|pt|learned|fcc_learned]
+                  [--workload fcc|bcc16|pt|learned|fcc_learned|l2body3]
 
 --impl reference times the FP64 CPU restatement of the reference's
 metropolis_sweep!/overrelaxation_sweep! (oracle/, colour-parallel over all host
@@ -86,6 +92,7 @@ WORKLOADS = {
     "learned": "bcc32_J1J2_body4_16T_learned_vs_plain",
     "pt": "bcc8-12-16-24_J1J2_triangles_4x16rungs_PT",
     "fcc_learned": "fcc{n}_l2_tri_zeeman_32rungs_learned+OR+exchange_vs_metropolis+OR+exchange",
+    "l2body3": "bcc16_l2_pairs_l2_triangles_5T_metropolis+OR",
 }
 
 
@@ -116,6 +123,8 @@ def workload(args):
         return WORKLOADS["fcc"].format(n=args.fcc_n), w, True
     if args.workload == "pt":
         return WORKLOADS["pt"], models.config3_bcc_pt(), True
+    if args.workload == "l2body3":
+        return WORKLOADS["l2body3"], models.bcc_l2_body3(16), False
     return WORKLOADS["bcc16"], models.config2_bcc_l2(16), False
 
 

@@ -66,6 +66,15 @@ int32_t fail(int32_t code, const std::string& m) {
       return fail(SCEMC_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
+// A host-to-device copy that has landed on the device when it returns. From pageable
+// memory cudaMemcpy may return once the source is staged, and the legacy stream's DMA
+// is not ordered before kernels on the batches' non-blocking streams; waiting for the
+// legacy stream closes that window. Used for tables and run parameters (not per step).
+inline cudaError_t h2d_sync(void* dst, const void* src, size_t bytes) {
+  cudaError_t e = cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+  return e == cudaSuccess ? cudaStreamSynchronize(0) : e;
+}
+
 enum Kind : int {
   K_GEN = 0,
   K_B1_L1 = 1,
@@ -75,7 +84,9 @@ enum Kind : int {
   K_B2_21 = 5,
   K_B2_22 = 6,
   K_B3_111 = 7,
-  K_B4_1111 = 8
+  K_B4_1111 = 8,
+  K_B3_L2 = 9  // body 3, every member l in {1, 2}, not all l = 1 (fast tables only; the generic
+               // records walk it as a sparse program)
 };
 constexpr int kKindShift = 26;
 constexpr int32_t kOffMask = (1 << kKindShift) - 1;
@@ -611,7 +622,10 @@ __global__ void k_barrier_selftest(GridSync* gs, long long limit_ns) {
 // reduces dE = sum_t c_t (znew_t - zold_t) with a fixed butterfly, so the result
 // does not depend on the launch shape.
 // ---------------------------------------------------------------------------
-constexpr int F_PAIR = 1, F_TRIP = 2, F_QUAD = 3, F_ONE = 4;
+// F_TRIP2: a merged body-3 block with l in {1, 2} members, NR x NR x NR floats
+// W[t][p][q] (t the site's row, p and q the rows of the neighbours with the smaller and
+// the larger local index); counted with the l = 1 triplets, told apart by its kind.
+constexpr int F_PAIR = 1, F_TRIP = 2, F_QUAD = 3, F_ONE = 4, F_TRIP2 = 5;
 
 template <int NR>
 __device__ __forceinline__ void zrow_nr(float x, float y, float z, float* o) {
@@ -729,12 +743,31 @@ __device__ __forceinline__ float fast_walk(const uint2* rb, const float* zb, con
       }
     }
   }
-  // l = 1 triplets and quads: rows 1..3 only
-  if (row < 3) {
-    for (int j = n_pair + slice; j < n_pair + n_trip; j += S) {
-      const uint2 fr = rb[j];
-      const float* z1 = zb + (fr.y & 0xffu) * NR;
-      const float* z2 = zb + ((fr.y >> 8) & 0xffu) * NR;
+  // triplets: l = 1 blocks feed rows 1..3 only; merged blocks with l = 2 members
+  // (NR = 8) feed every row: c_row += sum_p z1_p sum_q W[row][p][q] z2_q
+  for (int j = n_pair + slice; j < n_pair + n_trip; j += S) {
+    const uint2 fr = rb[j];
+    const float* z1 = zb + (fr.y & 0xffu) * NR;
+    const float* z2 = zb + ((fr.y >> 8) & 0xffu) * NR;
+    if (NR == 8 && (fr.x >> kKindShift) == (uint32_t)F_TRIP2) {
+      if (row < NR) {
+        const float4* w4 = reinterpret_cast<const float4*>(ft + (fr.x & kOffMask) + row * NR * NR);
+        const float4 za = *reinterpret_cast<const float4*>(z2), zc = *reinterpret_cast<const float4*>(z2 + 4);
+#pragma unroll
+        for (int p = 0; p < NR; ++p) {
+          const float4 a0 = __ldg(w4 + 2 * p), a1 = __ldg(w4 + 2 * p + 1);
+          float t = a0.x * za.x;
+          t = fmaf(a0.y, za.y, t);
+          t = fmaf(a0.z, za.z, t);
+          t = fmaf(a0.w, za.w, t);
+          t = fmaf(a1.x, zc.x, t);
+          t = fmaf(a1.y, zc.y, t);
+          t = fmaf(a1.z, zc.z, t);
+          t = fmaf(a1.w, zc.w, t);
+          acc2 = fmaf(z1[p], t, acc2);
+        }
+      }
+    } else if (row < 3) {
       const float4* w4 = reinterpret_cast<const float4*>(ft + (fr.x & kOffMask) + row * 12);
       const float4 a0 = __ldg(w4), a1 = __ldg(w4 + 1), a2 = __ldg(w4 + 2);
       const float w[9] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a2.x};
@@ -744,6 +777,9 @@ __device__ __forceinline__ float fast_walk(const uint2* rb, const float* zb, con
         acc = fmaf(z1[p], t, acc);
       }
     }
+  }
+  // l = 1 quads: rows 1..3 only
+  if (row < 3) {
     for (int j = n_pair + n_trip + slice; j < n_pair + n_trip + n_quad; j += S) {
       const uint2 fr = rb[j];
       const float* z1 = zb + (fr.y & 0xffu) * NR;
@@ -1255,11 +1291,7 @@ __device__ __forceinline__ void rep_coeffs(const DevLattice& L, const float4* __
 #pragma unroll
     for (int t = 0; t < NR; ++t) c[k][t] = 0.0f;
   // merged per-neighbour pair blocks: c += W z_nb
-#pragma unroll 1
-  for (int j = part; j < n_pair; j += NP) {
-    const uint2 rec = __ldg(fr + j);
-    float4 v[P];
-    gather((int)(rec.y & 0xffu), v);
+  auto pair = [&](uint2 rec, const float4 (&v)[P]) {
     float z[P][NR];
 #pragma unroll
     for (int k = 0; k < P; ++k) zrow_nr<NR>(v[k].x, v[k].y, v[k].z, z[k]);
@@ -1293,6 +1325,13 @@ __device__ __forceinline__ void rep_coeffs(const DevLattice& L, const float4* __
         for (int t = 0; t < 3; ++t)
           c[k][t] = fmaf(ww[3 * t], z[k][0], fmaf(ww[3 * t + 1], z[k][1], fmaf(ww[3 * t + 2], z[k][2], c[k][t])));
     }
+  };
+#pragma unroll 1
+  for (int j = part; j < n_pair; j += NP) {
+    const uint2 rec = __ldg(fr + j);
+    float4 v[P];
+    gather((int)(rec.y & 0xffu), v);
+    pair(rec, v);
   }
   // l = 1 triplets: c_t += sum_p z1_p sum_q W[t][3p + q] z2_q (rows padded to 12)
 #pragma unroll 1
@@ -1301,6 +1340,38 @@ __device__ __forceinline__ void rep_coeffs(const DevLattice& L, const float4* __
     float4 v1[P], v2[P];
     gather((int)(rec.y & 0xffu), v1);
     gather((int)((rec.y >> 8) & 0xffu), v2);
+    if constexpr (NR == 8) {
+      // merged body-3 block with l = 2 members: c_t += sum_p z1_p sum_q W[t][p][q] z2_q
+      if ((rec.x >> kKindShift) == (uint32_t)F_TRIP2) {
+        float y1[P][NR], y2[P][NR];
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+          zrow_nr<NR>(v1[k].x, v1[k].y, v1[k].z, y1[k]);
+          zrow_nr<NR>(v2[k].x, v2[k].y, v2[k].z, y2[k]);
+        }
+        const float4* w4 = reinterpret_cast<const float4*>(ft + (rec.x & kOffMask));
+#pragma unroll
+        for (int t = 0; t < NR; ++t) {
+#pragma unroll
+          for (int p = 0; p < NR; ++p) {
+            const float4 a0 = __ldg(w4 + (t * NR + p) * 2), a1 = __ldg(w4 + (t * NR + p) * 2 + 1);
+#pragma unroll
+            for (int k = 0; k < P; ++k) {
+              float u = a0.x * y2[k][0];
+              u = fmaf(a0.y, y2[k][1], u);
+              u = fmaf(a0.z, y2[k][2], u);
+              u = fmaf(a0.w, y2[k][3], u);
+              u = fmaf(a1.x, y2[k][4], u);
+              u = fmaf(a1.y, y2[k][5], u);
+              u = fmaf(a1.z, y2[k][6], u);
+              u = fmaf(a1.w, y2[k][7], u);
+              c[k][t] = fmaf(y1[k][p], u, c[k][t]);
+            }
+          }
+        }
+        continue;
+      }
+    }
     float z1[P][3], z2[P][3];
 #pragma unroll
     for (int k = 0; k < P; ++k) {
@@ -2063,7 +2134,7 @@ int32_t upload(std::vector<void*>& allocs, const std::vector<T>& v, const T** ou
   const size_t bytes = std::max<size_t>(v.size() * sizeof(T), 16);
   CUDA_TRY(cudaMalloc(&p, bytes));
   allocs.push_back(p);
-  if (!v.empty()) CUDA_TRY(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  if (!v.empty()) CUDA_TRY(h2d_sync(p, v.data(), v.size() * sizeof(T)));
   *out = static_cast<const T*>(p);
   return SCEMC_OK;
 }
@@ -2226,9 +2297,11 @@ struct FastBuild {
   int32_t dmax = 0, rmax = 0;
 };
 
+// prog_l: per program, the l of its own member and of its other members in slot
+// order (three entries; the body-3 block layout needs them).
 bool build_fast(const scemc_tables_desc* d, const std::vector<int32_t>& prog_kind,
-                const std::vector<int32_t>& prog_toff, const std::vector<float>& tensor,
-                const std::vector<int32_t>& pbase, FastBuild& F) {
+                const std::vector<int32_t>& prog_toff, const std::vector<int32_t>& prog_l,
+                const std::vector<float>& tensor, const std::vector<int32_t>& pbase, FastBuild& F) {
   if (d->lmax != 1 && d->lmax != 2) return false;
   const int NR = d->nlm - 1;
   for (int32_t k : prog_kind)
@@ -2239,7 +2312,7 @@ bool build_fast(const scemc_tables_desc* d, const std::vector<int32_t>& prog_kin
     F.ft.insert(F.ft.end(), v.begin(), v.end());
     return off;
   };
-  std::map<std::vector<int32_t>, int32_t> pair_cache, one_cache;
+  std::map<std::vector<int32_t>, int32_t> pair_cache, one_cache, tri2_cache;
   std::vector<int32_t> single_off(prog_kind.size(), -1);
   // program id -> (template, slot) for the l placement of pair blocks
   const int ns = d->n_sites;
@@ -2250,11 +2323,15 @@ bool build_fast(const scemc_tables_desc* d, const std::vector<int32_t>& prog_kin
   std::vector<std::pair<int32_t, std::vector<int32_t>>> pairs;  // (local, pids)
   std::vector<int32_t> ones;
   std::vector<std::array<int32_t, 5>> multi;  // (kind, pid, l0, l1, l2)
+  // body-3 programs with l = 2 members, merged per unordered neighbour pair:
+  // ((smaller local, larger local), [pid * 2 + (factor order reversed)])
+  std::vector<std::pair<std::pair<int32_t, int32_t>, std::vector<int32_t>>> tri2;
   for (int32_t s = 0; s < ns; ++s) {
     nbs.clear();
     pairs.clear();
     ones.clear();
     multi.clear();
+    tri2.clear();
     auto local = [&](int32_t site) {
       for (size_t i = 0; i < nbs.size(); ++i)
         if (nbs[i] == site) return (int32_t)i;
@@ -2282,6 +2359,17 @@ bool build_fast(const scemc_tables_desc* d, const std::vector<int32_t>& prog_kin
             break;
           }
         if (!found) pairs.push_back({loc[0], {pid}});
+      } else if (kind == K_B3_L2) {
+        const std::pair<int32_t, int32_t> key{std::min(loc[0], loc[1]), std::max(loc[0], loc[1])};
+        const int32_t tag = pid * 2 + (loc[0] > loc[1] ? 1 : 0);
+        bool found = false;
+        for (auto& t : tri2)
+          if (t.first == key) {
+            t.second.push_back(tag);
+            found = true;
+            break;
+          }
+        if (!found) tri2.push_back({key, {tag}});
       } else {
         multi.push_back({kind, pid, loc[0], loc[1], loc[2]});
       }
@@ -2318,6 +2406,38 @@ bool build_fast(const scemc_tables_desc* d, const std::vector<int32_t>& prog_kin
     std::stable_sort(multi.begin(), multi.end(),
                      [](const std::array<int32_t, 5>& x, const std::array<int32_t, 5>& y) { return x[0] < y[0]; });
     int n_trip = 0, n_quad = 0;
+    // merged body-3 blocks with l = 2 members (before the l = 1 triplets, in the triplet range)
+    for (auto& t : tri2) {
+      std::vector<int32_t> key = t.second;
+      std::sort(key.begin(), key.end());
+      auto it = tri2_cache.find(key);
+      int32_t off;
+      if (it != tri2_cache.end()) {
+        off = it->second;
+      } else {
+        std::vector<float> W((size_t)NR * NR * NR, 0.0f);
+        for (int32_t tag : key) {
+          const int32_t pid = tag >> 1;
+          const bool flip = (tag & 1) != 0;
+          const int lt = prog_l[3 * pid], l0 = prog_l[3 * pid + 1], l1 = prog_l[3 * pid + 2];
+          const int d0 = 2 * l0 + 1, d1 = 2 * l1 + 1;
+          const int rt = lt == 1 ? 0 : 3, r0 = l0 == 1 ? 0 : 3, r1 = l1 == 1 ? 0 : 3;
+          for (int mt = 0; mt < 2 * lt + 1; ++mt)
+            for (int m0 = 0; m0 < d0; ++m0)
+              for (int m1 = 0; m1 < d1; ++m1) {
+                const float v = tensor[prog_toff[pid] + (mt * d0 + m0) * d1 + m1];
+                const int p = flip ? r1 + m1 : r0 + m0, q = flip ? r0 + m0 : r1 + m1;
+                W[((size_t)(rt + mt) * NR + p) * NR + q] += v;
+              }
+        }
+        off = place(W);
+        tri2_cache[key] = off;
+      }
+      if (off > kOffMask) return false;
+      ++n_trip;
+      F.frec.push_back(make_uint2(((uint32_t)F_TRIP2 << kKindShift) | (uint32_t)off,
+                                  (uint32_t)t.first.first | ((uint32_t)t.first.second << 8)));
+    }
     for (auto& m : multi) {
       const int32_t pid = m[1];
       if (single_off[pid] < 0) {
@@ -2416,7 +2536,7 @@ int32_t compile_tables(const scemc_tables_desc* d, scemc_tables* T) {
       return fail(SCEMC_ERR_ARG, "instance size differs from its template's body order");
   }
   // programs: kind + dense tensor (fast kinds), sparse descriptors (all)
-  std::vector<int32_t> prog_kind(d->n_sprog, K_GEN), prog_toff(d->n_sprog, 0);
+  std::vector<int32_t> prog_kind(d->n_sprog, K_GEN), prog_toff(d->n_sprog, 0), prog_l(3 * d->n_sprog, 0);
   std::vector<DevProg> progs(d->n_sprog);
   std::vector<float> tensor;
   for (int64_t k = 0; k < d->n_terms; ++k) {
@@ -2446,6 +2566,7 @@ int32_t compile_tables(const scemc_tables_desc* d, scemc_tables* T) {
           if (D == 1) kind = lt == 1 ? K_B1_L1 : K_B1_L2;
           else if (D == 2) kind = lt == 1 ? (lf[0] == 1 ? K_B2_11 : K_B2_12) : (lf[0] == 1 ? K_B2_21 : K_B2_22);
           else if (D == 3 && lt == 1 && lf[0] == 1 && lf[1] == 1) kind = K_B3_111;
+          else if (D == 3 && d->lmax == 2) kind = K_B3_L2;
           else if (D == 4 && lt == 1 && lf[0] == 1 && lf[1] == 1 && lf[2] == 1) kind = K_B4_1111;
         }
       }
@@ -2476,6 +2597,8 @@ int32_t compile_tables(const scemc_tables_desc* d, scemc_tables* T) {
         prog_toff[pid] = off;
       }
       prog_kind[pid] = kind;
+      prog_l[3 * pid] = lt;
+      for (int q = 0; q < nf && q < 2; ++q) prog_l[3 * pid + 1 + q] = lf[q];
     }
   }
   if (d->n_sprog > kOffMask) return fail(SCEMC_ERR_UNSUPPORTED, "too many site programs");
@@ -2500,7 +2623,9 @@ int32_t compile_tables(const scemc_tables_desc* d, scemc_tables* T) {
       if (d->inst_sites[d->inst_ptr[inst] - 1 + own - 1] != s + 1)
         return fail(SCEMC_ERR_ARG, "site_slot does not point back at the site");
       int4 r4;
-      const int kind = prog_kind[pid];
+      // body-3 blocks with l = 2 members have a dense form only in the fast tables; the
+      // generic walk keeps the reference's sparse program for them
+      const int kind = prog_kind[pid] == K_B3_L2 ? (int)K_GEN : prog_kind[pid];
       r4.x = (kind << kKindShift) | (kind == K_GEN ? pid : prog_toff[pid]);
       r4.y = r4.z = r4.w = -1;
       if (D <= 4) {
@@ -2543,7 +2668,7 @@ int32_t compile_tables(const scemc_tables_desc* d, scemc_tables* T) {
   }
   for (int64_t f = 0; f < d->n_efac; ++f) efac_row[f] = (int8_t)(d->efac_row[f] - 1);
   FastBuild F;
-  const bool fast = build_fast(d, prog_kind, prog_toff, tensor, pbase, F);
+  const bool fast = build_fast(d, prog_kind, prog_toff, prog_l, tensor, pbase, F);
   // the generic records are kept for every model that needs them, and for small
   // fast ones (so the generic form can still be selected); huge fast models skip them
   const bool keep_generic = !fast || d->n_adj <= (int64_t)(1 << 24);
@@ -2653,6 +2778,9 @@ template <typename T>
 int32_t dalloc(T** p, size_t n) {
   CUDA_TRY(cudaMalloc((void**)p, std::max<size_t>(n * sizeof(T), 16)));
   CUDA_TRY(cudaMemset(*p, 0, std::max<size_t>(n * sizeof(T), 16)));
+  // the legacy-stream clear is not ordered before work on the batches' non-blocking
+  // streams: wait for it here (allocation happens at set-up, outside any capture)
+  CUDA_TRY(cudaStreamSynchronize(0));
   return SCEMC_OK;
 }
 
@@ -2835,7 +2963,7 @@ int32_t create_ensemble(int32_t n_tables, const scemc_tables* const* tables, con
     max_atoms = std::max(max_atoms, tables[i]->n_cell_atoms);
   }
   if ((rc = dalloc(&E->d_lat, n_tables))) return rc;
-  CUDA_TRY(cudaMemcpy(E->d_lat, lats.data(), sizeof(DevLattice) * n_tables, cudaMemcpyHostToDevice));
+  CUDA_TRY(h2d_sync(E->d_lat, lats.data(), sizeof(DevLattice) * n_tables));
   // per-colour item prefixes
   E->seg.assign((size_t)std::max(E->max_colors, 1) * (n_tables + 1), 0);
   for (int c = 0; c < E->max_colors; ++c) {
@@ -2849,7 +2977,7 @@ int32_t create_ensemble(int32_t n_tables, const scemc_tables* const* tables, con
     E->seg[(size_t)c * (n_tables + 1) + n_tables] = (int32_t)acc;
   }
   if ((rc = dalloc(&E->d_seg, E->seg.size()))) return rc;
-  CUDA_TRY(cudaMemcpy(E->d_seg, E->seg.data(), E->seg.size() * 4, cudaMemcpyHostToDevice));
+  CUDA_TRY(h2d_sync(E->d_seg, E->seg.data(), E->seg.size() * 4));
   E->item_base.assign(E->max_colors + 1, 0);
   for (int c = 0; c < E->max_colors; ++c) {
     const int64_t nb = (int64_t)E->item_base[c] + E->seg[(size_t)c * (n_tables + 1) + n_tables];
@@ -2857,7 +2985,7 @@ int32_t create_ensemble(int32_t n_tables, const scemc_tables* const* tables, con
     E->item_base[c + 1] = (int32_t)nb;
   }
   if ((rc = dalloc(&E->d_item_base, E->item_base.size()))) return rc;
-  CUDA_TRY(cudaMemcpy(E->d_item_base, E->item_base.data(), E->item_base.size() * 4, cudaMemcpyHostToDevice));
+  CUDA_TRY(h2d_sync(E->d_item_base, E->item_base.data(), E->item_base.size() * 4));
   E->fast = true;
   for (int i = 0; i < n_tables; ++i) {
     E->fast = E->fast && tables[i]->dl.fast && tables[i]->lmax == E->lmax;
@@ -2883,13 +3011,13 @@ int32_t create_ensemble(int32_t n_tables, const scemc_tables* const* tables, con
     return rc;
   std::vector<int32_t> ident(slots);
   for (int i = 0; i < slots; ++i) ident[i] = i;
-  CUDA_TRY(cudaMemcpy(E->d_slot_of_rung, ident.data(), 4 * slots, cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(E->d_rung_of_slot, ident.data(), 4 * slots, cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(E->d_energy, energies, 8 * slots, cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(E->d_step, steps, 8 * slots, cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(E->d_seed, seeds, 8 * slots, cudaMemcpyHostToDevice));
+  CUDA_TRY(h2d_sync(E->d_slot_of_rung, ident.data(), 4 * slots));
+  CUDA_TRY(h2d_sync(E->d_rung_of_slot, ident.data(), 4 * slots));
+  CUDA_TRY(h2d_sync(E->d_energy, energies, 8 * slots));
+  CUDA_TRY(h2d_sync(E->d_step, steps, 8 * slots));
+  CUDA_TRY(h2d_sync(E->d_seed, seeds, 8 * slots));
   std::vector<double> ones(slots, 1.0);
-  CUDA_TRY(cudaMemcpy(E->d_beta, ones.data(), 8 * slots, cudaMemcpyHostToDevice));
+  CUDA_TRY(h2d_sync(E->d_beta, ones.data(), 8 * slots));
   E->rec_len = 4 + 3 * max_atoms;
   if ((rc = payload_upload(E, configs, nullptr))) return rc;
   *out = guard.release();
@@ -3430,7 +3558,7 @@ int32_t check_error(scemc_ensemble* E) {
   CUDA_TRY(cudaStreamSynchronize(E->stream));
   if (gs.error) {
     GridSync z{};
-    cudaMemcpy(E->d_gs, &z, sizeof(z), cudaMemcpyHostToDevice);
+    CUDA_TRY(h2d_sync(E->d_gs, &z, sizeof(z)));
     E->bar_base = 0;
     return fail(SCEMC_ERR_TIMEOUT, "grid barrier wait gave up (bounded spin); state of this sweep is torn");
   }
@@ -3901,7 +4029,7 @@ int32_t scemc_set_step(scemc_chain* c, double step) {
   int32_t rc;
   if ((rc = check_single(c, nullptr))) return rc;
   if (!(step > 0) || !std::isfinite(step)) return fail(SCEMC_ERR_ARG, "step must be > 0");
-  CUDA_TRY(cudaMemcpy(c->d_step, &step, 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(h2d_sync(c->d_step, &step, 8));
   return SCEMC_OK;
 }
 
@@ -3916,8 +4044,8 @@ int32_t scemc_swap_payload(scemc_chain* a, scemc_chain* b) {
   double ea, eb;
   CUDA_TRY(cudaMemcpy(&ea, a->d_energy, 8, cudaMemcpyDeviceToHost));
   CUDA_TRY(cudaMemcpy(&eb, b->d_energy, 8, cudaMemcpyDeviceToHost));
-  CUDA_TRY(cudaMemcpy(a->d_energy, &eb, 8, cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(b->d_energy, &ea, 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(h2d_sync(a->d_energy, &eb, 8));
+  CUDA_TRY(h2d_sync(b->d_energy, &ea, 8));
   return SCEMC_OK;
 }
 
@@ -3945,7 +4073,7 @@ int32_t scemc_batch_set_betas(scemc_batch* b, const double* betas) {
   if (!b || !betas) return fail(SCEMC_ERR_ARG, "NULL argument");
   for (int i = 0; i < b->n_slots; ++i)
     if (!std::isfinite(betas[i])) return fail(SCEMC_ERR_ARG, "beta must be finite");
-  CUDA_TRY(cudaMemcpy(b->d_beta, betas, 8 * b->n_slots, cudaMemcpyHostToDevice));
+  CUDA_TRY(h2d_sync(b->d_beta, betas, 8 * b->n_slots));
   return SCEMC_OK;
 }
 
@@ -3953,7 +4081,7 @@ int32_t scemc_batch_set_steps(scemc_batch* b, const double* steps) {
   if (!b || !steps) return fail(SCEMC_ERR_ARG, "NULL argument");
   for (int i = 0; i < b->n_slots; ++i)
     if (!(steps[i] > 0)) return fail(SCEMC_ERR_ARG, "step must be > 0");
-  CUDA_TRY(cudaMemcpy(b->d_step, steps, 8 * b->n_slots, cudaMemcpyHostToDevice));
+  CUDA_TRY(h2d_sync(b->d_step, steps, 8 * b->n_slots));
   return SCEMC_OK;
 }
 
@@ -4293,8 +4421,14 @@ int32_t scemc_batch_record(scemc_batch* b, int32_t on) {
       return rc;
     b->rec_cap = cap;
   }
-  if (b->recording) CUDA_TRY(cudaMemset(b->d_rlqr, 0, sizeof(double) * cap));
-  if (b->recording) CUDA_TRY(cudaMemset(b->d_racc, 3, n));  // 3 = site not visited
+  // cleared on the batch's own (non-blocking) stream and waited for: a clear on the
+  // legacy stream is not ordered before the batch's next kernels, which may then record
+  // first and be overwritten
+  if (b->recording) {
+    CUDA_TRY(cudaMemsetAsync(b->d_rlqr, 0, sizeof(double) * cap, b->stream));
+    CUDA_TRY(cudaMemsetAsync(b->d_racc, 3, n, b->stream));  // 3 = site not visited
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+  }
   return SCEMC_OK;
 }
 
@@ -4357,7 +4491,7 @@ int32_t scemc_batch_set_learned(scemc_batch* b, const scemc_mlp* m, const int32_
         }
       int32_t rc;
       if ((rc = dalloc(&b->d_env[i], (size_t)n))) return rc;
-      CUDA_TRY(cudaMemcpy(b->d_env[i], env + off, sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+      CUDA_TRY(h2d_sync(b->d_env[i], env + off, sizeof(int32_t) * n));
       off += n;
     }
     b->mlp = m;
@@ -4366,7 +4500,7 @@ int32_t scemc_batch_set_learned(scemc_batch* b, const scemc_mlp* m, const int32_
     lats[i].env = b->d_env[i];
     lats[i].env_k = m ? k : 0;
   }
-  CUDA_TRY(cudaMemcpy(b->d_lat, lats.data(), sizeof(DevLattice) * lats.size(), cudaMemcpyHostToDevice));
+  CUDA_TRY(h2d_sync(b->d_lat, lats.data(), sizeof(DevLattice) * lats.size()));
   return SCEMC_OK;
 }
 

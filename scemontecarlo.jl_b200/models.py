@@ -237,6 +237,26 @@ def bcc_triangles(sigma: float, rng):
     return out
 
 
+def bcc_l2_triangles(sigma: float, rng):
+    """bcc (NN, NN, NNN) triangles with every member l in {1, 2}: one template per
+    (l1, l2, l3) combination, N(0, sigma) dense tensors (eV). The reference's fitted
+    models are dominated by body-3 terms of this kind (l up to 2 on every member)."""
+    nn, nnn = BCC.shells(2)
+    mem = []
+    for a in (1, 2):
+        pa = BCC.positions[a - 1]
+        for v1 in BCC.neighbours(a, nnn):
+            for v2 in BCC.neighbours(a, nn):
+                if abs(np.linalg.norm(v1 - v2) - nn) < 1e-9:
+                    mem.append([pa, pa + v2, pa + v1])
+    out = []
+    for atoms, shifts in BCC.clusters(mem):
+        for ls in itertools.product((1, 2), repeat=3):
+            f = sigma * rng.standard_normal(tuple(2 * l + 1 for l in ls)) / FOUR_PI ** 1.5
+            out.append(MultipoleTerm(1.0, atoms, shifts, list(ls), f))
+    return out
+
+
 def sc_plaquettes(lat: Lattice, sigma: float, rng):
     """4-site squares of each atom's simple-cubic sublattice (three planes per atom),
     l = 1, N(0, sigma) dense tensors (eV)."""
@@ -315,6 +335,19 @@ def config3_bcc_pt(sizes=(8, 12, 16, 24), rungs: int = 16) -> Workload:
     kts = np.geomspace(0.1, 3.0, rungs) * MEV
     return Workload("bcc_pt_uneven", 2, terms, [(s, s, s) for s in sizes], kts, sweeps_therm=2000,
                     sweeps_measure=8000, seed=3, exchange=True)
+
+
+def bcc_l2_body3(n: int = 16) -> Workload:
+    """bcc n^3 with l <= 2 pairs to shell 2 (means -1.0/-0.3 meV, sigma 0.1 meV) and
+    (NN, NN, NNN) triangles with every (l1, l2, l3) in {1, 2}^3, N(0, 0.05 meV); 5 kT in
+    [0.2, 2.0] meV; Metropolis + OR; seed 6. The body-3-with-l = 2 regime of fitted
+    models (not one of the five benchmark configurations)."""
+    rng = np.random.default_rng(6)
+    terms = multipole_pairs(BCC, [-1.0 * MEV, -0.3 * MEV], 0.1 * MEV, rng)
+    terms += bcc_l2_triangles(0.05 * MEV, rng)
+    kts = np.linspace(0.2, 2.0, 5) * MEV
+    return Workload("bcc16_l2_body3", 2, terms, [(n, n, n)], kts, sweeps_therm=2000, sweeps_measure=10000,
+                    or_per_metropolis=1, seed=6)
 
 
 def config4_bcc_body4(n: int = 32) -> Workload:

@@ -40,6 +40,7 @@ MODELS = {
     "bcc_triangles": (2, models.config3_bcc_pt().terms, (3, 3, 3), {}),
     "bcc_body4": (2, models.config4_bcc_body4().terms, (3, 3, 3), {}),
     "fcc_l2_tri_zeeman": (4, models.config5_fcc(n=2).terms, (2, 2, 2), dict(magmoms=[2.0] * 4, field=[0.3] * 3)),
+    "bcc_l2_body3": (2, models.bcc_l2_body3(3).terms, (3, 3, 3), {}),
 }
 
 
@@ -179,7 +180,7 @@ def test_sweep_replay(gpu, name, lanes, mode, kernel, proposals):
 REP_FORMS = [(P, NP, PF) for P in (1, 2) for NP in (1, 2) for PF in (1, 2)]
 
 
-@pytest.mark.parametrize("name", ["bcc_body4", "fcc_l2_tri_zeeman"])
+@pytest.mark.parametrize("name", ["bcc_body4", "fcc_l2_tri_zeeman", "bcc_l2_body3"])
 @pytest.mark.parametrize("P,NP,PF", REP_FORMS, ids=[f"P{p}-NP{n}-PF{f}" for p, n, f in REP_FORMS])
 def test_rep_colour_every_instance_replays(gpu, name, P, NP, PF):
     H, OH = build(name)

@@ -130,6 +130,7 @@ CASES = [
     ("chain", 1, models.chain_terms(0.05), (4, 1, 1)),
     ("mixed", 2, models.mixed_terms(7), (2, 2, 1)),
     ("high l", 1, models.highl_terms(11, 4), (3, 1, 1)),
+    ("body3 l<=2", 2, models.bcc_l2_triangles(0.05e-3, np.random.default_rng(6)), (2, 2, 2)),
 ]
 
 

@@ -37,6 +37,7 @@ FIXTURES = [
     ("bcc triangles", 2, models.config3_bcc_pt().terms, (3, 3, 3), {}),
     ("bcc body4", 2, models.config4_bcc_body4().terms, (3, 3, 3), {}),
     ("fcc l2 tri", 4, models.config5_fcc(n=2).terms, (3, 3, 3), dict(magmoms=[2.0] * 4, field=[0.3, 0.3, 0.3])),
+    ("bcc l2 body3", 2, models.bcc_l2_body3(3).terms, (3, 3, 3), {}),
 ]
 
 
