@@ -3733,7 +3733,7 @@ int32_t resolve_launch(const scemc_ensemble* E, int lanes, int mode, int kernel,
   for (const scemc_tables* T : E->tabs) generic_ok = generic_ok && T->has_generic;
   if ((kernel == 2 || kernel == 3) && !E->fast)
     return fail(SCEMC_ERR_ARG, "the fast and replica-parallel kernels need lmax 1 or 2 and dense l in {1,2} "
-                               "programs of body <= 4 (l = 1 only for bodies 3 and 4), equal lmax across the batch");
+                               "programs of body <= 4 (l = 1 only for body 4; l in {1, 2} for body 3 when lmax = 2), equal lmax across the batch");
   if (kernel == 1 && !generic_ok) return fail(SCEMC_ERR_ARG, "generic records were not kept for these tables");
   if (kernel == 3 && mode == 2)
     return fail(SCEMC_ERR_ARG, "the replica-parallel kernel runs per-colour launches (mode 1 or 3)");
