@@ -193,8 +193,9 @@ typedef struct scemc_run_params {
   int64_t phase_done;
   int64_t phase_total;
   int32_t kernel;     /* 0 = auto, 1 = generic record walk, 2 = row-parallel fast kernel (one warp per
-                         item), 3 = replica-parallel kernel (one thread per item; per-colour launches,
-                         mode 1 or 3), 4 = chain-resident cluster kernel (one thread-block cluster per
+                         item), 3 = replica-parallel kernel (one thread per item; per-colour launches
+                         with mode 1 or 3, one persistent cooperative launch per pass with mode 2),
+                         4 = chain-resident cluster kernel (one thread-block cluster per
                          replica slot holds the replica's spins in shared memory; the row-parallel
                          arithmetic, bit for bit; one launch per compound sweep, mode 1 or 3; needs
                          n_sites x 16 bytes plus scratch within one block's shared memory) */

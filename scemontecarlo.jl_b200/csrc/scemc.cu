@@ -1500,7 +1500,7 @@ __device__ void rep_colour(const SweepArgs& a, int col, unsigned long long* s_dE
       if (!ok[k]) continue;
       const int r = g + k * G;
       const int slot = L.slot0 + r;
-      const float4 e = __ldg(sp + row0 + r);
+      const float4 e = PF ? __ldg(sp + row0 + r) : __ldcg(sp + row0 + r);
       const double beta = p_beta[slot];
       float px, py, pz;
       double u, lq = 0.0;
@@ -1905,6 +1905,30 @@ __global__ void __launch_bounds__(256, P == 1 ? 4 : SCEMC_REP_MINB_P2) k_rep_col
   zero_block(a.n_slots, s_dE, s_cnt);
   stage_params(a, zsm);
   rep_colour<LMAX, P, NP, PF>(a, a.colour, s_dE, s_cnt, zsm);
+  flush_block(a, s_dE, s_cnt);
+}
+
+// Persistent replica-parallel pass (mode 2 with kernel 3): one cooperative launch runs
+// the pass's proposal precompute (when requested) and every colour, with the bounded
+// grid barrier between them. Spins written by other blocks in earlier colours are
+// read through L2 (the non-prefetching form's loads), never from a stale L1 line.
+template <int LMAX, int P, int NP>
+__global__ void __launch_bounds__(256, P == 1 ? 4 : SCEMC_REP_MINB_P2) k_rep_persistent(SweepArgs a) {
+  extern __shared__ __align__(16) float zsm[];
+  __shared__ unsigned long long s_dE[kMaxSlots];
+  __shared__ unsigned int s_cnt[3 * kMaxSlots];
+  zero_block(a.n_slots, s_dE, s_cnt);
+  stage_params(a, zsm);
+  bool ok = true;
+  int k = 0;
+  if (a.pass < 0 && a.prop != nullptr) {
+    make_proposals<true>(a);
+    ok = grid_barrier(a.gs, a.bar_base, k++, gridDim.x, a.barrier_limit_ns);
+  }
+  for (int col = 0; ok && col < a.max_colors; ++col) {
+    rep_colour<LMAX, P, NP, false>(a, col, s_dE, s_cnt, zsm);
+    if (col + 1 < a.max_colors) ok = grid_barrier(a.gs, a.bar_base, k++, gridDim.x, a.barrier_limit_ns);
+  }
   flush_block(a, s_dE, s_cnt);
 }
 
@@ -3237,6 +3261,7 @@ int64_t rep_threads(const scemc_ensemble* E, int c, int P) {
 // measured 9 % faster on the PT ladders, 7 % slower at fcc 48^3 x 32).
 struct RepForm {
   int P;
+  int np;  // threads per item
   int64_t nt;
   int32_t pf;
   FastFn fn;
@@ -3253,6 +3278,7 @@ RepForm rep_form(const scemc_ensemble* E, int c, int forced, int forced_np = 0, 
   // NP depends on the colour's size only, so a forced P does not change the chains.
   const int NP = forced_np == 1 || forced_np == 2 ? forced_np : (2 * nt1 <= sms * 1024 ? 2 : 1);
   f.P = forced == 1 || forced == 2 ? forced : (NP == 2 ? 1 : 2);
+  f.np = NP;
   f.nt = rep_threads(E, c, f.P) * NP;
   f.pf = forced_pf == 1 ? 1 : forced_pf == 2 ? 0 : (f.nt <= sms * (f.P == 1 ? 1024 : 768) * 2 ? 1 : 0);
   // [lmax - 1][P - 1][NP - 1][pf]
@@ -3319,6 +3345,48 @@ int32_t run_learned_pass(scemc_ensemble* E, const Launch& Lc) {
   return SCEMC_OK;
 }
 
+// The persistent replica-parallel pass: its P and NP are the form rep_form picks for
+// the colour with the most items (or the forced ones); cooperative launch of at most
+// the co-resident blocks.
+int32_t run_rep_persistent(scemc_ensemble* E, SweepArgs a, const Launch& Lc) {
+  int cbig = 0;
+  for (int c = 0; c < E->max_colors; ++c)
+    if (E->seg[(size_t)c * (E->tabs.size() + 1) + E->tabs.size()] >
+        E->seg[(size_t)cbig * (E->tabs.size() + 1) + E->tabs.size()])
+      cbig = c;
+  const RepForm f = rep_form(E, cbig, Lc.rep_p, Lc.rep_np, 2);
+  const int NP = f.np;
+  using PFn = void (*)(SweepArgs);
+  static const PFn forms[2][2][2] = {{{k_rep_persistent<1, 1, 1>, k_rep_persistent<1, 1, 2>},
+                                      {k_rep_persistent<1, 2, 1>, k_rep_persistent<1, 2, 2>}},
+                                     {{k_rep_persistent<2, 1, 1>, k_rep_persistent<2, 1, 2>},
+                                      {k_rep_persistent<2, 2, 1>, k_rep_persistent<2, 2, 2>}}};
+  if (f.P != 1 && f.P != 2) return fail(SCEMC_ERR_ARG, "the persistent replica-parallel form takes 1 or 2 replicas per thread");
+  const PFn fn = forms[E->lmax == 1 ? 0 : 1][f.P - 1][NP - 1];
+  const int threads = 256;
+  const size_t smem = fast_param_floats(E->n_slots) * sizeof(float);
+  CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int key[4] = {3, E->lmax, f.P, NP};
+  if (!std::equal(key, key + 4, E->coop_key)) {
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, threads, smem));
+    if (per_sm < 1) return fail(SCEMC_ERR_CUDA, "persistent replica-parallel kernel cannot be resident");
+    E->coop_blocks = per_sm * sm_count(E->device);
+    std::copy(key, key + 4, E->coop_key);
+  }
+  int64_t need = 1;
+  for (int c = 0; c < E->max_colors; ++c) need = std::max<int64_t>(need, rep_threads(E, c, f.P) * NP);
+  need = (need + threads - 1) / threads;
+  if (a.prop) need = std::max<int64_t>(need, ((int64_t)E->item_base.back() + threads - 1) / threads);
+  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(E->coop_blocks, need));
+  a.bar_base = E->bar_base;
+  void* params[] = {&a};
+  ++E->launches;
+  CUDA_TRY(cudaLaunchCooperativeKernel((const void*)fn, dim3(blocks), dim3(threads), params, smem, E->stream));
+  E->bar_base += (unsigned long long)blocks * ((a.prop ? 1 : 0) + std::max(E->max_colors - 1, 0));
+  return SCEMC_OK;
+}
+
 int32_t run_pass_impl(scemc_ensemble* E, int pass, const Launch& Lc) {
   const int lmax = E->lmax;
   if (Lc.learned && pass < 0) return run_learned_pass(E, Lc);
@@ -3334,11 +3402,13 @@ int32_t run_pass_impl(scemc_ensemble* E, int pass, const Launch& Lc) {
       if ((rc = ensure_props(E))) return rc;
       a.prop = E->d_prop;
       a.propu = E->d_propu;
+      if (Lc.mode == 2) return run_rep_persistent(E, a, Lc);  // proposals inside the persistent launch
       const int blocks = (int)std::min<int64_t>(cap, ((int64_t)E->item_base.back() + 255) / 256);
       ++E->launches;
       k_proposals<<<std::max(blocks, 1), 256, 0, E->stream>>>(a);
       CUDA_TRY(cudaGetLastError());
     }
+    if (Lc.mode == 2) return run_rep_persistent(E, a, Lc);
     for (int c = 0; c < E->max_colors; ++c) {
       const int n = E->seg[(size_t)c * (E->tabs.size() + 1) + E->tabs.size()];
       if (n == 0) continue;
@@ -3735,8 +3805,6 @@ int32_t resolve_launch(const scemc_ensemble* E, int lanes, int mode, int kernel,
     return fail(SCEMC_ERR_ARG, "the fast and replica-parallel kernels need lmax 1 or 2 and dense l in {1,2} "
                                "programs of body <= 4 (l = 1 only for body 4; l in {1, 2} for body 3 when lmax = 2), equal lmax across the batch");
   if (kernel == 1 && !generic_ok) return fail(SCEMC_ERR_ARG, "generic records were not kept for these tables");
-  if (kernel == 3 && mode == 2)
-    return fail(SCEMC_ERR_ARG, "the replica-parallel kernel runs per-colour launches (mode 1 or 3)");
   // untuned auto choice: threads that carry replicas once every site has at least 16
   // of them and a colour holds enough items to fill the SMs (256 per SM)
   int min_r = 1 << 30;
@@ -4155,6 +4223,7 @@ int32_t scemc_batch_autotune(scemc_batch* b, int32_t or_per_metropolis, int32_t 
       for (int q : {1, 2}) cands.push_back({m, q, 0, 2});
     cands.push_back({4, 2, 0, 2});
     for (int q : {1, 2}) cands.push_back({3, q, 0, 3});
+    for (int q : {1, 2}) cands.push_back({2, q, 0, 3});
     if (cluster_fits(b) == SCEMC_OK)
       for (int q : {1, 2}) cands.push_back({3, q, 0, 4});
   } else {

@@ -472,7 +472,9 @@ def gpu_run_pt(gHs, *, temperature=None, kT=None, exchange: bool = True, exchang
     chains at their temperatures (run_mc with one chain per temperature).
 
     Seeds: a numpy Generator seeded with `seed` draws, in order, the initial spins of
-    every slot (uniform on S^2) and then one 64-bit device key per slot.
+    every slot (uniform on S^2) and then one 64-bit device key per slot. `init` replaces
+    the random start: one configuration (n_sites x 3) for every rung, or one direction
+    (3 values) for the uniform state of every table set.
 
     learned=(net, env) registers a learned proposal network (scemc.learned) with the
     batch; proposals=3 then draws every Metropolis proposal from it. The wall time
@@ -514,6 +516,8 @@ def gpu_run_pt(gHs, *, temperature=None, kT=None, exchange: bool = True, exchang
             configs += _random_configs(g.n_sites, R, rng)
         else:
             c = np.asarray(init, np.float64).reshape(-1, 3)
+            if c.shape[0] == 1:  # one direction: the uniform state of every table set
+                c = np.tile(c / np.linalg.norm(c), (g.n_sites, 1))
             configs += [c.copy() for _ in range(R)]
     seeds = rng.integers(0, 2 ** 64, size=R * len(gHs), dtype=np.uint64)
     batch = GPUBatch(gHs, [R] * len(gHs), configs, seeds, step)

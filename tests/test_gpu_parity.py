@@ -123,7 +123,7 @@ def check_pass(OH, cfg, rec, beta, kind, seed=None, sweep=None, step=None, orpas
     return int(tie[mism].sum()), int(att.sum()), n_sites
 
 
-NOT_FAST = {"mixed", "high_l"}  # programs outside the fast kinds (l = 0 / l >= 3 members)
+NOT_FAST = {"high_l"}  # programs outside the fast kinds (l >= 3 members)
 FAST = [m for m in MODELS if m not in NOT_FAST]
 
 # (model, lanes, mode, kernel, proposals): kernel 1 = generic record walk, 0 = auto
@@ -139,7 +139,8 @@ REPLAY_CASES = [(m, 4, 2, 1, 0) for m in MODELS] + [(m, 0, 2, 0, 1) for m in FAS
     ("mixed", 8, 3, 0, 0),
 ] + [(m, 0, 1, 3, 2) for m in FAST] + [("bcc_l2_plaq_zeeman", 0, 3, 3, 1), ("fcc_l2_tri_zeeman", 0, 3, 3, 2)] + [
     (m, 0, 4, 2, 2) for m in FAST] + [(m, 0, 1, 4, 2) for m in FAST] + [
-    ("bcc_l2_plaq_zeeman", 0, 3, 4, 1), ("fcc_l2_tri_zeeman", 0, 1, 4, 1), ("bcc_body4", 0, 3, 4, 2)]
+    ("bcc_l2_plaq_zeeman", 0, 3, 4, 1), ("fcc_l2_tri_zeeman", 0, 1, 4, 1), ("bcc_body4", 0, 3, 4, 2)] + [
+    (m, 0, 2, 3, 1 + (i % 2)) for i, m in enumerate(FAST)]
 
 
 @pytest.mark.parametrize("name,lanes,mode,kernel,proposals", REPLAY_CASES,
@@ -228,6 +229,30 @@ def test_rep_prefetch_changes_no_arithmetic(gpu, P, NP):
         outs.append((np.stack(st["configs"]), st["energies"].copy(), st["counters"].copy()))
     assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
     assert np.array_equal(outs[0][2], outs[1][2])
+
+
+@pytest.mark.parametrize("P,NP", [(1, 1), (1, 2), (2, 1), (2, 2)])
+def test_rep_persistent_equals_per_colour_launches(gpu, P, NP):
+    """The persistent replica-parallel pass (one cooperative launch per pass, bounded
+    grid barrier between colours, proposals precomputed inside it) gives chains bitwise
+    equal to the per-colour launches of the same form, on a batch of two lattices."""
+    w = models.config3_bcc_pt(sizes=(2, 3))
+    Hs = [scemc.TiledHamiltonian(2, w.terms, dims=(s_, s_, s_)) for s_ in (2, 3)]
+    gHs = [scemc.GPUTiledHamiltonian(H) for H in Hs]
+    cfgs = [rand_cfg(H.n_sites, 50 + i) for i, H in enumerate(Hs) for _ in range(3)]
+    betas = np.tile(1 / np.array([0.3e-3, 1e-3, 3e-3]), 2)
+    outs = []
+    for mode, prop in [(1, 1), (2, 1), (2, 2)]:
+        b = scemc.GPUBatch(gHs, [3, 3], cfgs, [90 + i for i in range(6)], 0.6)
+        b.set_betas(betas)
+        b.run(6, kernel=3, mode=mode, proposals=prop, rep_replicas=P, rep_threads_per_item=NP, rep_prefetch=2,
+              exchange=True, exchange_interval=1, phase_total=100)
+        st = b.download()
+        outs.append((np.concatenate([c.reshape(-1) for c in st["configs"]]), st["energies"].copy(),
+                     st["counters"].copy(), st["slot_of_rung"].copy()))
+    for o in outs[1:]:
+        for x, y in zip(o, outs[0]):
+            np.testing.assert_array_equal(x, y)
 
 
 def test_rep_forms_refuse_bad_values(gpu):
@@ -365,7 +390,7 @@ def test_cluster_kernel_refusals(gpu):
     b = scemc.GPUBatch([scemc.GPUTiledHamiltonian(H)], [1], [rand_cfg(H.n_sites, 1)], [1], 0.6)
     with pytest.raises(_lib.ScemcArgumentError):
         b.run(1, kernel=4, mode=2)
-    Hm, _ = build("mixed")  # no fast tables
+    Hm, _ = build("high_l")  # no fast tables (l = 3 and 4 members)
     bm = scemc.GPUBatch([scemc.GPUTiledHamiltonian(Hm)], [1], [rand_cfg(Hm.n_sites, 1)], [1], 0.6)
     with pytest.raises(_lib.ScemcArgumentError):
         bm.run(1, kernel=4)
@@ -383,8 +408,10 @@ def test_autotune_keeps_a_valid_launch_form(gpu):
     b.set_betas([1 / 0.002, 1 / 0.004, 1 / 0.008])
     t = b.autotune(or_per_metropolis=1, sweeps_per_trial=3)
     assert t["mode"] in (2, 3, 4) and t["proposals"] in (1, 2) and t["kernel"] in (2, 3, 4) and t["ms_per_sweep"] > 0
-    if t["kernel"] in (3, 4):
+    if t["kernel"] == 4:
         assert t["mode"] == 3
+    if t["kernel"] == 3:
+        assert t["mode"] in (2, 3)
     before = b.download()["counters"].copy()
     b.run(4, or_per_metropolis=1)  # mode 0 now uses the tuned form
     after = b.download()["counters"]
@@ -395,7 +422,7 @@ def test_autotune_keeps_a_valid_launch_form(gpu):
 
 
 def test_fast_kernel_refused_where_it_does_not_apply(gpu):
-    H, _ = build("mixed")
+    H, _ = build("high_l")
     gH = scemc.GPUTiledHamiltonian(H)
     b = scemc.GPUBatch([gH], [1], [rand_cfg(H.n_sites, 1)], [1], 0.6)
     with pytest.raises(_lib.ScemcArgumentError):
@@ -405,8 +432,7 @@ def test_fast_kernel_refused_where_it_does_not_apply(gpu):
     b.run(1, kernel=0)  # auto falls back to the generic record walk
     H2, _ = build("bcc_l2_plaq_zeeman")
     b2 = scemc.GPUBatch([scemc.GPUTiledHamiltonian(H2)], [1], [rand_cfg(H2.n_sites, 1)], [1], 0.6)
-    with pytest.raises(_lib.ScemcArgumentError):
-        b2.run(1, kernel=3, mode=2)  # the replica-parallel kernel has no persistent form
+    b2.run(1, kernel=3, mode=2)  # the replica-parallel kernel's persistent form
 
 
 def test_proposal_stream_is_the_reference_stream(gpu):
