@@ -1255,7 +1255,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_chain_cluster(SweepArgs 
 // many-wave form carries no per-load branch.
 // NP > 1: only the records j with j % NP == part (the one-body record with part 0),
 // for NP threads that share one site's walk.
-template <int LMAX, int P, int NP, bool PF>
+template <int LMAX, int P, int NP, bool PF, bool T2 = (LMAX == 2)>
 __device__ __forceinline__ void rep_coeffs(const DevLattice& L, const float4* __restrict__ sp, int4 dsc, int R, int G,
                                            int g, const bool (&ok)[P],
                                            float (&c)[P][(LMAX + 1) * (LMAX + 1) - 1], int part = 0) {
@@ -1340,7 +1340,7 @@ __device__ __forceinline__ void rep_coeffs(const DevLattice& L, const float4* __
     float4 v1[P], v2[P];
     gather((int)(rec.y & 0xffu), v1);
     gather((int)((rec.y >> 8) & 0xffu), v2);
-    if constexpr (NR == 8) {
+    if constexpr (NR == 8 && T2) {
       // merged body-3 block with l = 2 members: c_t += sum_p z1_p sum_q W[t][p][q] z2_q
       if ((rec.x >> kKindShift) == (uint32_t)F_TRIP2) {
         float y1[P][NR], y2[P][NR];
@@ -1448,7 +1448,7 @@ __device__ __forceinline__ void rep_coeffs(const DevLattice& L, const float4* __
 // NP = 2: two adjacent threads share an item's record walk (alternate records) and
 // add their halves with one shuffle; the even thread decides. For colours too small
 // to fill the GPU, where each thread's walk is the critical path.
-template <int LMAX, int P, int NP, bool PF>
+template <int LMAX, int P, int NP, bool PF, bool T2 = (LMAX == 2), int PK = -1>
 __device__ void rep_colour(const SweepArgs& a, int col, unsigned long long* s_dE, unsigned int* s_cnt,
                            const float* zsm) {
   constexpr int NR = (LMAX + 1) * (LMAX + 1) - 1;
@@ -1456,7 +1456,8 @@ __device__ void rep_colour(const SweepArgs& a, int col, unsigned long long* s_dE
   const double* p_beta = reinterpret_cast<const double*>(zsm);
   const double* p_step = p_beta + a.n_slots;
   const unsigned long long* p_seed = reinterpret_cast<const unsigned long long*>(p_step + a.n_slots);
-  const bool do_or = a.pass >= 0;
+  // PK: -1 the pass kind is read at run time; 0 a Metropolis pass, 1 an overrelaxation pass
+  const bool do_or = PK < 0 ? a.pass >= 0 : PK == 1;
   int n_threads = 0;  // threads of this colour over every lattice (G per site)
   for (int l = 0; l < a.n_lat; ++l) {
     const int R = a.lat[l].R;
@@ -1485,7 +1486,7 @@ __device__ void rep_colour(const SweepArgs& a, int col, unsigned long long* s_dE
 #pragma unroll
     for (int k = 0; k < P; ++k) ok[k] = g + k * G < R;
     float c[P][NR];
-    rep_coeffs<LMAX, P, NP, PF>(L, sp, dsc, R, G, g, ok, c, part);
+    rep_coeffs<LMAX, P, NP, PF, T2>(L, sp, dsc, R, G, g, ok, c, part);
     if (NP == 2) {
       const unsigned pair = 3u << (threadIdx.x & 30u);
 #pragma unroll
@@ -1897,14 +1898,17 @@ __global__ void __launch_bounds__(256, 2) k_learned_fused(SweepArgs a, LearnedNe
 #ifndef SCEMC_REP_MINB_P2
 #define SCEMC_REP_MINB_P2 3
 #endif
-template <int LMAX, int P, int NP, bool PF>
+#ifndef SCEMC_REP_SPLIT
+#define SCEMC_REP_SPLIT 0
+#endif
+template <int LMAX, int P, int NP, bool PF, bool T2 = (LMAX == 2), int PK = -1>
 __global__ void __launch_bounds__(256, P == 1 ? 4 : SCEMC_REP_MINB_P2) k_rep_colour(SweepArgs a) {
   extern __shared__ __align__(16) float zsm[];
   __shared__ unsigned long long s_dE[kMaxSlots];
   __shared__ unsigned int s_cnt[3 * kMaxSlots];
   zero_block(a.n_slots, s_dE, s_cnt);
   stage_params(a, zsm);
-  rep_colour<LMAX, P, NP, PF>(a, a.colour, s_dE, s_cnt, zsm);
+  rep_colour<LMAX, P, NP, PF, T2, PK>(a, a.colour, s_dE, s_cnt, zsm);
   flush_block(a, s_dE, s_cnt);
 }
 
@@ -1912,7 +1916,7 @@ __global__ void __launch_bounds__(256, P == 1 ? 4 : SCEMC_REP_MINB_P2) k_rep_col
 // the pass's proposal precompute (when requested) and every colour, with the bounded
 // grid barrier between them. Spins written by other blocks in earlier colours are
 // read through L2 (the non-prefetching form's loads), never from a stale L1 line.
-template <int LMAX, int P, int NP>
+template <int LMAX, int P, int NP, bool T2 = (LMAX == 2)>
 __global__ void __launch_bounds__(256, P == 1 ? 4 : SCEMC_REP_MINB_P2) k_rep_persistent(SweepArgs a) {
   extern __shared__ __align__(16) float zsm[];
   __shared__ unsigned long long s_dE[kMaxSlots];
@@ -1926,7 +1930,7 @@ __global__ void __launch_bounds__(256, P == 1 ? 4 : SCEMC_REP_MINB_P2) k_rep_per
     ok = grid_barrier(a.gs, a.bar_base, k++, gridDim.x, a.barrier_limit_ns);
   }
   for (int col = 0; ok && col < a.max_colors; ++col) {
-    rep_colour<LMAX, P, NP, false>(a, col, s_dE, s_cnt, zsm);
+    rep_colour<LMAX, P, NP, false, T2>(a, col, s_dE, s_cnt, zsm);
     if (col + 1 < a.max_colors) ok = grid_barrier(a.gs, a.bar_base, k++, gridDim.x, a.barrier_limit_ns);
   }
   flush_block(a, s_dE, s_cnt);
@@ -2178,6 +2182,7 @@ struct scemc_tables {
   int64_t bytes = 0;
   bool has_generic = true;
   int64_t fast_records = 0;
+  bool trip2 = false;  // the fast records hold body-3 blocks with l = 2 members
   ~scemc_tables() {
     for (void* p : allocs) cudaFree(p);
   }
@@ -2246,6 +2251,7 @@ struct scemc_ensemble {
   uint32_t* d_flags = nullptr;  // data-flow form: per item slot completion epochs
   // row-parallel fast kernel
   bool fast = false;
+  bool trip2 = false;  // some table has body-3 blocks with l = 2 members
   int32_t dmax = 0, rmax = 0;
   std::vector<int32_t> item_base;  // max_colors+1
   int32_t* d_item_base = nullptr;
@@ -2319,6 +2325,7 @@ struct FastBuild {
   std::vector<uint2> frec;
   std::vector<float> ft;
   int32_t dmax = 0, rmax = 0;
+  int64_t n_trip2 = 0;  // merged body-3 blocks with l = 2 members
 };
 
 // prog_l: per program, the l of its own member and of its other members in slot
@@ -2459,6 +2466,7 @@ bool build_fast(const scemc_tables_desc* d, const std::vector<int32_t>& prog_kin
       }
       if (off > kOffMask) return false;
       ++n_trip;
+      ++F.n_trip2;
       F.frec.push_back(make_uint2(((uint32_t)F_TRIP2 << kKindShift) | (uint32_t)off,
                                   (uint32_t)t.first.first | ((uint32_t)t.first.second << 8)));
     }
@@ -2772,6 +2780,7 @@ int32_t compile_tables(const scemc_tables_desc* d, scemc_tables* T) {
   }
   T->has_generic = keep_generic;
   T->fast_records = (int64_t)F.frec.size();
+  T->trip2 = F.n_trip2 > 0;
   T->color_ptr = cp;
   T->site_col_of.assign(ns, 0);
   for (int32_t c = 0; c < d->n_colors; ++c)
@@ -3013,6 +3022,7 @@ int32_t create_ensemble(int32_t n_tables, const scemc_tables* const* tables, con
   E->fast = true;
   for (int i = 0; i < n_tables; ++i) {
     E->fast = E->fast && tables[i]->dl.fast && tables[i]->lmax == E->lmax;
+    E->trip2 = E->trip2 || tables[i]->trip2;
     E->dmax = std::max(E->dmax, tables[i]->dl.dmax);
     E->rmax = std::max(E->rmax, tables[i]->dl.rmax);
   }
@@ -3266,7 +3276,7 @@ struct RepForm {
   int32_t pf;
   FastFn fn;
 };
-RepForm rep_form(const scemc_ensemble* E, int c, int forced, int forced_np = 0, int forced_pf = 0) {
+RepForm rep_form(const scemc_ensemble* E, int c, int forced, int forced_np = 0, int forced_pf = 0, int pass = -1) {
   RepForm f;
   const int64_t sms = sm_count(E->device);
   const int64_t nt1 = rep_threads(E, c, 1);
@@ -3282,16 +3292,32 @@ RepForm rep_form(const scemc_ensemble* E, int c, int forced, int forced_np = 0, 
   f.nt = rep_threads(E, c, f.P) * NP;
   f.pf = forced_pf == 1 ? 1 : forced_pf == 2 ? 0 : (f.nt <= sms * (f.P == 1 ? 1024 : 768) * 2 ? 1 : 0);
   // [lmax - 1][P - 1][NP - 1][pf]
-  static const FastFn forms[2][2][2][2] = {
+  // [0: lmax 1, 1: lmax 2 without body-3 l = 2 blocks, 2: lmax 2 with them][P - 1][NP - 1][pf]
+  // (the block walk costs registers, so tables without such blocks run instances without it)
+  static const FastFn forms[3][2][2][2] = {
       {{{k_rep_colour<1, 1, 1, false>, k_rep_colour<1, 1, 1, true>},
         {k_rep_colour<1, 1, 2, false>, k_rep_colour<1, 1, 2, true>}},
        {{k_rep_colour<1, 2, 1, false>, k_rep_colour<1, 2, 1, true>},
         {k_rep_colour<1, 2, 2, false>, k_rep_colour<1, 2, 2, true>}}},
-      {{{k_rep_colour<2, 1, 1, false>, k_rep_colour<2, 1, 1, true>},
-        {k_rep_colour<2, 1, 2, false>, k_rep_colour<2, 1, 2, true>}},
-       {{k_rep_colour<2, 2, 1, false>, k_rep_colour<2, 2, 1, true>},
-        {k_rep_colour<2, 2, 2, false>, k_rep_colour<2, 2, 2, true>}}}};
-  f.fn = forms[E->lmax == 1 ? 0 : 1][f.P - 1][NP - 1][f.pf];
+      {{{k_rep_colour<2, 1, 1, false, false>, k_rep_colour<2, 1, 1, true, false>},
+        {k_rep_colour<2, 1, 2, false, false>, k_rep_colour<2, 1, 2, true, false>}},
+       {{k_rep_colour<2, 2, 1, false, false>, k_rep_colour<2, 2, 1, true, false>},
+        {k_rep_colour<2, 2, 2, false, false>, k_rep_colour<2, 2, 2, true, false>}}},
+      {{{k_rep_colour<2, 1, 1, false, true>, k_rep_colour<2, 1, 1, true, true>},
+        {k_rep_colour<2, 1, 2, false, true>, k_rep_colour<2, 1, 2, true, true>}},
+       {{k_rep_colour<2, 2, 1, false, true>, k_rep_colour<2, 2, 1, true, true>},
+        {k_rep_colour<2, 2, 2, false, true>, k_rep_colour<2, 2, 2, true, true>}}}};
+  f.fn = forms[E->lmax == 1 ? 0 : (E->trip2 ? 2 : 1)][f.P - 1][NP - 1][f.pf];
+#if SCEMC_REP_SPLIT
+  // one instance per pass kind: the Metropolis and overrelaxation decisions compiled apart
+  static const FastFn formsk[2][3][2][2][2] = {{{{{k_rep_colour<1, 1, 1, false, false, 0>, k_rep_colour<1, 1, 1, true, false, 0>}, {k_rep_colour<1, 1, 2, false, false, 0>, k_rep_colour<1, 1, 2, true, false, 0>}}, {{k_rep_colour<1, 2, 1, false, false, 0>, k_rep_colour<1, 2, 1, true, false, 0>}, {k_rep_colour<1, 2, 2, false, false, 0>, k_rep_colour<1, 2, 2, true, false, 0>}}},
+       {{{k_rep_colour<2, 1, 1, false, false, 0>, k_rep_colour<2, 1, 1, true, false, 0>}, {k_rep_colour<2, 1, 2, false, false, 0>, k_rep_colour<2, 1, 2, true, false, 0>}}, {{k_rep_colour<2, 2, 1, false, false, 0>, k_rep_colour<2, 2, 1, true, false, 0>}, {k_rep_colour<2, 2, 2, false, false, 0>, k_rep_colour<2, 2, 2, true, false, 0>}}},
+       {{{k_rep_colour<2, 1, 1, false, true, 0>, k_rep_colour<2, 1, 1, true, true, 0>}, {k_rep_colour<2, 1, 2, false, true, 0>, k_rep_colour<2, 1, 2, true, true, 0>}}, {{k_rep_colour<2, 2, 1, false, true, 0>, k_rep_colour<2, 2, 1, true, true, 0>}, {k_rep_colour<2, 2, 2, false, true, 0>, k_rep_colour<2, 2, 2, true, true, 0>}}}},
+      {{{{k_rep_colour<1, 1, 1, false, false, 1>, k_rep_colour<1, 1, 1, true, false, 1>}, {k_rep_colour<1, 1, 2, false, false, 1>, k_rep_colour<1, 1, 2, true, false, 1>}}, {{k_rep_colour<1, 2, 1, false, false, 1>, k_rep_colour<1, 2, 1, true, false, 1>}, {k_rep_colour<1, 2, 2, false, false, 1>, k_rep_colour<1, 2, 2, true, false, 1>}}},
+       {{{k_rep_colour<2, 1, 1, false, false, 1>, k_rep_colour<2, 1, 1, true, false, 1>}, {k_rep_colour<2, 1, 2, false, false, 1>, k_rep_colour<2, 1, 2, true, false, 1>}}, {{k_rep_colour<2, 2, 1, false, false, 1>, k_rep_colour<2, 2, 1, true, false, 1>}, {k_rep_colour<2, 2, 2, false, false, 1>, k_rep_colour<2, 2, 2, true, false, 1>}}},
+       {{{k_rep_colour<2, 1, 1, false, true, 1>, k_rep_colour<2, 1, 1, true, true, 1>}, {k_rep_colour<2, 1, 2, false, true, 1>, k_rep_colour<2, 1, 2, true, true, 1>}}, {{k_rep_colour<2, 2, 1, false, true, 1>, k_rep_colour<2, 2, 1, true, true, 1>}, {k_rep_colour<2, 2, 2, false, true, 1>, k_rep_colour<2, 2, 2, true, true, 1>}}}}};
+  if (pass != -2) f.fn = formsk[pass >= 0 ? 1 : 0][E->lmax == 1 ? 0 : (E->trip2 ? 2 : 1)][f.P - 1][NP - 1][f.pf];
+#endif
   return f;
 }
 
@@ -3357,12 +3383,14 @@ int32_t run_rep_persistent(scemc_ensemble* E, SweepArgs a, const Launch& Lc) {
   const RepForm f = rep_form(E, cbig, Lc.rep_p, Lc.rep_np, 2);
   const int NP = f.np;
   using PFn = void (*)(SweepArgs);
-  static const PFn forms[2][2][2] = {{{k_rep_persistent<1, 1, 1>, k_rep_persistent<1, 1, 2>},
+  static const PFn forms[3][2][2] = {{{k_rep_persistent<1, 1, 1>, k_rep_persistent<1, 1, 2>},
                                       {k_rep_persistent<1, 2, 1>, k_rep_persistent<1, 2, 2>}},
-                                     {{k_rep_persistent<2, 1, 1>, k_rep_persistent<2, 1, 2>},
-                                      {k_rep_persistent<2, 2, 1>, k_rep_persistent<2, 2, 2>}}};
+                                     {{k_rep_persistent<2, 1, 1, false>, k_rep_persistent<2, 1, 2, false>},
+                                      {k_rep_persistent<2, 2, 1, false>, k_rep_persistent<2, 2, 2, false>}},
+                                     {{k_rep_persistent<2, 1, 1, true>, k_rep_persistent<2, 1, 2, true>},
+                                      {k_rep_persistent<2, 2, 1, true>, k_rep_persistent<2, 2, 2, true>}}};
   if (f.P != 1 && f.P != 2) return fail(SCEMC_ERR_ARG, "the persistent replica-parallel form takes 1 or 2 replicas per thread");
-  const PFn fn = forms[E->lmax == 1 ? 0 : 1][f.P - 1][NP - 1];
+  const PFn fn = forms[E->lmax == 1 ? 0 : (E->trip2 ? 2 : 1)][f.P - 1][NP - 1];
   const int threads = 256;
   const size_t smem = fast_param_floats(E->n_slots) * sizeof(float);
   CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -3413,7 +3441,7 @@ int32_t run_pass_impl(scemc_ensemble* E, int pass, const Launch& Lc) {
       const int n = E->seg[(size_t)c * (E->tabs.size() + 1) + E->tabs.size()];
       if (n == 0) continue;
       a.colour = c;
-      const RepForm f = rep_form(E, c, Lc.rep_p, Lc.rep_np, Lc.rep_pf);
+      const RepForm f = rep_form(E, c, Lc.rep_p, Lc.rep_np, Lc.rep_pf, pass);
       CUDA_TRY(cudaFuncSetAttribute((const void*)f.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       const int blocks = (int)std::min<int64_t>(cap, (f.nt + threads - 1) / threads);
       ++E->launches;
@@ -3882,8 +3910,9 @@ int32_t sweep_graph(scemc_ensemble* E, int n_or, const Launch& L, cudaGraphExec_
   if (L.rep) {
     const size_t smem = fast_param_floats(E->n_slots) * sizeof(float);
     for (int c = 0; c < E->max_colors; ++c)
-      CUDA_TRY(cudaFuncSetAttribute((const void*)rep_form(E, c, L.rep_p, L.rep_np, L.rep_pf).fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem));
+      for (int pass : {-1, 0})
+        CUDA_TRY(cudaFuncSetAttribute((const void*)rep_form(E, c, L.rep_p, L.rep_np, L.rep_pf, pass).fn,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   }
   const bool prof = E->profiling;
   E->profiling = false;  // graph launches are timed as a whole
