@@ -48,8 +48,10 @@ flushed before every step. Compare the default (merged dense body-3 records) wit
 --kernel 1 (the generic walk of the reference's sparse programs).
 
 --workload fcc_learned (the large frustrated configuration as specified): the fcc
-workload with the learned proposal. The network (18-site environment, 55 inputs) is
-trained on 200k environments from plain chains at the 32 kT values; then Metropolis
+workload with the learned proposal in field mode: the network reads each site's eight
+leave-one-out coefficients and kT (the couplings reach the fourth shell, beyond any
+raw-spin environment). It is trained on 200k sites from plain chains at the 32 kT
+values; then Metropolis
 + OR + exchange and learned Metropolis-Hastings + OR + exchange each run 1000
 thermalisation and --steps (default 4000) measured compound sweeps of the 32 rungs.
 The metric is tau_int-corrected samples/s, as for --workload learned.
@@ -220,11 +222,14 @@ def run_fcc_learned(args) -> int:
     w = models.config5_fcc(n=n, replicas=32)
     H = w.hamiltonians()[0]
     gH = scemc.GPUTiledHamiltonian(H)
-    env = learned.environment_table(models.FCC.positions, (n, n, n))
+    # field mode: the network reads each site's leave-one-out coefficients (8 numbers for
+    # lmax 2) and kT; the model's couplings reach the fourth shell (54 neighbours), which
+    # an environment of raw neighbour spins (at most 21 sites) cannot cover
     t0 = time.perf_counter()
-    X, Y = learned.collect_training_set(gH, env, w.kts, 200_000, sweeps_therm=1000, snapshots=4, spacing=50, seed=5)
+    X, Y = learned.collect_field_training_set(gH, w.kts, 200_000, sweeps_therm=1000, snapshots=4, spacing=50,
+                                              seed=5, or_per_metropolis=1)
     t1 = time.perf_counter()
-    net = learned.ProposalNet(seed=5, n_env=env.shape[1])
+    net = learned.ProposalNet(seed=5, field_rows=8)
     losses = net.train(X, Y, batch=1024, epochs=args.epochs, lr=1e-3, seed=5)
     torch.cuda.synchronize()
     t2 = time.perf_counter()
@@ -232,7 +237,7 @@ def run_fcc_learned(args) -> int:
     kw = dict(kT=w.kts, exchange=True, exchange_interval=1, or_per_metropolis=1, sweeps_therm=args.therm,
               sweeps_measure=measure, seed=5, kernel=3)
     plain = scemc.gpu_run_pt(gH, **kw)
-    lrn = scemc.gpu_run_pt(gH, learned=(net, env), proposals=3, **kw)
+    lrn = scemc.gpu_run_pt(gH, learned=(net, None), proposals=3, **kw)
     torch.cuda.synchronize()
     ess_p, _, tau_p = learned.ess_per_second(plain)
     ess_l, _, tau_l = learned.ess_per_second(lrn)

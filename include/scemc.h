@@ -290,6 +290,13 @@ int32_t scemc_energy_gradient(const scemc_tables* t, const double* config, int32
  * Metropolis proposal from the network's vMF mixture and accept it with
  * probability min(1, exp(-beta dE) q(e | env) / q(e' | env)). */
 int32_t scemc_batch_set_learned(scemc_batch* b, const scemc_mlp* m, const int32_t* env, int32_t k);
+/* Leave-one-out coefficients c_t of every site of a replica slot's current spins,
+ * rows 1..NR of the site's tesseral basis (NR = 3 for lmax 1, 8 for lmax 2), FP32,
+ * n_sites(table) x NR values; zeros for inactive sites. They fix each site's
+ * conditional distribution, exp(-beta sum_t c_t Z_t(e)), and are the inputs of a
+ * learned proposal in field mode (scemc_batch_set_learned with k = 0). Needs the fast
+ * tables. */
+int32_t scemc_batch_site_coeffs(scemc_batch* b, int32_t slot, float* c);
 /* log q(e | env) - log q(e' | env) of the recorded learned Metropolis pass (the
  * recorded replica; n_sites values, 0 where no learned proposal was recorded). */
 int32_t scemc_batch_fetch_record_ratio(const scemc_batch* b, double* lqr);

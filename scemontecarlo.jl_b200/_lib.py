@@ -105,6 +105,7 @@ SIGNATURES = [
     ("scemc_energy_gradient", C.c_int32, [C.c_void_p, F64P, C.c_int32, F64P]),
     ("scemc_batch_set_learned", C.c_int32, [C.c_void_p, C.c_void_p, I32P, C.c_int32]),
     ("scemc_batch_fetch_record_ratio", C.c_int32, [C.c_void_p, F64P]),
+    ("scemc_batch_site_coeffs", C.c_int32, [C.c_void_p, C.c_int32, F32P]),
     ("scemc_mlp_create", C.c_int32, [C.c_uint64, C.c_int32, C.POINTER(C.c_void_p)]),
     ("scemc_mlp_destroy", C.c_int32, [C.c_void_p]),
     ("scemc_mlp_get_params", C.c_int32, [C.c_void_p, F32P]),

@@ -1448,7 +1448,7 @@ __device__ __forceinline__ void rep_coeffs(const DevLattice& L, const float4* __
 // NP = 2: two adjacent threads share an item's record walk (alternate records) and
 // add their halves with one shuffle; the even thread decides. For colours too small
 // to fill the GPU, where each thread's walk is the critical path.
-template <int LMAX, int P, int NP, bool PF, bool T2 = (LMAX == 2), int PK = -1>
+template <int LMAX, int P, int NP, bool PF, bool T2 = (LMAX == 2)>
 __device__ void rep_colour(const SweepArgs& a, int col, unsigned long long* s_dE, unsigned int* s_cnt,
                            const float* zsm) {
   constexpr int NR = (LMAX + 1) * (LMAX + 1) - 1;
@@ -1456,8 +1456,7 @@ __device__ void rep_colour(const SweepArgs& a, int col, unsigned long long* s_dE
   const double* p_beta = reinterpret_cast<const double*>(zsm);
   const double* p_step = p_beta + a.n_slots;
   const unsigned long long* p_seed = reinterpret_cast<const unsigned long long*>(p_step + a.n_slots);
-  // PK: -1 the pass kind is read at run time; 0 a Metropolis pass, 1 an overrelaxation pass
-  const bool do_or = PK < 0 ? a.pass >= 0 : PK == 1;
+  const bool do_or = a.pass >= 0;
   int n_threads = 0;  // threads of this colour over every lattice (G per site)
   for (int l = 0; l < a.n_lat; ++l) {
     const int R = a.lat[l].R;
@@ -1656,7 +1655,10 @@ __device__ __forceinline__ void learned_layer(uint32_t tmem_d, const uint8_t* A,
 // e^-z is infinite and the quotient is 0, the function's limit.
 __device__ __forceinline__ float silu_fast(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 
-template <int LMAX, bool MH>
+// FIELD (with MH): the network reads the item's leave-one-out coefficients (rows 1..NR,
+// in meV) and kT instead of its environment spins; they fix the site's conditional
+// distribution whatever the range of the couplings.
+template <int LMAX, bool MH, bool FIELD = false>
 __global__ void __launch_bounds__(256, 2) k_learned_fused(SweepArgs a, LearnedNet net, double* lqr) {
   constexpr int NR = (LMAX + 1) * (LMAX + 1) - 1;
   extern __shared__ __align__(1024) uint8_t lsm[];
@@ -1763,10 +1765,26 @@ __global__ void __launch_bounds__(256, 2) k_learned_fused(SweepArgs a, LearnedNe
 #pragma unroll
     for (int t = 0; t < NR; ++t) cc[t] = c1[0][t];
   };
+  // FIELD: the network input row of an item from its two coefficient halves (warpgroup
+  // 1's half through shared memory, free between the last layer and the next tile's
+  // first): columns 0..NR-1 the coefficients in meV, column NR kT in meV.
+  auto field_input = [&](const Gather& g, const float (&cc)[NR]) {
+    __syncthreads();  // the previous use of sC (the decisions) is over
+    if (wg == 1)
+#pragma unroll
+      for (int t = 0; t < NR; ++t) sC[row * NR + t] = cc[t];
+    __syncthreads();
+    if (wg == 0) {
+#pragma unroll
+      for (int t = 0; t < NR; ++t) put(t, 1.0e3f * (cc[t] + sC[row * NR + t]));
+      put(NR, g.valid ? g.tau : 0.0f);
+    }
+  };
   Gather cur, nxt;
   gather(blockIdx.x, cur);
   float ccur[NR];  // MH: this warpgroup's half of the current tile's coefficients
   if (MH) coeffs(cur, ccur);
+  if (FIELD) field_input(cur, ccur);
   for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
     const int item = tile * kTile + row;
     const bool valid = cur.valid;
@@ -1882,6 +1900,7 @@ __global__ void __launch_bounds__(256, 2) k_learned_fused(SweepArgs a, LearnedNe
     };
     if (wg == 0 && valid && ok) draw_decide();
     if (MH && wg == 0) coeffs(cur, ccur);  // the next tile's half, after this tile's decisions
+    if (FIELD) field_input(cur, ccur);
   }
   if (!ok && tid == 0 && net.err) atomicExch(net.err, 1);
   if (MH) flush_block(a, s_dE, s_cnt);
@@ -1898,17 +1917,14 @@ __global__ void __launch_bounds__(256, 2) k_learned_fused(SweepArgs a, LearnedNe
 #ifndef SCEMC_REP_MINB_P2
 #define SCEMC_REP_MINB_P2 3
 #endif
-#ifndef SCEMC_REP_SPLIT
-#define SCEMC_REP_SPLIT 0
-#endif
-template <int LMAX, int P, int NP, bool PF, bool T2 = (LMAX == 2), int PK = -1>
+template <int LMAX, int P, int NP, bool PF, bool T2 = (LMAX == 2)>
 __global__ void __launch_bounds__(256, P == 1 ? 4 : SCEMC_REP_MINB_P2) k_rep_colour(SweepArgs a) {
   extern __shared__ __align__(16) float zsm[];
   __shared__ unsigned long long s_dE[kMaxSlots];
   __shared__ unsigned int s_cnt[3 * kMaxSlots];
   zero_block(a.n_slots, s_dE, s_cnt);
   stage_params(a, zsm);
-  rep_colour<LMAX, P, NP, PF, T2, PK>(a, a.colour, s_dE, s_cnt, zsm);
+  rep_colour<LMAX, P, NP, PF, T2>(a, a.colour, s_dE, s_cnt, zsm);
   flush_block(a, s_dE, s_cnt);
 }
 
@@ -1936,6 +1952,32 @@ __global__ void __launch_bounds__(256, P == 1 ? 4 : SCEMC_REP_MINB_P2) k_rep_per
   flush_block(a, s_dE, s_cnt);
 }
 
+
+// Leave-one-out coefficient rows 1..NR of every site of replica r of lattice li, one
+// thread per site through the replica-parallel walk (one replica per thread): the
+// learned proposal's field inputs for training. Inactive sites get zeros.
+template <int LMAX, bool T2>
+__global__ void __launch_bounds__(256) k_site_coeffs(const DevLattice* lat, int li, int r, const float4* spins,
+                                                     float* out) {
+  constexpr int NR = (LMAX + 1) * (LMAX + 1) - 1;
+  const DevLattice& L = lat[li];
+  const float4* sp = spins + L.spin_off;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < L.n_sites; s += gridDim.x * blockDim.x) {
+    float c[1][NR];
+#pragma unroll
+    for (int t = 0; t < NR; ++t) c[0][t] = 0.0f;
+    if (L.active[s]) {
+      const uint32_t cnt = L.fr_cnt[s];
+      const int nd = L.nb_ptr[s + 1] - L.nb_ptr[s];
+      const int4 dsc = make_int4(s | ((cnt >> 24) ? (int)(1u << 31) : 0), L.nb_ptr[s], L.fr_ptr[s],
+                                 (int32_t)((cnt & 0xffffffu) | ((uint32_t)nd << 24)));
+      const bool ok[1] = {true};
+      rep_coeffs<LMAX, 1, 1, false, T2>(L, sp, dsc, L.R, L.R, r, ok, c, 0);
+    }
+#pragma unroll
+    for (int t = 0; t < NR; ++t) out[(int64_t)s * NR + t] = c[0][t];
+  }
+}
 
 struct TailArgs {
   int32_t n_slots, n_rungs, n_lat;
@@ -2245,6 +2287,7 @@ struct scemc_ensemble {
   unsigned char* h_small = nullptr;     // pinned: flag, energies in, per-slot arrays out
   // learned proposal (network not owned)
   const scemc_mlp* mlp = nullptr;
+  bool learned_field = false;  // the network reads the site coefficients (set_learned with k = 0)
   std::vector<int32_t*> d_env;
   double* d_lqr = nullptr;
   double* d_rlqr = nullptr;
@@ -3240,7 +3283,10 @@ int max_colour_items(const scemc_ensemble* E) {
 // The fused learned kernel with the Metropolis-Hastings decision, and its dynamic
 // shared memory (the per-slot accumulators follow the network's tiles).
 using LearnedFn = void (*)(SweepArgs, LearnedNet, double*);
-LearnedFn learned_mh_kernel(int lmax) { return lmax == 1 ? k_learned_fused<1, true> : k_learned_fused<2, true>; }
+LearnedFn learned_mh_kernel(int lmax, bool field) {
+  if (field) return lmax == 1 ? k_learned_fused<1, true, true> : k_learned_fused<2, true, true>;
+  return lmax == 1 ? k_learned_fused<1, true> : k_learned_fused<2, true>;
+}
 size_t learned_smem(const scemc_ensemble* E, bool mh) {
   return kLearnedSmem + (mh ? (size_t)20 * E->n_slots + 16 : 0);
 }
@@ -3251,7 +3297,8 @@ int32_t prepare_learned(scemc_ensemble* E) {
   if (!E->d_lqr && (rc = dalloc(&E->d_lqr, (size_t)std::max<int32_t>(E->item_base.back(), 1)))) return rc;
   CUDA_TRY(cudaFuncSetAttribute((const void*)k_learned_fused<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)kLearnedSmem));
-  CUDA_TRY(cudaFuncSetAttribute((const void*)learned_mh_kernel(E->lmax), cudaFuncAttributeMaxDynamicSharedMemorySize,
+  CUDA_TRY(cudaFuncSetAttribute((const void*)learned_mh_kernel(E->lmax, E->learned_field),
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)learned_smem(E, true)));
   return SCEMC_OK;
 }
@@ -3276,7 +3323,7 @@ struct RepForm {
   int32_t pf;
   FastFn fn;
 };
-RepForm rep_form(const scemc_ensemble* E, int c, int forced, int forced_np = 0, int forced_pf = 0, int pass = -1) {
+RepForm rep_form(const scemc_ensemble* E, int c, int forced, int forced_np = 0, int forced_pf = 0) {
   RepForm f;
   const int64_t sms = sm_count(E->device);
   const int64_t nt1 = rep_threads(E, c, 1);
@@ -3291,7 +3338,6 @@ RepForm rep_form(const scemc_ensemble* E, int c, int forced, int forced_np = 0, 
   f.np = NP;
   f.nt = rep_threads(E, c, f.P) * NP;
   f.pf = forced_pf == 1 ? 1 : forced_pf == 2 ? 0 : (f.nt <= sms * (f.P == 1 ? 1024 : 768) * 2 ? 1 : 0);
-  // [lmax - 1][P - 1][NP - 1][pf]
   // [0: lmax 1, 1: lmax 2 without body-3 l = 2 blocks, 2: lmax 2 with them][P - 1][NP - 1][pf]
   // (the block walk costs registers, so tables without such blocks run instances without it)
   static const FastFn forms[3][2][2][2] = {
@@ -3308,16 +3354,6 @@ RepForm rep_form(const scemc_ensemble* E, int c, int forced, int forced_np = 0, 
        {{k_rep_colour<2, 2, 1, false, true>, k_rep_colour<2, 2, 1, true, true>},
         {k_rep_colour<2, 2, 2, false, true>, k_rep_colour<2, 2, 2, true, true>}}}};
   f.fn = forms[E->lmax == 1 ? 0 : (E->trip2 ? 2 : 1)][f.P - 1][NP - 1][f.pf];
-#if SCEMC_REP_SPLIT
-  // one instance per pass kind: the Metropolis and overrelaxation decisions compiled apart
-  static const FastFn formsk[2][3][2][2][2] = {{{{{k_rep_colour<1, 1, 1, false, false, 0>, k_rep_colour<1, 1, 1, true, false, 0>}, {k_rep_colour<1, 1, 2, false, false, 0>, k_rep_colour<1, 1, 2, true, false, 0>}}, {{k_rep_colour<1, 2, 1, false, false, 0>, k_rep_colour<1, 2, 1, true, false, 0>}, {k_rep_colour<1, 2, 2, false, false, 0>, k_rep_colour<1, 2, 2, true, false, 0>}}},
-       {{{k_rep_colour<2, 1, 1, false, false, 0>, k_rep_colour<2, 1, 1, true, false, 0>}, {k_rep_colour<2, 1, 2, false, false, 0>, k_rep_colour<2, 1, 2, true, false, 0>}}, {{k_rep_colour<2, 2, 1, false, false, 0>, k_rep_colour<2, 2, 1, true, false, 0>}, {k_rep_colour<2, 2, 2, false, false, 0>, k_rep_colour<2, 2, 2, true, false, 0>}}},
-       {{{k_rep_colour<2, 1, 1, false, true, 0>, k_rep_colour<2, 1, 1, true, true, 0>}, {k_rep_colour<2, 1, 2, false, true, 0>, k_rep_colour<2, 1, 2, true, true, 0>}}, {{k_rep_colour<2, 2, 1, false, true, 0>, k_rep_colour<2, 2, 1, true, true, 0>}, {k_rep_colour<2, 2, 2, false, true, 0>, k_rep_colour<2, 2, 2, true, true, 0>}}}},
-      {{{{k_rep_colour<1, 1, 1, false, false, 1>, k_rep_colour<1, 1, 1, true, false, 1>}, {k_rep_colour<1, 1, 2, false, false, 1>, k_rep_colour<1, 1, 2, true, false, 1>}}, {{k_rep_colour<1, 2, 1, false, false, 1>, k_rep_colour<1, 2, 1, true, false, 1>}, {k_rep_colour<1, 2, 2, false, false, 1>, k_rep_colour<1, 2, 2, true, false, 1>}}},
-       {{{k_rep_colour<2, 1, 1, false, false, 1>, k_rep_colour<2, 1, 1, true, false, 1>}, {k_rep_colour<2, 1, 2, false, false, 1>, k_rep_colour<2, 1, 2, true, false, 1>}}, {{k_rep_colour<2, 2, 1, false, false, 1>, k_rep_colour<2, 2, 1, true, false, 1>}, {k_rep_colour<2, 2, 2, false, false, 1>, k_rep_colour<2, 2, 2, true, false, 1>}}},
-       {{{k_rep_colour<2, 1, 1, false, true, 1>, k_rep_colour<2, 1, 1, true, true, 1>}, {k_rep_colour<2, 1, 2, false, true, 1>, k_rep_colour<2, 1, 2, true, true, 1>}}, {{k_rep_colour<2, 2, 1, false, true, 1>, k_rep_colour<2, 2, 1, true, true, 1>}, {k_rep_colour<2, 2, 2, false, true, 1>, k_rep_colour<2, 2, 2, true, true, 1>}}}}};
-  if (pass != -2) f.fn = formsk[pass >= 0 ? 1 : 0][E->lmax == 1 ? 0 : (E->trip2 ? 2 : 1)][f.P - 1][NP - 1][f.pf];
-#endif
   return f;
 }
 
@@ -3348,7 +3384,7 @@ int32_t run_learned_pass(scemc_ensemble* E, const Launch& Lc) {
     const unsigned grid = (unsigned)std::min(tiles, 2 * sm_count(E->device));
     ++E->launches;
     if (Lc.rep) {  // the replica-parallel decision runs inside the fused kernel
-      const auto fn = learned_mh_kernel(E->lmax);
+      const auto fn = learned_mh_kernel(E->lmax, E->learned_field);
       fn<<<grid, 256, learned_smem(E, true), E->stream>>>(a, net, E->d_lqr);
       CUDA_TRY(cudaGetLastError());
       continue;
@@ -3441,7 +3477,7 @@ int32_t run_pass_impl(scemc_ensemble* E, int pass, const Launch& Lc) {
       const int n = E->seg[(size_t)c * (E->tabs.size() + 1) + E->tabs.size()];
       if (n == 0) continue;
       a.colour = c;
-      const RepForm f = rep_form(E, c, Lc.rep_p, Lc.rep_np, Lc.rep_pf, pass);
+      const RepForm f = rep_form(E, c, Lc.rep_p, Lc.rep_np, Lc.rep_pf);
       CUDA_TRY(cudaFuncSetAttribute((const void*)f.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       const int blocks = (int)std::min<int64_t>(cap, (f.nt + threads - 1) / threads);
       ++E->launches;
@@ -3825,6 +3861,8 @@ int32_t resolve_launch(const scemc_ensemble* E, int lanes, int mode, int kernel,
     if (!E->mlp) return fail(SCEMC_ERR_ARG, "learned proposals need scemc_batch_set_learned first");
     if (!E->fast) return fail(SCEMC_ERR_ARG, "learned proposals need the fast tables (lmax 1 or 2 dense programs)");
     if (kernel == 1) return fail(SCEMC_ERR_ARG, "learned proposals run with kernel 2 or 3, not the generic walk");
+    if (E->learned_field && kernel != 3 && kernel != 0)
+      return fail(SCEMC_ERR_ARG, "a field-input learned proposal runs with kernel 3 (the fused decision)");
     if (mode == 2) return fail(SCEMC_ERR_ARG, "learned proposals run per-colour launches (mode 1 or 3)");
   }
   bool generic_ok = true;
@@ -3840,7 +3878,7 @@ int32_t resolve_launch(const scemc_ensemble* E, int lanes, int mode, int kernel,
   const bool rep_auto = E->fast && mode != 2 && min_r >= 16 &&
                         (int64_t)max_colour_items(E) >= (int64_t)sm_count(E->device) * 256;
   L.cluster = kernel == 4;
-  L.rep = kernel == 3 || (kernel == 0 && rep_auto);
+  L.rep = kernel == 3 || (kernel == 0 && (rep_auto || (proposals == 3 && E->learned_field)));
   L.fast = !L.rep && (kernel == 2 || kernel == 4 || (kernel == 0 && E->fast));
   L.learned = proposals == 3;
   L.mode = mode == 0 ? ((L.rep || L.learned || L.cluster) ? 1 : 2) : mode;
@@ -3911,7 +3949,7 @@ int32_t sweep_graph(scemc_ensemble* E, int n_or, const Launch& L, cudaGraphExec_
     const size_t smem = fast_param_floats(E->n_slots) * sizeof(float);
     for (int c = 0; c < E->max_colors; ++c)
       for (int pass : {-1, 0})
-        CUDA_TRY(cudaFuncSetAttribute((const void*)rep_form(E, c, L.rep_p, L.rep_np, L.rep_pf, pass).fn,
+        CUDA_TRY(cudaFuncSetAttribute((const void*)rep_form(E, c, L.rep_p, L.rep_np, L.rep_pf).fn,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   }
   const bool prof = E->profiling;
@@ -4553,6 +4591,29 @@ int32_t scemc_batch_fetch_record(const scemc_batch* b, int32_t pass, float* prop
   return SCEMC_OK;
 }
 
+int32_t scemc_batch_site_coeffs(scemc_batch* b, int32_t slot, float* c) {
+  if (!b || !c) return fail(SCEMC_ERR_ARG, "NULL argument");
+  if (!b->fast) return fail(SCEMC_ERR_ARG, "site coefficients need the fast tables (lmax 1 or 2 dense programs)");
+  if (slot < 0 || slot >= b->n_slots) return fail(SCEMC_ERR_ARG, "slot out of range");
+  int li = 0;
+  while (li + 1 < (int)b->tabs.size() && slot >= b->slot0[li + 1]) ++li;
+  const int r = slot - b->slot0[li];
+  const int NR = b->lmax == 1 ? 3 : 8;
+  const int64_t n = (int64_t)b->tabs[li]->n_sites * NR;
+  float* d_out = nullptr;
+  CUDA_TRY(cudaMalloc(&d_out, sizeof(float) * std::max<int64_t>(n, 1)));
+  const int blocks = (int)std::min<int64_t>(sm_count(b->device) * 8, (b->tabs[li]->n_sites + 255) / 256 + 1);
+  if (b->lmax == 1) k_site_coeffs<1, false><<<blocks, 256, 0, b->stream>>>(b->d_lat, li, r, b->d_spins, d_out);
+  else if (b->trip2) k_site_coeffs<2, true><<<blocks, 256, 0, b->stream>>>(b->d_lat, li, r, b->d_spins, d_out);
+  else k_site_coeffs<2, false><<<blocks, 256, 0, b->stream>>>(b->d_lat, li, r, b->d_spins, d_out);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(c, d_out, sizeof(float) * n, cudaMemcpyDeviceToHost, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  cudaFree(d_out);
+  if (e != cudaSuccess) return fail(SCEMC_ERR_CUDA, std::string("site coefficients: ") + cudaGetErrorString(e));
+  return SCEMC_OK;
+}
+
 int32_t scemc_batch_fetch_record_ratio(const scemc_batch* b, double* lqr) {
   if (!b || !b->d_rlqr || !lqr) return fail(SCEMC_ERR_ARG, "recording was never enabled");
   CUDA_TRY(cudaMemcpy(lqr, b->d_rlqr, sizeof(double) * b->tabs[b->rec_li]->n_sites, cudaMemcpyDeviceToHost));
@@ -4567,9 +4628,17 @@ int32_t scemc_batch_set_learned(scemc_batch* b, const scemc_mlp* m, const int32_
     if (p) cudaFree(p);
   b->d_env.assign(b->tabs.size(), nullptr);
   b->mlp = nullptr;
+  b->learned_field = false;
   for (auto& g : b->graphs) cudaGraphExecDestroy(g.exec);
   b->graphs.clear();
-  if (m) {
+  if (m && k == 0) {  // field mode: the inputs are the site's coefficients and kT
+    const int nr = b->lmax == 1 ? 3 : 8;
+    if (!b->fast) return fail(SCEMC_ERR_ARG, "a field-input learned proposal needs the fast tables");
+    if (m->n_in != nr + 1)
+      return fail(SCEMC_ERR_ARG, "a field-input network reads n_in = NR + 1 inputs (" + std::to_string(nr + 1) + ")");
+    b->mlp = m;
+    b->learned_field = true;
+  } else if (m) {
     if (!env) return fail(SCEMC_ERR_ARG, "env is NULL");
     if (k < 1 || k > 21 || m->n_in != 3 * k + 1)
       return fail(SCEMC_ERR_ARG, "the network reads n_in = 3 k + 1 inputs (k environment spins and kT, k <= 21)");
@@ -4596,7 +4665,7 @@ int32_t scemc_batch_set_learned(scemc_batch* b, const scemc_mlp* m, const int32_
   }
   for (size_t i = 0; i < lats.size(); ++i) {
     lats[i].env = b->d_env[i];
-    lats[i].env_k = m ? k : 0;
+    lats[i].env_k = m && !b->learned_field ? k : 0;
   }
   CUDA_TRY(h2d_sync(b->d_lat, lats.data(), sizeof(DevLattice) * lats.size()));
   return SCEMC_OK;

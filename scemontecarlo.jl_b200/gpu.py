@@ -352,6 +352,10 @@ class GPUBatch:
             check(_lib.lib().scemc_batch_set_learned(self.h, None, None, 14))
             self._net = None
             return
+        if net.n_env == 0:  # field mode: the network reads the site coefficients
+            check(_lib.lib().scemc_batch_set_learned(self.h, net.h, None, 0))
+            self._net = net
+            return
         tabs = env if isinstance(env, (list, tuple)) else [env]
         k = int(net.n_env)
         if any(np.asarray(e).reshape(-1).size != g.n_sites * k for e, g in zip(tabs, self.gHs)):
@@ -359,6 +363,22 @@ class GPUBatch:
         env = np.ascontiguousarray(np.concatenate([np.asarray(e, np.int32).reshape(-1) for e in tabs]), np.int32)
         check(_lib.lib().scemc_batch_set_learned(self.h, net.h, ptr(env, C.c_int32), k))
         self._net = net  # the batch does not own the network: keep it alive
+
+    def site_coeffs(self, slot: int) -> np.ndarray:
+        """Leave-one-out coefficients (rows 1..NR) of every site of a slot's current
+        spins, (n_sites, NR) float32 (scemc_batch_site_coeffs)."""
+        li = 0
+        off = 0
+        for i, r in enumerate(self.replicas):
+            if slot < off + r:
+                li = i
+                break
+            off += r
+        n = self.gHs[li].n_sites
+        nr = 3 if self.gHs[li].host.lmax == 1 else 8
+        out = np.zeros(n * nr, np.float32)
+        check(_lib.lib().scemc_batch_site_coeffs(self.h, int(slot), ptr(out, C.c_float)))
+        return out.reshape(n, nr)
 
     def fetch_record_ratio(self) -> np.ndarray:
         """log q(e|env) - log q(e'|env) of the recorded learned Metropolis pass."""

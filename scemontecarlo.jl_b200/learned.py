@@ -38,14 +38,23 @@ def pack(P: dict) -> np.ndarray:
 
 
 class ProposalNet:
-    """The learned proposal network (device resident) for environments of n_env spins:
-    n_in = 3 n_env + 1 inputs (the spins, then kT in meV)."""
+    """The learned proposal network (device resident). Environment mode: n_in = 3 n_env
+    + 1 inputs (n_env environment spins, then kT in meV). Field mode (field_rows = 3 for
+    lmax 1, 8 for lmax 2): n_in = field_rows + 1 inputs, the site's leave-one-out
+    coefficients in meV and kT in meV; they fix the site's conditional distribution
+    whatever the range of the couplings."""
 
-    def __init__(self, seed: int = 0, n_env: int = 14):
-        if not 1 <= n_env <= 21:
-            raise ValueError("n_env must be 1..21")
-        self.n_env = int(n_env)
-        self.n_in = 3 * self.n_env + 1
+    def __init__(self, seed: int = 0, n_env: int = 14, field_rows: int = 0):
+        if field_rows:
+            if field_rows not in (3, 8):
+                raise ValueError("field_rows must be 3 (lmax 1) or 8 (lmax 2)")
+            self.n_env = 0
+            self.n_in = int(field_rows) + 1
+        else:
+            if not 1 <= n_env <= 21:
+                raise ValueError("n_env must be 1..21")
+            self.n_env = int(n_env)
+            self.n_in = 3 * self.n_env + 1
         h = C.c_void_p()
         check(_lib.lib().scemc_mlp_create(int(seed) & (2 ** 64 - 1), self.n_in, C.byref(h)))
         self.h = h
@@ -244,6 +253,51 @@ def easy_axis(gH, n_dirs: int = 4096, rounds: int = 3) -> np.ndarray:
         best = cand[int(np.argmin(e))]
         width /= 8.0
     return best
+
+
+def collect_field_training_set(H, kts, n_rows: int, *, sweeps_therm: int = 2000, snapshots: int = 4,
+                               spacing: int = 50, seed: int = 0, kernel: int = 0, init=None,
+                               or_per_metropolis: int = 0):
+    """Field-mode training rows from plain-Metropolis chains, one per kT (one device
+    batch): after `sweeps_therm` adaptive-step sweeps, `snapshots` configurations
+    `spacing` sweeps apart; each row is a site's leave-one-out coefficients in meV
+    (scemc_batch_site_coeffs) and kT in meV, its target the site's spin.
+    Returns (X (n, NR + 1) float32, Y (n, 3) float32)."""
+    from .gpu import GPUBatch, GPUTiledHamiltonian
+    gH = H if isinstance(H, GPUTiledHamiltonian) else GPUTiledHamiltonian(H)
+    host = gH.host
+    rng = np.random.default_rng(seed)
+    R = len(kts)
+    if init is None:
+        cfgs = []
+        for _ in range(R):
+            v = rng.standard_normal((host.n_sites, 3))
+            cfgs.append(v / np.linalg.norm(v, axis=1, keepdims=True))
+    else:
+        c0 = np.asarray(init, np.float64).reshape(-1, 3)
+        if c0.shape[0] == 1:
+            c0 = np.tile(c0 / np.linalg.norm(c0), (host.n_sites, 1))
+        cfgs = [c0.copy() for _ in range(R)]
+    b = GPUBatch([gH], [R], cfgs, rng.integers(0, 2 ** 63, size=R).tolist(), 0.6)
+    b.set_betas(1.0 / np.asarray(kts))
+    b.run(sweeps_therm, adapt_interval=50, adapt_target=0.5, phase_total=sweeps_therm, kernel=kernel,
+          or_per_metropolis=or_per_metropolis)
+    per = int(np.ceil(n_rows / (R * snapshots)))
+    X, Y = [], []
+    for _ in range(snapshots):
+        b.run(spacing, kernel=kernel, or_per_metropolis=or_per_metropolis)
+        st = b.download()
+        for r in range(R):
+            slot = st["slot_of_rung"][r]
+            c = b.site_coeffs(slot)
+            cfg = np.asarray(st["configs"][slot])
+            sites = rng.choice(host.n_sites, size=per, replace=per > host.n_sites)
+            x = np.empty((per, c.shape[1] + 1), np.float32)
+            x[:, :-1] = 1.0e3 * c[sites]
+            x[:, -1] = kts[r] / MEV
+            X.append(x)
+            Y.append(cfg[sites].astype(np.float32))
+    return np.concatenate(X)[:n_rows], np.concatenate(Y)[:n_rows]
 
 
 def ess_per_second(result) -> tuple:

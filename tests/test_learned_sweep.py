@@ -304,3 +304,107 @@ def test_learned_dimer_is_exact_with_a_sharp_network(gpu, kernel):
     cnt = b.download()["counters"]
     acc = cnt[:, 0].sum() / cnt[:, 1].sum()
     assert 0.01 < acc < 0.9, acc
+
+
+def test_site_coeffs_match_the_oracle(gpu):
+    """scemc_batch_site_coeffs (the field-mode network inputs) against the oracle's
+    leave-one-out coefficients of the same spins, to the FP32 walk's accuracy."""
+    for lattice in ("bcc", "fcc"):
+        w, H, OH, _ = c4_small(4) if lattice == "bcc" else fcc_small(3)
+        gH = scemc.GPUTiledHamiltonian(H)
+        b = scemc.GPUBatch([gH], [2], [models.random_config(H.n_sites, 5), models.random_config(H.n_sites, 6)],
+                           [1, 2], 0.6)
+        for slot in (0, 1):
+            c = b.site_coeffs(slot).astype(np.float64)
+            cfg = b.download()["configs"][slot]
+            z = OH.zrows(cfg)
+            ref = np.array([OH.site_coeffs(s + 1, z)[1:] for s in range(H.n_sites)])
+            scale = np.abs(ref).sum(axis=1, keepdims=True) + 1e-30
+            assert np.max(np.abs(c - ref) / scale) < 1e-5, (lattice, slot)
+
+
+def test_learned_field_pass_replay(gpu):
+    """A field-mode learned pass (the network reads each item's coefficients in meV and
+    kT) on the fcc l <= 2 model, kernel 3: dE and the Hastings decisions at every site
+    (with the recorded density ratio), and the draws and the ratio recomputed from the
+    network on the oracle's coefficients (their BF16 rounding can differ from the
+    device's FP32 ones at a rounding boundary, so 99 % of the sites must match)."""
+    w, H, OH, _ = fcc_small(3)
+    gH = scemc.GPUTiledHamiltonian(H)
+    net = learned.ProposalNet(seed=3, field_rows=8)
+    seeds = [0xABC, 0xDEF]
+    kts = np.array([0.5, 1.5]) * MEV
+    b = scemc.GPUBatch([gH], [2], [models.random_config(H.n_sites, 1), models.random_config(H.n_sites, 2)], seeds,
+                       0.6)
+    b.set_betas(1.0 / kts)
+    b.set_learned(net, None)
+    beta = 1.0 / kts[0]
+    kt_mev = np.float32(1e3 / beta)
+    matched = total = 0
+    for sw in range(1, 4):
+        pre = b.download()["configs"][0].copy()
+        cfg = pre.copy()
+        b.record(True)
+        b.run(1, kernel=3, proposals=3, mode=1)
+        prop, u, dE32, flag = b.fetch_record(-1)
+        lqr = b.fetch_record_ratio()
+        assert np.all(flag != 3)
+        dE64, scale, _, c = OH.replay_sweep(cfg, prop.astype(np.float64), u, (flag == 1).astype(np.uint8), beta,
+                                            want_c=True)
+        np.testing.assert_array_equal(b.download()["configs"][0], cfg)
+        tol = 1e-5 * scale + 1e-30
+        assert np.all(np.abs(dE32.astype(np.float64) - dE64) <= tol)
+        la = -beta * dE64 + lqr
+        oacc = (la >= 0) | (u < np.exp(np.minimum(la, 0.0)))
+        tie = (np.abs(la - np.log(u)) <= beta * tol) | (np.abs(la) <= beta * tol)
+        assert not (((flag == 1) != oacc) & ~tie).any()
+        X = np.zeros((H.n_sites, 9), np.float32)
+        X[:, :8] = 1.0e3 * c[:, 1:]
+        X[:, 8] = kt_mev
+        out = np.zeros((H.n_sites, 32))
+        out[:, :20] = net.forward(X)
+        tau = np.full(H.n_sites, float(kt_mev))
+        lq_ref = LO.log_q(out, tau, pre) - LO.log_q(out, tau, prop.astype(np.float64))
+        for s in range(H.n_sites):
+            b0 = O.philox_block(seeds[0], s + 1, sw, 0, tag=4)
+            b1 = O.philox_block(seeds[0], s + 1, sw, 1, tag=4)
+            x, _ = LO.sample(out[s], float(kt_mev), O.philox_uniform(b0[0], b0[1]), O.philox_uniform(b0[2], b0[3]),
+                             O.philox_uniform(b1[0], b1[1]))
+            total += 1
+            if np.max(np.abs(prop[s] - x.astype(np.float32))) <= 3e-5 and abs(lqr[s] - lq_ref[s]) <= 2e-4:
+                matched += 1
+            assert u[s] == O.philox_uniform(b1[2], b1[3])
+    assert matched >= 0.99 * total, (matched, total)
+
+
+def test_learned_field_moments_in_a_field_are_exact(gpu):
+    """Field mode, moments in a field (vanishing bonds set the colouring): whatever the
+    untrained network proposes from the coefficients, Metropolis-Hastings samples
+    exp(-beta E): <E> per site = -h L(beta h)."""
+    n = 4
+    terms = models.heisenberg_pairs(models.BCC, [1e-12 * MEV, 1e-12 * MEV])
+    H = scemc.TiledHamiltonian(2, terms, dims=(n, n, n), magmoms=[2.0, 2.0], field=[0.0, 0.0, 1.0])
+    gH = scemc.GPUTiledHamiltonian(H)
+    up = np.tile([0.0, 0.0, 1.0], (H.n_sites, 1))
+    OH = O.OracleHamiltonian(2, terms, (n, n, n), magmoms=[2.0, 2.0], field=[0.0, 0.0, 1.0])
+    h = (OH.total_energy(-up) - OH.total_energy(up)) / (2 * H.n_sites)
+    net = learned.ProposalNet(seed=22, field_rows=3)
+    P = learned.unpack(net.params().copy())
+    P["W3"] *= 0.1
+    P["b3"][4:20:5] = -3.0
+    net.set_params(learned.pack(P))
+    R = 8
+    bh = 2.0
+    b = scemc.GPUBatch([gH], [R], [models.random_config(H.n_sites, 10 + r) for r in range(R)],
+                       list(range(200, 200 + R)), 0.6)
+    b.set_betas(np.full(R, bh / h))
+    b.set_learned(net, None)
+    b.run(200, proposals=3, kernel=3)
+    es = []
+    for _ in range(300):
+        b.run(5, proposals=3, kernel=3)
+        es.append(b.download()["energies"].copy())
+    es = np.asarray(es) / H.n_sites
+    m = es.mean()
+    err = es.mean(axis=0).std(ddof=1) / math.sqrt(R)
+    assert abs(m - (-h * langevin(bh))) < max(4 * err, 2e-3 * h), (m, -h * langevin(bh), err)
