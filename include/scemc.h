@@ -198,7 +198,11 @@ typedef struct scemc_run_params {
                          4 = chain-resident cluster kernel (one thread-block cluster per
                          replica slot holds the replica's spins in shared memory; the row-parallel
                          arithmetic, bit for bit; one launch per compound sweep, mode 1 or 3; needs
-                         n_sites x 16 bytes plus scratch within one block's shared memory) */
+                         n_sites x 16 bytes plus scratch within one block's shared memory),
+                         5 = replica-parallel kernel with the pair records on the tensor cores (lmax 2
+                         fast tables; one warp per site and 32 replicas, mma.sync TF32 with both
+                         operands split into a TF32 head and tail; mode 1 or 3, plain proposals; dE
+                         agrees with the FMA kernels' to rounding, not bit for bit) */
   int32_t proposals;  /* 0 = auto, 1 = precompute a pass's Metropolis proposals, 2 = inline, 3 = learned
                          network (scemc_batch_set_learned; kernels 2 or 3, per-colour modes 1 or 3) */
   int32_t rep_replicas; /* kernel 3: replicas per thread, 1 or 2; 0 = per colour launch, 1 when its

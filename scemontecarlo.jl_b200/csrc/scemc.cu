@@ -1254,8 +1254,9 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_chain_cluster(SweepArgs 
 // first and read through it (else through L2); a template parameter, so the
 // many-wave form carries no per-load branch.
 // NP > 1: only the records j with j % NP == part (the one-body record with part 0),
-// for NP threads that share one site's walk.
-template <int LMAX, int P, int NP, bool PF, bool T2 = (LMAX == 2)>
+// for NP threads that share one site's walk. PAIRS = false: every record but the
+// pair records (whose sum the caller forms on the tensor cores).
+template <int LMAX, int P, int NP, bool PF, bool T2 = (LMAX == 2), bool PAIRS = true>
 __device__ __forceinline__ void rep_coeffs(const DevLattice& L, const float4* __restrict__ sp, int4 dsc, int R, int G,
                                            int g, const bool (&ok)[P],
                                            float (&c)[P][(LMAX + 1) * (LMAX + 1) - 1], int part = 0) {
@@ -1327,7 +1328,7 @@ __device__ __forceinline__ void rep_coeffs(const DevLattice& L, const float4* __
     }
   };
 #pragma unroll 1
-  for (int j = part; j < n_pair; j += NP) {
+  for (int j = part; PAIRS && j < n_pair; j += NP) {
     const uint2 rec = __ldg(fr + j);
     float4 v[P];
     gather((int)(rec.y & 0xffu), v);
@@ -1445,6 +1446,90 @@ __device__ __forceinline__ void rep_coeffs(const DevLattice& L, const float4* __
   }
 }
 
+// One replica of a replica-parallel item: the proposal (precomputed, keyed inline or
+// the overrelaxation reflection about the site's l = 1 field), dE = c . (znew - zold),
+// the Metropolis (or Metropolis-Hastings) test, the write-back, the counters and the
+// record. c holds the replica's leave-one-out coefficients.
+template <int NR, bool PF>
+__device__ __forceinline__ void rep_decide(const SweepArgs& a, const DevLattice& L, int li, int col,
+                                           const int32_t* seg_c, int q, int s, int64_t row0, int r,
+                                           const float (&c)[NR], const double* p_beta, const double* p_step,
+                                           const unsigned long long* p_seed, unsigned long long* s_dE,
+                                           unsigned int* s_cnt) {
+  const bool do_or = a.pass >= 0;
+  const float4* __restrict__ sp = a.spins + L.spin_off;
+  const int slot = L.slot0 + r;
+  const float4 e = PF ? __ldg(sp + row0 + r) : __ldcg(sp + row0 + r);
+  const double beta = p_beta[slot];
+  float px, py, pz;
+  double u, lq = 0.0;
+  bool attempted = true;
+  if (!do_or) {
+    if (a.prop != nullptr) {
+      const int idx = a.item_base[col] + seg_c[li] + q * L.R + r;
+      const float4 p4 = a.prop[idx];
+      px = p4.x, py = p4.y, pz = p4.z;
+      u = a.propu[idx];
+      if (a.lqr != nullptr) lq = a.lqr[idx];
+    } else {
+      u = keyed_proposal(p_seed[slot], (uint32_t)(s + 1), a.st->sweep + 1u, e.x, e.y, e.z, p_step[slot], px, py,
+                         pz);
+    }
+  } else {
+    // reflection about h = (c4, c2, c3) = rows (3, 1, 2)
+    const double h0 = c[2], h1 = c[0], h2 = c[1];
+    const double hn = sqrt((h0 * h0 + h1 * h1) + h2 * h2);
+    if (hn < 1e-12) {
+      attempted = false;
+      px = e.x, py = e.y, pz = e.z;
+    } else {
+      const double a0 = h0 / hn, a1 = h1 / hn, a2 = h2 / hn;
+      const double d2 = 2.0 * (((double)e.x * a0 + (double)e.y * a1) + (double)e.z * a2);
+      const double r0 = d2 * a0 - e.x, r1 = d2 * a1 - e.y, r2 = d2 * a2 - e.z;
+      const double rn = sqrt((r0 * r0 + r1 * r1) + r2 * r2);
+      px = (float)(r0 / rn);
+      py = (float)(r1 / rn);
+      pz = (float)(r2 / rn);
+    }
+    const Blk bk = philox_block(p_seed[slot], (uint32_t)(s + 1), a.st->sweep + 1u, (uint32_t)a.pass, kTagOR);
+    u = philox_uniform(bk.w0, bk.w1);
+  }
+  float zo[NR], zn[NR];
+  zrow_nr<NR>(e.x, e.y, e.z, zo);
+  zrow_nr<NR>(px, py, pz, zn);
+  float term = 0.0f;
+#pragma unroll
+  for (int t = 0; t < NR; ++t) term = fmaf(c[t], zn[t] - zo[t], term);
+  const float dE = attempted ? term : 0.0f;
+  bool acc_ok;
+  if (!do_or && a.lqr != nullptr) {  // Metropolis-Hastings with the learned proposal's density ratio
+    const double la = -beta * (double)dE + lq;
+    acc_ok = la >= 0.0 || u < exp(la);
+  } else {
+    acc_ok = attempted && (dE <= 0.0f || u < exp(-beta * (double)dE));
+  }
+  if (acc_ok) {
+    a.spins[L.spin_off + row0 + r] = make_float4(px, py, pz, 0.0f);
+    atomicAdd(s_dE + slot, (unsigned long long)llrint((double)dE * kFixScale));
+  }
+  if (do_or) {
+    if (attempted) atomicAdd(s_cnt + 3 * slot + 2, 1u);
+    if (acc_ok) atomicAdd(s_cnt + 3 * slot + 1, 1u);
+  } else if (acc_ok) {
+    atomicAdd(s_cnt + 3 * slot + 0, 1u);
+  }
+  if (a.rec_prop != nullptr && li == a.rec_li && r == a.rec_r && a.pass + 1 < kRecPasses) {
+    const int64_t qq = (int64_t)(a.pass + 1) * a.rec_cap + s;
+    a.rec_prop[3 * qq + 0] = px;
+    a.rec_prop[3 * qq + 1] = py;
+    a.rec_prop[3 * qq + 2] = pz;
+    a.rec_u[qq] = u;
+    a.rec_dE[qq] = dE;
+    a.rec_acc[qq] = (uint8_t)(acc_ok ? 1 : (attempted ? 0 : 2));
+    if (a.rec_lqr != nullptr && !do_or) a.rec_lqr[s] = lq;
+  }
+}
+
 // NP = 2: two adjacent threads share an item's record walk (alternate records) and
 // add their halves with one shuffle; the even thread decides. For colours too small
 // to fill the GPU, where each thread's walk is the critical path.
@@ -1496,80 +1581,9 @@ __device__ void rep_colour(const SweepArgs& a, int col, unsigned long long* s_dE
     }
     // per replica: proposal, dE, decision, write-back
 #pragma unroll
-    for (int k = 0; k < P; ++k) {
-      if (!ok[k]) continue;
-      const int r = g + k * G;
-      const int slot = L.slot0 + r;
-      const float4 e = PF ? __ldg(sp + row0 + r) : __ldcg(sp + row0 + r);
-      const double beta = p_beta[slot];
-      float px, py, pz;
-      double u, lq = 0.0;
-      bool attempted = true;
-      if (!do_or) {
-        if (a.prop != nullptr) {
-          const int idx = a.item_base[col] + seg_c[li] + q * R + r;
-          const float4 p4 = a.prop[idx];
-          px = p4.x, py = p4.y, pz = p4.z;
-          u = a.propu[idx];
-          if (a.lqr != nullptr) lq = a.lqr[idx];
-        } else {
-          u = keyed_proposal(p_seed[slot], (uint32_t)(s + 1), a.st->sweep + 1u, e.x, e.y, e.z, p_step[slot], px, py,
-                             pz);
-        }
-      } else {
-        // reflection about h = (c4, c2, c3) = rows (3, 1, 2)
-        const double h0 = c[k][2], h1 = c[k][0], h2 = c[k][1];
-        const double hn = sqrt((h0 * h0 + h1 * h1) + h2 * h2);
-        if (hn < 1e-12) {
-          attempted = false;
-          px = e.x, py = e.y, pz = e.z;
-        } else {
-          const double a0 = h0 / hn, a1 = h1 / hn, a2 = h2 / hn;
-          const double d2 = 2.0 * (((double)e.x * a0 + (double)e.y * a1) + (double)e.z * a2);
-          const double r0 = d2 * a0 - e.x, r1 = d2 * a1 - e.y, r2 = d2 * a2 - e.z;
-          const double rn = sqrt((r0 * r0 + r1 * r1) + r2 * r2);
-          px = (float)(r0 / rn);
-          py = (float)(r1 / rn);
-          pz = (float)(r2 / rn);
-        }
-        const Blk bk = philox_block(p_seed[slot], (uint32_t)(s + 1), a.st->sweep + 1u, (uint32_t)a.pass, kTagOR);
-        u = philox_uniform(bk.w0, bk.w1);
-      }
-      float zo[NR], zn[NR];
-      zrow_nr<NR>(e.x, e.y, e.z, zo);
-      zrow_nr<NR>(px, py, pz, zn);
-      float term = 0.0f;
-#pragma unroll
-      for (int t = 0; t < NR; ++t) term = fmaf(c[k][t], zn[t] - zo[t], term);
-      const float dE = attempted ? term : 0.0f;
-      bool acc_ok;
-      if (!do_or && a.lqr != nullptr) {  // Metropolis-Hastings with the learned proposal's density ratio
-        const double la = -beta * (double)dE + lq;
-        acc_ok = la >= 0.0 || u < exp(la);
-      } else {
-        acc_ok = attempted && (dE <= 0.0f || u < exp(-beta * (double)dE));
-      }
-      if (acc_ok) {
-        a.spins[L.spin_off + row0 + r] = make_float4(px, py, pz, 0.0f);
-        atomicAdd(s_dE + slot, (unsigned long long)llrint((double)dE * kFixScale));
-      }
-      if (do_or) {
-        if (attempted) atomicAdd(s_cnt + 3 * slot + 2, 1u);
-        if (acc_ok) atomicAdd(s_cnt + 3 * slot + 1, 1u);
-      } else if (acc_ok) {
-        atomicAdd(s_cnt + 3 * slot + 0, 1u);
-      }
-      if (a.rec_prop != nullptr && li == a.rec_li && r == a.rec_r && a.pass + 1 < kRecPasses) {
-        const int64_t qq = (int64_t)(a.pass + 1) * a.rec_cap + s;
-        a.rec_prop[3 * qq + 0] = px;
-        a.rec_prop[3 * qq + 1] = py;
-        a.rec_prop[3 * qq + 2] = pz;
-        a.rec_u[qq] = u;
-        a.rec_dE[qq] = dE;
-        a.rec_acc[qq] = (uint8_t)(acc_ok ? 1 : (attempted ? 0 : 2));
-        if (a.rec_lqr != nullptr && !do_or) a.rec_lqr[s] = lq;
-      }
-    }
+    for (int k = 0; k < P; ++k)
+      if (ok[k])
+        rep_decide<NR, PF>(a, L, li, col, seg_c, q, s, row0, g + k * G, c[k], p_beta, p_step, p_seed, s_dE, s_cnt);
   }
 }
 
@@ -1925,6 +1939,171 @@ __global__ void __launch_bounds__(256, P == 1 ? 4 : SCEMC_REP_MINB_P2) k_rep_col
   zero_block(a.n_slots, s_dE, s_cnt);
   stage_params(a, zsm);
   rep_colour<LMAX, P, NP, PF, T2>(a, a.colour, s_dE, s_cnt, zsm);
+  flush_block(a, s_dE, s_cnt);
+}
+
+// ---------------------------------------------------------------------------
+// Replica-parallel pass with the pair records on the tensor cores (lmax 2, kernel 5).
+// A warp owns one site and 32 of its replicas. The pair records' share of the
+// coefficients, c[rep][i] = sum_rec sum_j W_rec[i][j] z_j(nb_rec, rep), is the product
+// of a (replicas x 8K) matrix of neighbour Z rows with the (8K x 8) stack of the
+// site's K coupling blocks. It runs as mma.sync m16n8k8 TF32 over groups of eight
+// records: for component j, K indexes the group's eight records, the A operand holds
+// z_j of their neighbours for 16 replicas and the B operand holds column j of their
+// blocks. A lane's A values over the eight components are then four whole Z rows
+// (two neighbours x two replicas per 16-replica tile), which it computes from the
+// spins it loads, so no operand moves between lanes; its B values are row g of two
+// blocks. FP32 accuracy comes from splitting both operands (x = hi + lo, hi = x
+// rounded to TF32) and summing hi.hi + hi.lo + lo.hi: about 2^-21 relative per
+// product. After the last group the accumulators pass through shared memory to
+// lane = replica; the lane adds its triplet, quad and one-body records (FP32 FMAs,
+// as the replica-parallel kernel) and decides. The sums run in another order than
+// the FMA kernels', so the chains agree with theirs to rounding, not bit for bit.
+// ---------------------------------------------------------------------------
+constexpr int kTcRowFloats = 12;  // a row of the 32 x 8 coefficient tile: 16-byte aligned, no bank conflicts
+
+__host__ __device__ __forceinline__ size_t tc_warp_floats(int dmax, int rmax) {
+  return fast_rec_floats(rmax) + fast_nbid_words(dmax) + 32 * kTcRowFloats;
+}
+
+__device__ __forceinline__ uint32_t tf32_rna(float x) {
+  uint32_t h;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
+  return h;
+}
+
+// d += a . b: one m16n8k8 product, TF32 operands, FP32 accumulators
+__device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         uint32_t b0, uint32_t b1) {
+  asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+      "{%0, %1, %2, %3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+template <bool T2>
+__global__ void __launch_bounds__(256, 2) k_rep_tc(SweepArgs a) {
+  constexpr int NR = 8;
+  extern __shared__ __align__(16) float zsm[];
+  __shared__ unsigned long long s_dE[kMaxSlots];
+  __shared__ unsigned int s_cnt[3 * kMaxSlots];
+  zero_block(a.n_slots, s_dE, s_cnt);
+  stage_params(a, zsm);
+  const int col = a.colour;
+  const int32_t* seg_c = a.seg + (size_t)col * (a.n_lat + 1);
+  const double* p_beta = reinterpret_cast<const double*>(zsm);
+  const double* p_step = p_beta + a.n_slots;
+  const unsigned long long* p_seed = reinterpret_cast<const unsigned long long*>(p_step + a.n_slots);
+  const bool do_or = a.pass >= 0;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;  // fragment row group and column of this lane
+  float* wbase = zsm + fast_param_floats(a.n_slots) + (size_t)wib * tc_warp_floats(a.dmax, a.rmax);
+  uint2* rb = reinterpret_cast<uint2*>(wbase);
+  int* nbid = reinterpret_cast<int*>(wbase + fast_rec_floats(a.rmax));
+  float* tile = wbase + fast_rec_floats(a.rmax) + fast_nbid_words(a.dmax);
+  int n_items = 0;  // (site, 32-replica chunk) items of this colour over every lattice
+  for (int l = 0; l < a.n_lat; ++l) {
+    const int R = a.lat[l].R;
+    n_items += (seg_c[l + 1] - seg_c[l]) / R * ((R + 31) >> 5);
+  }
+  const int n_warps = gridDim.x * (blockDim.x >> 5);
+  for (int w = blockIdx.x * (blockDim.x >> 5) + wib; w < n_items; w += n_warps) {  // warp-uniform
+    int li = 0, base = 0, R = 1, nch = 1;
+    for (; li < a.n_lat; ++li) {
+      R = a.lat[li].R;
+      nch = (R + 31) >> 5;
+      const int ni = (seg_c[li + 1] - seg_c[li]) / R * nch;
+      if (w < base + ni) break;
+      base += ni;
+    }
+    const DevLattice& L = a.lat[li];
+    const int q = (w - base) / nch;
+    const int r0 = ((w - base) - q * nch) * 32;
+    const int4 dsc = __ldg(L.idesc + __ldg(L.color_ptr + col) + q);
+    if (do_or && !(dsc.x & (1 << 30))) continue;  // no l = 1 channel
+    const int s = dsc.x & 0x3fffffff;
+    const uint32_t cnt = (uint32_t)dsc.w;
+    const int n_pair = (int)(cnt & 0xffu);
+    const int nd = (int)(cnt >> 24);
+    const float4* __restrict__ sp = a.spins + L.spin_off;
+    __syncwarp();  // the previous item's readers of rb, nbid and the tile are done
+    for (int k = lane; k < n_pair; k += 32) rb[k] = __ldg(L.frec + dsc.z + k);
+    for (int k = lane; k < nd; k += 32) nbid[k] = __ldg(L.nb_list + dsc.y + k);
+    __syncwarp();
+    float acc[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+#pragma unroll 1
+    for (int j0 = 0; j0 < n_pair; j0 += 8) {
+      // this lane's K columns: records j0 + t and j0 + t + 4 (zero blocks past the last)
+      const int k1 = j0 + t, k2 = k1 + 4;
+      const bool v1 = k1 < n_pair, v2 = k2 < n_pair;
+      const uint2 rc1 = rb[v1 ? k1 : 0], rc2 = rb[v2 ? k2 : 0];
+      const int nb1 = nbid[rc1.y & 0xffu], nb2 = nbid[rc2.y & 0xffu];
+      uint32_t b1h[NR], b1l[NR], b2h[NR], b2l[NR];
+      {
+        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4* w1 = reinterpret_cast<const float4*>(L.ftensor + (rc1.x & kOffMask)) + 2 * g;
+        const float4* w2 = reinterpret_cast<const float4*>(L.ftensor + (rc2.x & kOffMask)) + 2 * g;
+        const float4 p0 = v1 ? __ldg(w1) : z4, p1 = v1 ? __ldg(w1 + 1) : z4;
+        const float4 q0 = v2 ? __ldg(w2) : z4, q1 = v2 ? __ldg(w2 + 1) : z4;
+        const float x1[NR] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
+        const float x2[NR] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+#pragma unroll
+        for (int m = 0; m < NR; ++m) {
+          b1h[m] = tf32_rna(x1[m]);
+          b1l[m] = __float_as_uint(x1[m] - __uint_as_float(b1h[m]));
+          b2h[m] = tf32_rna(x2[m]);
+          b2l[m] = __float_as_uint(x2[m] - __uint_as_float(b2h[m]));
+        }
+      }
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt) {
+        // rows g and g + 8 of this 16-replica tile
+        const int ra = r0 + 16 * mt + g, rc = ra + 8;
+        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 s0 = v1 && ra < R ? __ldcg(sp + (int64_t)nb1 * R + ra) : z4;
+        const float4 s1 = v1 && rc < R ? __ldcg(sp + (int64_t)nb1 * R + rc) : z4;
+        const float4 s2 = v2 && ra < R ? __ldcg(sp + (int64_t)nb2 * R + ra) : z4;
+        const float4 s3 = v2 && rc < R ? __ldcg(sp + (int64_t)nb2 * R + rc) : z4;
+        float z0[NR], z1[NR], z2[NR], z3[NR];
+        zrow_nr<NR>(s0.x, s0.y, s0.z, z0);
+        zrow_nr<NR>(s1.x, s1.y, s1.z, z1);
+        zrow_nr<NR>(s2.x, s2.y, s2.z, z2);
+        zrow_nr<NR>(s3.x, s3.y, s3.z, z3);
+#pragma unroll
+        for (int j = 0; j < NR; ++j) {
+          const uint32_t h0 = tf32_rna(z0[j]), h1 = tf32_rna(z1[j]), h2 = tf32_rna(z2[j]), h3 = tf32_rna(z3[j]);
+          const uint32_t l0 = __float_as_uint(z0[j] - __uint_as_float(h0));
+          const uint32_t l1 = __float_as_uint(z1[j] - __uint_as_float(h1));
+          const uint32_t l2 = __float_as_uint(z2[j] - __uint_as_float(h2));
+          const uint32_t l3 = __float_as_uint(z3[j] - __uint_as_float(h3));
+          mma_tf32(acc[mt], l0, l1, l2, l3, b1h[j], b2h[j]);
+          mma_tf32(acc[mt], h0, h1, h2, h3, b1l[j], b2l[j]);
+          mma_tf32(acc[mt], h0, h1, h2, h3, b1h[j], b2h[j]);
+        }
+      }
+    }
+    // accumulator fragments (rows g, g + 8; columns 2t, 2t + 1) to lane = replica
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {
+      float* ta = tile + (16 * mt + g) * kTcRowFloats + 2 * t;
+      *reinterpret_cast<float2*>(ta) = make_float2(acc[mt][0], acc[mt][1]);
+      *reinterpret_cast<float2*>(ta + 8 * kTcRowFloats) = make_float2(acc[mt][2], acc[mt][3]);
+    }
+    __syncwarp();
+    const int r = r0 + lane;
+    if (r < R) {
+      const float4 cp0 = *reinterpret_cast<const float4*>(tile + lane * kTcRowFloats);
+      const float4 cp1 = *reinterpret_cast<const float4*>(tile + lane * kTcRowFloats + 4);
+      float c[1][NR];
+      const bool ok[1] = {true};
+      rep_coeffs<2, 1, 1, false, T2, false>(L, sp, dsc, R, R, r, ok, c, 0);
+      const float cp[NR] = {cp0.x, cp0.y, cp0.z, cp0.w, cp1.x, cp1.y, cp1.z, cp1.w};
+#pragma unroll
+      for (int m = 0; m < NR; ++m) c[0][m] += cp[m];
+      rep_decide<NR, false>(a, L, li, col, seg_c, q, s, (int64_t)s * R, r, c[0], p_beta, p_step, p_seed, s_dE,
+                            s_cnt);
+    }
+  }
   flush_block(a, s_dE, s_cnt);
 }
 
@@ -3224,6 +3403,7 @@ struct Launch {
   int rep_np = 0;           // replica-parallel kernel: threads per item (0 = per colour, by its size)
   int rep_pf = 0;           // replica-parallel kernel: 1 prefetch, 2 no prefetch (0 = per colour, by its size)
   bool cluster = false;     // chain-resident cluster kernel: one launch per compound sweep
+  bool rep_tc = false;      // replica-parallel pass with the pair records on the tensor cores (kernel 5)
 };
 
 using FastFn = void (*)(SweepArgs);
@@ -3322,10 +3502,26 @@ struct RepForm {
   int64_t nt;
   int32_t pf;
   FastFn fn;
+  size_t smem;  // dynamic shared memory (bytes)
 };
-RepForm rep_form(const scemc_ensemble* E, int c, int forced, int forced_np = 0, int forced_pf = 0) {
+RepForm rep_form(const scemc_ensemble* E, int c, int forced, int forced_np = 0, int forced_pf = 0, bool tc = false) {
   RepForm f;
   const int64_t sms = sm_count(E->device);
+  if (tc) {  // one warp per (site, 32 replicas)
+    int64_t items = 0;
+    const int32_t* sc = E->seg.data() + (size_t)c * (E->tabs.size() + 1);
+    for (size_t li = 0; li < E->tabs.size(); ++li)
+      items += (int64_t)(sc[li + 1] - sc[li]) / E->R[li] * ((E->R[li] + 31) / 32);
+    f.P = 1;
+    f.np = 1;
+    f.pf = 0;
+    f.nt = items * 32;
+    f.fn = E->trip2 ? k_rep_tc<true> : k_rep_tc<false>;
+    f.smem = (fast_param_floats(E->n_slots) + 8 * tc_warp_floats(std::max(E->dmax, 1), std::max(E->rmax, 1))) *
+             sizeof(float);
+    return f;
+  }
+  f.smem = fast_param_floats(E->n_slots) * sizeof(float);
   const int64_t nt1 = rep_threads(E, c, 1);
   // Small colours (twice the one-replica threads still fit one wave of four
   // 256-thread blocks per SM): one replica per thread and two threads per item, for
@@ -3458,7 +3654,6 @@ int32_t run_pass_impl(scemc_ensemble* E, int pass, const Launch& Lc) {
   const int max_items = max_colour_items(E);
   if (Lc.rep) {
     const int threads = 256;
-    const size_t smem = fast_param_floats(E->n_slots) * sizeof(float);
     a.item_base = E->d_item_base;
     const int cap = sm_count(E->device) * 64;
     if (Lc.precompute && pass < 0) {
@@ -3473,15 +3668,17 @@ int32_t run_pass_impl(scemc_ensemble* E, int pass, const Launch& Lc) {
       CUDA_TRY(cudaGetLastError());
     }
     if (Lc.mode == 2) return run_rep_persistent(E, a, Lc);
+    a.dmax = std::max(E->dmax, 1);
+    a.rmax = std::max(E->rmax, 1);
     for (int c = 0; c < E->max_colors; ++c) {
       const int n = E->seg[(size_t)c * (E->tabs.size() + 1) + E->tabs.size()];
       if (n == 0) continue;
       a.colour = c;
-      const RepForm f = rep_form(E, c, Lc.rep_p, Lc.rep_np, Lc.rep_pf);
-      CUDA_TRY(cudaFuncSetAttribute((const void*)f.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      const RepForm f = rep_form(E, c, Lc.rep_p, Lc.rep_np, Lc.rep_pf, Lc.rep_tc);
+      CUDA_TRY(cudaFuncSetAttribute((const void*)f.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.smem));
       const int blocks = (int)std::min<int64_t>(cap, (f.nt + threads - 1) / threads);
       ++E->launches;
-      f.fn<<<std::max(blocks, 1), threads, smem, E->stream>>>(a);
+      f.fn<<<std::max(blocks, 1), threads, f.smem, E->stream>>>(a);
       CUDA_TRY(cudaGetLastError());
     }
     return SCEMC_OK;
@@ -3828,7 +4025,8 @@ int auto_lanes(const scemc_ensemble* E) {
   return G;
 }
 
-// kernel: 0 auto, 1 generic, 2 row-parallel fast, 3 replica-parallel; proposals: 0 auto,
+// kernel: 0 auto, 1 generic, 2 row-parallel fast, 3 replica-parallel, 4 chain-resident
+// cluster, 5 replica-parallel with the pair records on the tensor cores; proposals: 0 auto,
 // 1 precompute, 2 inline.
 int32_t resolve_launch(const scemc_ensemble* E, int lanes, int mode, int kernel, int proposals, Launch* out,
                        int rep_replicas = 0, int rep_np = 0, int rep_pf = 0) {
@@ -3845,12 +4043,19 @@ int32_t resolve_launch(const scemc_ensemble* E, int lanes, int mode, int kernel,
     if (proposals == 0) proposals = E->tuned_proposals;
     if (lanes == 0) lanes = E->tuned_lanes;
     if (proposals == 3 && (mode == 2 || mode == 4)) mode = 3;  // learned passes run per colour
+    if (proposals == 3 && (kernel == 4 || kernel == 5)) kernel = 3;  // with the replica-parallel decision
   }
   if (mode < 0 || mode > 4) return fail(SCEMC_ERR_ARG, "mode must be 0..4");
-  if (mode == 4 && (!E->fast || kernel == 1 || kernel == 3 || proposals == 3))
+  if (mode == 4 && (!E->fast || kernel == 1 || kernel == 3 || kernel == 5 || proposals == 3))
     return fail(SCEMC_ERR_ARG, "the data-flow form (mode 4) runs the row-parallel kernel with plain proposals");
-  if (kernel < 0 || kernel > 4 || proposals < 0 || proposals > 3)
-    return fail(SCEMC_ERR_ARG, "kernel must be 0..4 and proposals 0..3");
+  if (kernel < 0 || kernel > 5 || proposals < 0 || proposals > 3)
+    return fail(SCEMC_ERR_ARG, "kernel must be 0..5 and proposals 0..3");
+  if (kernel == 5) {
+    if (!E->fast || E->lmax != 2)
+      return fail(SCEMC_ERR_ARG, "the tensor-core replica pass (kernel 5) needs the fast tables of lmax 2");
+    if (proposals == 3) return fail(SCEMC_ERR_ARG, "the tensor-core replica pass (kernel 5) runs plain proposals");
+    if (mode == 2 || mode == 4) return fail(SCEMC_ERR_ARG, "the tensor-core replica pass (kernel 5) runs with mode 1 or 3");
+  }
   if (kernel == 4) {
     int32_t rc;
     if ((rc = cluster_fits(E))) return rc;
@@ -3878,7 +4083,8 @@ int32_t resolve_launch(const scemc_ensemble* E, int lanes, int mode, int kernel,
   const bool rep_auto = E->fast && mode != 2 && min_r >= 16 &&
                         (int64_t)max_colour_items(E) >= (int64_t)sm_count(E->device) * 256;
   L.cluster = kernel == 4;
-  L.rep = kernel == 3 || (kernel == 0 && (rep_auto || (proposals == 3 && E->learned_field)));
+  L.rep = kernel == 3 || kernel == 5 || (kernel == 0 && (rep_auto || (proposals == 3 && E->learned_field)));
+  L.rep_tc = kernel == 5;
   L.fast = !L.rep && (kernel == 2 || kernel == 4 || (kernel == 0 && E->fast));
   L.learned = proposals == 3;
   L.mode = mode == 0 ? ((L.rep || L.learned || L.cluster) ? 1 : 2) : mode;
@@ -3922,7 +4128,7 @@ int32_t sweep_once(scemc_ensemble* E, int n_or, const Launch& L) {
 // configuration, replayed every sweep). Every launch reads the sweep counter from
 // device memory and the tail advances it, so one capture serves all sweeps.
 int32_t sweep_graph(scemc_ensemble* E, int n_or, const Launch& L, cudaGraphExec_t* out, int64_t* n_launch) {
-  const int key[7] = {n_or, L.cluster ? 3 : (L.rep ? 2 : (L.fast ? 1 : 0)), L.learned ? 2 : (L.precompute ? 1 : 0),
+  const int key[7] = {n_or, L.cluster ? 3 : (L.rep ? (L.rep_tc ? 4 : 2) : (L.fast ? 1 : 0)), L.learned ? 2 : (L.precompute ? 1 : 0),
                       L.fast ? 0 : (L.rep ? L.rep_p : L.G), E->recording ? 1 : 0, L.rep ? L.rep_np : 0,
                       L.rep ? L.rep_pf : 0};
   for (auto& g : E->graphs)
@@ -3946,11 +4152,10 @@ int32_t sweep_graph(scemc_ensemble* E, int n_or, const Launch& L, cudaGraphExec_
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   }
   if (L.rep) {
-    const size_t smem = fast_param_floats(E->n_slots) * sizeof(float);
-    for (int c = 0; c < E->max_colors; ++c)
-      for (int pass : {-1, 0})
-        CUDA_TRY(cudaFuncSetAttribute((const void*)rep_form(E, c, L.rep_p, L.rep_np, L.rep_pf).fn,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    for (int c = 0; c < E->max_colors; ++c) {
+      const RepForm f = rep_form(E, c, L.rep_p, L.rep_np, L.rep_pf, L.rep_tc);
+      CUDA_TRY(cudaFuncSetAttribute((const void*)f.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.smem));
+    }
   }
   const bool prof = E->profiling;
   E->profiling = false;  // graph launches are timed as a whole
@@ -4291,6 +4496,8 @@ int32_t scemc_batch_autotune(scemc_batch* b, int32_t or_per_metropolis, int32_t 
     cands.push_back({4, 2, 0, 2});
     for (int q : {1, 2}) cands.push_back({3, q, 0, 3});
     for (int q : {1, 2}) cands.push_back({2, q, 0, 3});
+    if (b->lmax == 2)
+      for (int q : {1, 2}) cands.push_back({3, q, 0, 5});
     if (cluster_fits(b) == SCEMC_OK)
       for (int q : {1, 2}) cands.push_back({3, q, 0, 4});
   } else {

@@ -268,14 +268,77 @@ def test_rep_forms_refuse_bad_values(gpu):
         b.record_slot(1, 0)
 
 
-def test_fcc64_32_rungs_replays_at_full_size(gpu):
+# The tensor-core replica pass (kernel 5) on every lmax-2 model with fast records: pair
+# records only (biquadratic), l = 1 and l = 2 pairs (mixed), plaquette quads and
+# Zeeman (bcc_l2_plaq_zeeman), l = 1 triangles (fcc), merged body-3 l <= 2 blocks
+# (bcc_l2_body3). A warp owns 32 replicas of a site: R = 1 and 3 leave most rows of
+# the tile empty; R = 32 records replica 25 (second 16-replica tile, row g + 8 of its
+# fragment); R = 40 runs two chunks per site and records replica 37 (second chunk).
+TC_MODELS = ["biquadratic_zeeman", "mixed", "bcc_l2_plaq_zeeman", "fcc_l2_tri_zeeman", "bcc_l2_body3"]
+TC_SHAPES = [(1, 0), (3, 2), (32, 25), (40, 37)]
+
+
+@pytest.mark.parametrize("name", TC_MODELS)
+@pytest.mark.parametrize("R,rec", TC_SHAPES, ids=[f"R{r}-rec{k}" for r, k in TC_SHAPES])
+def test_rep_tc_replays(gpu, name, R, rec):
+    """Kernel 5 (pair records as mma.sync TF32 products, both operands split into a
+    TF32 head and tail) replayed through the FP64 oracle: dE within the FP32 bar,
+    identical decisions except ties, the proposals, the configuration after the
+    compound sweep and the running energy, over Metropolis and overrelaxation passes
+    with precomputed and inline proposals, per-colour launches and the graph."""
+    H, OH = build(name)
+    gH = scemc.GPUTiledHamiltonian(H)
+    step = 0.6
+    seeds = [0x7C0 + 13 * i for i in range(R)]
+    betas = 1.0 / np.geomspace(0.02, 0.1, R)
+    b = scemc.GPUBatch([gH], [R], [rand_cfg(H.n_sites, 300 + i) for i in range(R)], seeds, step)
+    b.set_betas(betas)
+    b.record_slot(0, rec)
+    n_or = 2 if H.site_has_l1.any() else 0
+    ties = att = 0
+    for sw in range(1, 4):
+        cfg = b.download()["configs"][rec].copy()
+        b.record(True)
+        b.run(1, or_per_metropolis=n_or, kernel=5, mode=1 + 2 * (sw == 3), proposals=1 + (sw % 2))
+        t, a, _ = check_pass(OH, cfg, b.fetch_record(-1), betas[rec], "metro", seed=seeds[rec], sweep=sw, step=step)
+        ties, att = ties + t, att + a
+        for k in range(n_or):
+            t, a, _ = check_pass(OH, cfg, b.fetch_record(k), betas[rec], "or", seed=seeds[rec], sweep=sw, orpass=k)
+            ties, att = ties + t, att + a
+        post = b.download()
+        np.testing.assert_array_equal(post["configs"][rec], cfg)
+        E_or = OH.total_energy(post["configs"][rec])
+        assert abs(b.total_energy(rec) - E_or) <= 1e-10 * max(1.0, abs(E_or))
+        assert abs(post["energies"][rec] - E_or) <= 1e-5 * max(1.0, abs(E_or))
+    assert ties <= max(1, att // 100)
+
+
+def test_rep_tc_refusals(gpu):
+    """Kernel 5 needs lmax-2 fast tables, runs per-colour launches (mode 1 or 3) and
+    plain proposals."""
+    H, _ = build("bcc_body4")  # lmax 1
+    b = scemc.GPUBatch([scemc.GPUTiledHamiltonian(H)], [2], [rand_cfg(H.n_sites, 1)] * 2, [1, 2], 0.6)
+    with pytest.raises(_lib.ScemcArgumentError):
+        b.run(1, kernel=5, mode=1)
+    H2, _ = build("fcc_l2_tri_zeeman")
+    b2 = scemc.GPUBatch([scemc.GPUTiledHamiltonian(H2)], [2], [rand_cfg(H2.n_sites, 1)] * 2, [1, 2], 0.6)
+    for mode in (2, 4):
+        with pytest.raises(_lib.ScemcArgumentError):
+            b2.run(1, kernel=5, mode=mode)
+    b2.run(2, kernel=5, mode=3, or_per_metropolis=1)
+
+
+@pytest.mark.parametrize("kernel,recs", [(3, (0, 17)), (5, (0, 25))])
+def test_fcc64_32_rungs_replays_at_full_size(gpu, kernel, recs):
     """The large frustrated configuration at its own size (fcc 64^3 x 4 sites, 32
-    rungs, kT geometric in [0.05, 2.0] meV), through the launch form the library
-    picks by itself: its colours fill many waves, so k_rep_colour runs with two
-    replicas per thread, one thread per item and no prefetch. Rung 0 (the first lane
-    of a thread) and rung 17 (the second lane of thread 1) are recorded over a
-    Metropolis and an overrelaxation pass and replayed through the FP64 oracle
-    (dE and the decisions at every site, the proposals at 3000 sampled sites)."""
+    rungs, kT geometric in [0.05, 2.0] meV). Kernel 3 runs the form the library picks
+    by itself: its colours fill many waves, so k_rep_colour runs with two replicas per
+    thread, one thread per item and no prefetch; rung 0 (the first lane of a thread)
+    and rung 17 (the second lane of thread 1) are recorded. Kernel 5 (the tensor-core
+    pass) records rung 0 and rung 25 (second 16-replica tile, fragment row g + 8).
+    Each recorded rung is replayed over a Metropolis and an overrelaxation pass
+    through the FP64 oracle (dE and the decisions at every site, the proposals at
+    3000 sampled sites)."""
     w = models.config5_fcc(n=64, replicas=32)
     H = w.hamiltonians()[0]
     OH = O.OracleHamiltonian(4, w.terms, (64, 64, 64), magmoms=w.magmoms, field=w.field)
@@ -288,11 +351,11 @@ def test_fcc64_32_rungs_replays_at_full_size(gpu):
     b = scemc.GPUBatch([gH], [R], cfgs, seeds, step)
     b.set_betas(betas)
     ties = att = 0
-    for sw, rec in ((1, 0), (2, 17)):
+    for sw, rec in zip((1, 2), recs):
         b.record_slot(0, rec)
         cfg = b.download()["configs"][rec].copy()
         b.record(True)
-        b.run(1, or_per_metropolis=1, kernel=3, mode=1)
+        b.run(1, or_per_metropolis=1, kernel=kernel, mode=1)
         t, a, _ = check_pass(OH, cfg, b.fetch_record(-1), betas[rec], "metro", seed=seeds[rec], sweep=sw,
                              step=step, sample=3000)
         ties, att = ties + t, att + a
@@ -407,8 +470,8 @@ def test_autotune_keeps_a_valid_launch_form(gpu):
     b = scemc.GPUBatch([gH], [3], [rand_cfg(H.n_sites, i) for i in range(3)], [1, 2, 3], 0.6)
     b.set_betas([1 / 0.002, 1 / 0.004, 1 / 0.008])
     t = b.autotune(or_per_metropolis=1, sweeps_per_trial=3)
-    assert t["mode"] in (2, 3, 4) and t["proposals"] in (1, 2) and t["kernel"] in (2, 3, 4) and t["ms_per_sweep"] > 0
-    if t["kernel"] == 4:
+    assert t["mode"] in (2, 3, 4) and t["proposals"] in (1, 2) and t["kernel"] in (2, 3, 4, 5) and t["ms_per_sweep"] > 0
+    if t["kernel"] in (4, 5):
         assert t["mode"] == 3
     if t["kernel"] == 3:
         assert t["mode"] in (2, 3)
@@ -763,7 +826,7 @@ def test_launch_count_matches_the_launch_form(gpu):
     gH = scemc.GPUTiledHamiltonian(H)
     b = scemc.GPUBatch([gH], [2], [rand_cfg(H.n_sites, 1), rand_cfg(H.n_sites, 2)], [1, 2], 0.6)
     per_sweep = 1 + 2 * H.n_colors + 1
-    for kernel, mode in [(2, 1), (2, 3), (3, 1), (3, 3)]:
+    for kernel, mode in [(2, 1), (2, 3), (3, 1), (3, 3), (5, 1), (5, 3)]:
         b.run(1, or_per_metropolis=1, mode=mode, kernel=kernel, proposals=1)  # graph capture, if any
         n0 = b.launches()
         b.run(3, or_per_metropolis=1, mode=mode, kernel=kernel, proposals=1)
