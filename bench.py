@@ -233,6 +233,7 @@ def run_fcc_learned(args) -> int:
     losses = net.train(X, Y, batch=1024, epochs=args.epochs, lr=1e-3, seed=5)
     torch.cuda.synchronize()
     t2 = time.perf_counter()
+    relax = fcc_relaxation(gH, w.kts, net, sweeps=1500, every=25)
     measure = args.steps
     kw = dict(kT=w.kts, exchange=True, exchange_interval=1, or_per_metropolis=1, sweeps_therm=args.therm,
               sweeps_measure=measure, seed=5, kernel=3)
@@ -264,9 +265,62 @@ def run_fcc_learned(args) -> int:
                        "energy_plain": e_p, "energy_learned": e_l, "energy_err_plain": s_p,
                        "energy_err_learned": s_l, "energy_z": z.tolist(), "energy_z_max": float(np.max(z)),
                        "training_rows": int(X.shape[0]), "epochs": args.epochs, "collect_s": t1 - t0,
-                       "train_s": t2 - t1, "train_loss_first_last": [float(losses[0]), float(losses[-1])]}}
+                       "train_s": t2 - t1, "train_loss_first_last": [float(losses[0]), float(losses[-1])],
+                       "relaxation": relax}}
     print(json.dumps(line))
     return 0
+
+
+def fcc_relaxation(gH, kts, net, *, sweeps: int, every: int, seed: int = 11) -> dict:
+    """Relaxation from one random start: both arms (Metropolis + OR + exchange, and
+    learned Metropolis-Hastings + OR + exchange) run `sweeps` compound sweeps from the
+    same random configurations with the same keys, recording every rung's energy each
+    `every` sweeps (step adaptation on, as in a thermalisation phase). Per rung, the
+    target is the plain arm's final energy (mean of its last four records); the
+    learned arm's time to reach it (first record at or below, its sweeps x its seconds
+    per sweep) against the plain arm's whole run gives the speed-up in reaching that
+    energy."""
+    import scemc
+    from scemc import models
+    R = len(kts)
+    n = gH.n_sites
+    cfgs = [models.random_config(n, seed + r) for r in range(R)]
+    out = {"sweeps": [every * (k + 1) for k in range(sweeps // every)]}
+    per_sweep, traces, drift = {}, {}, {}
+    for arm in ("plain", "learned"):
+        b = scemc.GPUBatch([gH], [R], cfgs, [seed * 100 + r for r in range(R)], 0.6)
+        b.set_betas(1.0 / np.asarray(kts))
+        if arm == "learned":
+            b.set_learned(net, None)
+        kw = dict(or_per_metropolis=1, exchange=True, exchange_interval=1, kernel=3, measure_interval=every,
+                  phase_total=sweeps, proposals=3 if arm == "learned" else 0, adapt_interval=50, adapt_target=0.5)
+        b.run(2, **dict(kw, measure_interval=0, phase_total=2))  # warm-up: graph capture, attributes
+        b.upload(cfgs)
+        t0 = time.perf_counter()
+        b.run(sweeps, **kw)
+        per_sweep[arm] = (time.perf_counter() - t0) / sweeps
+        rec = b.fetch_measurements()  # (records, rungs, columns); column 0 the energy (eV)
+        traces[arm] = rec[:, :R, 0] / n
+        # the running energies (FP32 dE, fixed-point sums) against the FP64 recompute
+        run_e = b.download()["energies"]
+        drift[arm] = max(abs(run_e[k] - b.total_energy(k)) / n for k in range(R))
+        del b
+    target = traces["plain"][-4:].mean(axis=0)
+    speedups, reach = [], []
+    for r in range(R):
+        hit = np.nonzero(traces["learned"][:, r] <= target[r])[0]
+        k = int(hit[0]) + 1 if len(hit) else None
+        reach.append(None if k is None else every * k)
+        speedups.append(None if k is None else (sweeps * per_sweep["plain"]) / (every * k * per_sweep["learned"]))
+    got = [x for x in speedups if x is not None]
+    out.update({"plain_s_per_sweep": per_sweep["plain"], "learned_s_per_sweep": per_sweep["learned"],
+                "max_drift_eV_per_site": drift,
+                "plain_energy_ueV_per_site": (1e6 * traces["plain"].mean(axis=1)).tolist(),
+                "learned_energy_ueV_per_site": (1e6 * traces["learned"].mean(axis=1)).tolist(),
+                "learned_sweeps_to_plain_final": reach, "speedup_to_plain_final": speedups,
+                "speedup_median": float(np.median(got)) if len(got) == R else None,
+                "speedup_min": float(np.min(got)) if len(got) == R else None})
+    return out
 
 
 def run_learned(args) -> int:

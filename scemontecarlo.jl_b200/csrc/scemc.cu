@@ -1953,9 +1953,11 @@ __global__ void __launch_bounds__(256, P == 1 ? 4 : SCEMC_REP_MINB_P2) k_rep_col
 // blocks. A lane's A values over the eight components are then four whole Z rows
 // (two neighbours x two replicas per 16-replica tile), which it computes from the
 // spins it loads, so no operand moves between lanes; its B values are row g of two
-// blocks. FP32 accuracy comes from splitting both operands (x = hi + lo, hi = x
-// rounded to TF32) and summing hi.hi + hi.lo + lo.hi: about 2^-21 relative per
-// product. After the last group the accumulators pass through shared memory to
+// blocks. FP32 accuracy comes from splitting both operands, x = hi + lo with hi = x
+// rounded to TF32, and summing hi.hi + hi.lo + lo.hi; the tensor core truncates lo to
+// TF32, which leaves under 2^-21 relative per product (the block rows are read once
+// per group of eight records and split in registers: measured faster than reading
+// host-split copies, which doubles the block loads). After the last group the accumulators pass through shared memory to
 // lane = replica; the lane adds its triplet, quad and one-body records (FP32 FMAs,
 // as the replica-parallel kernel) and decides. The sums run in another order than
 // the FMA kernels', so the chains agree with theirs to rounding, not bit for bit.
@@ -1972,6 +1974,15 @@ __device__ __forceinline__ uint32_t tf32_rna(float x) {
   return h;
 }
 
+// The head of a Z value: rounded to TF32 (SCEMC_TC_ZMASK = 0) or truncated to its
+// sign, exponent and 10 significand bits (1); the tail is the exact FP32 remainder.
+#ifndef SCEMC_TC_ZMASK
+#define SCEMC_TC_ZMASK 0
+#endif
+__device__ __forceinline__ uint32_t tf32_head(float x) {
+  return SCEMC_TC_ZMASK ? (__float_as_uint(x) & 0xffffe000u) : tf32_rna(x);
+}
+
 // d += a . b: one m16n8k8 product, TF32 operands, FP32 accumulators
 __device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
                                          uint32_t b0, uint32_t b1) {
@@ -1981,8 +1992,11 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1
       : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
+#ifndef SCEMC_TC_MINB
+#define SCEMC_TC_MINB 2
+#endif
 template <bool T2>
-__global__ void __launch_bounds__(256, 2) k_rep_tc(SweepArgs a) {
+__global__ void __launch_bounds__(256, SCEMC_TC_MINB) k_rep_tc(SweepArgs a) {
   constexpr int NR = 8;
   extern __shared__ __align__(16) float zsm[];
   __shared__ unsigned long long s_dE[kMaxSlots];
@@ -2038,6 +2052,7 @@ __global__ void __launch_bounds__(256, 2) k_rep_tc(SweepArgs a) {
       const bool v1 = k1 < n_pair, v2 = k2 < n_pair;
       const uint2 rc1 = rb[v1 ? k1 : 0], rc2 = rb[v2 ? k2 : 0];
       const int nb1 = nbid[rc1.y & 0xffu], nb2 = nbid[rc2.y & 0xffu];
+      // rows g of the two blocks, split into head and tail (zero past the last record)
       uint32_t b1h[NR], b1l[NR], b2h[NR], b2l[NR];
       {
         const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -2071,7 +2086,7 @@ __global__ void __launch_bounds__(256, 2) k_rep_tc(SweepArgs a) {
         zrow_nr<NR>(s3.x, s3.y, s3.z, z3);
 #pragma unroll
         for (int j = 0; j < NR; ++j) {
-          const uint32_t h0 = tf32_rna(z0[j]), h1 = tf32_rna(z1[j]), h2 = tf32_rna(z2[j]), h3 = tf32_rna(z3[j]);
+          const uint32_t h0 = tf32_head(z0[j]), h1 = tf32_head(z1[j]), h2 = tf32_head(z2[j]), h3 = tf32_head(z3[j]);
           const uint32_t l0 = __float_as_uint(z0[j] - __uint_as_float(h0));
           const uint32_t l1 = __float_as_uint(z1[j] - __uint_as_float(h1));
           const uint32_t l2 = __float_as_uint(z2[j] - __uint_as_float(h2));

@@ -408,3 +408,38 @@ def test_learned_field_moments_in_a_field_are_exact(gpu):
     m = es.mean()
     err = es.mean(axis=0).std(ddof=1) / math.sqrt(R)
     assert abs(m - (-h * langevin(bh))) < max(4 * err, 2e-3 * h), (m, -h * langevin(bh), err)
+
+
+def test_learned_field_dimer_is_exact(gpu):
+    """Field mode on the interacting dimer E = J e1.e2, <E> = J L(beta |J|)
+    (test_gpu_pt.jl:13-42): each spin's proposal is a sharp mixture about directions
+    the network computes from its coefficients (J times the other spin) and kT, so the
+    Hastings ratio carries the whole correction."""
+    J = -0.02
+    H = models.dimer(J=J)
+    gH = scemc.GPUTiledHamiltonian(H)
+    net = learned.ProposalNet(seed=8, field_rows=3)
+    P = learned.unpack(net.params().copy())
+    P["b3"][4:20:5] = 50.0  # softplus ~ 50: kappa = 50 / kT[meV] ~ 8 at kT = 6.7 meV
+    net.set_params(learned.pack(P))
+    kt = abs(J) / 3.0
+    R = 32
+    b = scemc.GPUBatch([gH], [R], [models.random_config(4, 90 + r) for r in range(R)], list(range(700, 700 + R)),
+                       0.6)
+    b.set_betas(np.full(R, 1.0 / kt))
+    b.set_learned(net, None)
+    b.run(500, proposals=3, kernel=3)
+    es = []
+    for _ in range(2000):
+        b.run(5, proposals=3, kernel=3)
+        es.append(b.download()["energies"].copy())
+    es = np.asarray(es)
+    m = es.mean()
+    err = es.mean(axis=0).std(ddof=1) / math.sqrt(R)
+    exact = J * langevin(abs(J) / kt)
+    assert abs(m - exact) < 4 * err + 1e-4 * abs(J), (m, exact, err)
+    cnt = b.download()["counters"]
+    acc = cnt[:, 0].sum() / cnt[:, 1].sum()
+    assert 0.01 < acc < 0.95, acc
+    for r in range(R):  # the running energy tracks the FP64 recompute
+        assert abs(b.download()["energies"][r] - b.total_energy(r)) <= 1e-6 * abs(J) + 1e-9
