@@ -1954,10 +1954,11 @@ __global__ void __launch_bounds__(256, P == 1 ? 4 : SCEMC_REP_MINB_P2) k_rep_col
 // (two neighbours x two replicas per 16-replica tile), which it computes from the
 // spins it loads, so no operand moves between lanes; its B values are row g of two
 // blocks. FP32 accuracy comes from splitting both operands, x = hi + lo with hi = x
-// rounded to TF32, and summing hi.hi + hi.lo + lo.hi; the tensor core truncates lo to
-// TF32, which leaves under 2^-21 relative per product (the block rows are read once
-// per group of eight records and split in registers: measured faster than reading
-// host-split copies, which doubles the block loads). After the last group the accumulators pass through shared memory to
+// truncated to TF32 (|lo| < 2^-10 |x|), and summing hi.hi + hi.lo + lo.hi; the tensor
+// core keeps 11 significant bits of lo and the lo.lo product is dropped, which leaves
+// under 2^-19 relative per product (the block rows are read once per group of eight
+// records and split in registers: measured faster than reading host-split copies,
+// which doubles the block loads). After the last group the accumulators pass through shared memory to
 // lane = replica; the lane adds its triplet, quad and one-body records (FP32 FMAs,
 // as the replica-parallel kernel) and decides. The sums run in another order than
 // the FMA kernels', so the chains agree with theirs to rounding, not bit for bit.
@@ -1974,13 +1975,14 @@ __device__ __forceinline__ uint32_t tf32_rna(float x) {
   return h;
 }
 
-// The head of a Z value: rounded to TF32 (SCEMC_TC_ZMASK = 0) or truncated to its
-// sign, exponent and 10 significand bits (1); the tail is the exact FP32 remainder.
-#ifndef SCEMC_TC_ZMASK
-#define SCEMC_TC_ZMASK 0
+// The head of an operand: its sign, exponent and 10 significand bits (one mask), or
+// with SCEMC_TC_RNA = 1 the value rounded to TF32 (cvt.rna, measured 7 % slower per
+// compound sweep at fcc 48^3 x 32); the tail is the exact FP32 remainder.
+#ifndef SCEMC_TC_RNA
+#define SCEMC_TC_RNA 0
 #endif
 __device__ __forceinline__ uint32_t tf32_head(float x) {
-  return SCEMC_TC_ZMASK ? (__float_as_uint(x) & 0xffffe000u) : tf32_rna(x);
+  return SCEMC_TC_RNA ? tf32_rna(x) : (__float_as_uint(x) & 0xffffe000u);
 }
 
 // d += a . b: one m16n8k8 product, TF32 operands, FP32 accumulators
@@ -2064,9 +2066,9 @@ __global__ void __launch_bounds__(256, SCEMC_TC_MINB) k_rep_tc(SweepArgs a) {
         const float x2[NR] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
 #pragma unroll
         for (int m = 0; m < NR; ++m) {
-          b1h[m] = tf32_rna(x1[m]);
+          b1h[m] = tf32_head(x1[m]);
           b1l[m] = __float_as_uint(x1[m] - __uint_as_float(b1h[m]));
-          b2h[m] = tf32_rna(x2[m]);
+          b2h[m] = tf32_head(x2[m]);
           b2l[m] = __float_as_uint(x2[m] - __uint_as_float(b2h[m]));
         }
       }

@@ -30,5 +30,7 @@ def test_reference_arm_prints_one_contract_line():
 
 def test_dram_traffic_record_names_the_default_workload():
     d = json.loads((ROOT / "profiles" / "dram_traffic.json").read_text())
-    rec = d["fcc64_l2_tri_zeeman_32rungs_metropolis+OR+exchange"]
-    assert 100 < rec["bytes_per_attempt"] < 5000 and rec["source"]
+    recs = d["fcc64_l2_tri_zeeman_32rungs_metropolis+OR+exchange"]
+    assert "3" in recs  # by kernel id of the launch form the autotuner may pick
+    for rec in recs.values():
+        assert 100 < rec["bytes_per_attempt"] < 5000 and rec["source"] and rec["kernel"]

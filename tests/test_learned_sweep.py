@@ -441,5 +441,5 @@ def test_learned_field_dimer_is_exact(gpu):
     cnt = b.download()["counters"]
     acc = cnt[:, 0].sum() / cnt[:, 1].sum()
     assert 0.01 < acc < 0.95, acc
-    for r in range(R):  # the running energy tracks the FP64 recompute
-        assert abs(b.download()["energies"][r] - b.total_energy(r)) <= 1e-6 * abs(J) + 1e-9
+    for r in range(R):  # the running energy (FP32 dE over ~10^4 moves) tracks the FP64 recompute
+        assert abs(b.download()["energies"][r] - b.total_energy(r)) <= 1e-5 * abs(J)
