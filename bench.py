@@ -439,7 +439,9 @@ def main():
                     help="fcc on one GPU: skip the learned-vs-plain extra object")
     ap.add_argument("--fcc-n", type=int, default=64, help="cells per edge of the fcc workload")
     ap.add_argument("--mode", type=int, default=0, help="0 auto, 1 per-colour launches, 2 persistent, 3 graph")
-    ap.add_argument("--kernel", type=int, default=0, help="0 auto, 1 generic, 2 row-parallel, 3 replica-parallel")
+    ap.add_argument("--kernel", type=int, default=0,
+                    help="0 auto, 1 generic, 2 row-parallel, 3 replica-parallel, 4 chain-resident cluster, "
+                         "5 replica-parallel with tensor-core pair records")
     ap.add_argument("--lanes", type=int, default=0, help="lanes per site (0 = autotuned)")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--therm", type=int, default=2000,
