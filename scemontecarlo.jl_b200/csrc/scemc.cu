@@ -1994,9 +1994,32 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1
       : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
+// three 256-thread blocks per SM (80 registers, a few spills): measured 7 % faster per compound sweep
+// than two blocks at 128 registers at fcc 64^3 x 32, where the pass waits on its neighbour gathers
 #ifndef SCEMC_TC_MINB
-#define SCEMC_TC_MINB 2
+#define SCEMC_TC_MINB 3
 #endif
+// SCEMC_TC_FOLD = 1: the Z rows' normalisation constants move into the block columns
+// (scaled once per group of records), and each lane evaluates the bare polynomials
+// (y, z, x, xy, yz, 3z^2 - 1, xz, x^2 - y^2) of its eight spins per group.
+// (measured 3 % faster at fcc 64^3 x 32; 0 evaluates the normalised rows)
+#ifndef SCEMC_TC_FOLD
+#define SCEMC_TC_FOLD 1
+#endif
+__device__ __forceinline__ float tc_col_scale(int m) {
+  if (!SCEMC_TC_FOLD) return 1.0f;
+  return m < 3 ? kN1 : (m == 5 ? kC20 : (m == 7 ? kC22 : kC2a));
+}
+__device__ __forceinline__ void tc_zrow(float4 v, float (&o)[8]) {
+  if (SCEMC_TC_FOLD) {
+    o[0] = v.y, o[1] = v.z, o[2] = v.x;
+    o[3] = v.x * v.y, o[4] = v.y * v.z, o[5] = 3.0f * (v.z * v.z) - 1.0f;
+    o[6] = v.x * v.z, o[7] = v.x * v.x - v.y * v.y;
+  } else {
+    zrow_nr<8>(v.x, v.y, v.z, o);
+  }
+}
+
 template <bool T2>
 __global__ void __launch_bounds__(256, SCEMC_TC_MINB) k_rep_tc(SweepArgs a) {
   constexpr int NR = 8;
@@ -2062,10 +2085,12 @@ __global__ void __launch_bounds__(256, SCEMC_TC_MINB) k_rep_tc(SweepArgs a) {
         const float4* w2 = reinterpret_cast<const float4*>(L.ftensor + (rc2.x & kOffMask)) + 2 * g;
         const float4 p0 = v1 ? __ldg(w1) : z4, p1 = v1 ? __ldg(w1 + 1) : z4;
         const float4 q0 = v2 ? __ldg(w2) : z4, q1 = v2 ? __ldg(w2 + 1) : z4;
-        const float x1[NR] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
-        const float x2[NR] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+        float x1[NR] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
+        float x2[NR] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
 #pragma unroll
         for (int m = 0; m < NR; ++m) {
+          x1[m] *= tc_col_scale(m);
+          x2[m] *= tc_col_scale(m);
           b1h[m] = tf32_head(x1[m]);
           b1l[m] = __float_as_uint(x1[m] - __uint_as_float(b1h[m]));
           b2h[m] = tf32_head(x2[m]);
@@ -2082,10 +2107,10 @@ __global__ void __launch_bounds__(256, SCEMC_TC_MINB) k_rep_tc(SweepArgs a) {
         const float4 s2 = v2 && ra < R ? __ldcg(sp + (int64_t)nb2 * R + ra) : z4;
         const float4 s3 = v2 && rc < R ? __ldcg(sp + (int64_t)nb2 * R + rc) : z4;
         float z0[NR], z1[NR], z2[NR], z3[NR];
-        zrow_nr<NR>(s0.x, s0.y, s0.z, z0);
-        zrow_nr<NR>(s1.x, s1.y, s1.z, z1);
-        zrow_nr<NR>(s2.x, s2.y, s2.z, z2);
-        zrow_nr<NR>(s3.x, s3.y, s3.z, z3);
+        tc_zrow(s0, z0);
+        tc_zrow(s1, z1);
+        tc_zrow(s2, z2);
+        tc_zrow(s3, z3);
 #pragma unroll
         for (int j = 0; j < NR; ++j) {
           const uint32_t h0 = tf32_head(z0[j]), h1 = tf32_head(z1[j]), h2 = tf32_head(z2[j]), h3 = tf32_head(z3[j]);
