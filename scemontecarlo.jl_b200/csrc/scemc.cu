@@ -1958,10 +1958,11 @@ __global__ void __launch_bounds__(256, P == 1 ? 4 : SCEMC_REP_MINB_P2) k_rep_col
 // core keeps 11 significant bits of lo and the lo.lo product is dropped, which leaves
 // under 2^-19 relative per product (the block rows are read once per group of eight
 // records and split in registers: measured faster than reading host-split copies,
-// which doubles the block loads). After the last group the accumulators pass through shared memory to
-// lane = replica; the lane adds its triplet, quad and one-body records (FP32 FMAs,
-// as the replica-parallel kernel) and decides. The sums run in another order than
-// the FMA kernels', so the chains agree with theirs to rounding, not bit for bit.
+// which doubles the block loads). After the last group the accumulators pass through
+// shared memory to lane = replica; the lane adds its triplet, quad and one-body
+// records (FP32 FMAs, as the replica-parallel kernel) and decides. The sums run in
+// another order than the FMA kernels', so the chains agree with theirs to rounding,
+// not bit for bit.
 // ---------------------------------------------------------------------------
 constexpr int kTcRowFloats = 12;  // a row of the 32 x 8 coefficient tile: 16-byte aligned, no bank conflicts
 
@@ -1994,15 +1995,16 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1
       : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-// three 256-thread blocks per SM (80 registers, 112 bytes of spills): measured 7 % faster per compound sweep
-// than two blocks at 128 registers at fcc 64^3 x 32, where the pass waits on its neighbour gathers
+// Three 256-thread blocks per SM (80 registers, 112 bytes of spills): measured 7 %
+// faster per compound sweep than two blocks at 128 registers at fcc 64^3 x 32, where
+// the pass waits on its neighbour gathers.
 #ifndef SCEMC_TC_MINB
 #define SCEMC_TC_MINB 3
 #endif
 // SCEMC_TC_FOLD = 1: the Z rows' normalisation constants move into the block columns
 // (scaled once per group of records), and each lane evaluates the bare polynomials
-// (y, z, x, xy, yz, 3z^2 - 1, xz, x^2 - y^2) of its eight spins per group.
-// (measured 3 % faster at fcc 64^3 x 32; 0 evaluates the normalised rows)
+// (y, z, x, xy, yz, 3z^2 - 1, xz, x^2 - y^2) of its eight spins per group: measured
+// 3 % faster at fcc 64^3 x 32. 0 evaluates the normalised rows.
 #ifndef SCEMC_TC_FOLD
 #define SCEMC_TC_FOLD 1
 #endif
