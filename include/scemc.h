@@ -225,7 +225,8 @@ int32_t scemc_batch_sync(scemc_batch* b);
 /* The batch's cudaStream_t (as void*), for callers that order or time work on it. */
 int32_t scemc_batch_stream(const scemc_batch* b, void** stream);
 /* Replaces every slot's spins (3 x n_sites FP64 per slot, payload order) and, when
- * energies is not NULL, the running energies. The payload crosses the bus unchanged
+ * energies is not NULL, the running energies (with NULL they keep their old values;
+ * scemc_renormalize on the batch recomputes them). The payload crosses the bus unchanged
  * in one copy; the device checks it (SCEMC_ERR_NUMERIC names the first non-finite
  * spin's replica and column, and nothing changes), rounds it to FP32 and interleaves
  * the replicas. Replaces _from_host! (src/gpu/gpu_state.jl:81-86) for every slot. */

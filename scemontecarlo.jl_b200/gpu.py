@@ -310,7 +310,9 @@ class GPUBatch:
 
     def upload(self, configs, energies=None):
         """Replaces every chain's spins (the payload of all chains, table-major, each
-        3 x n_sites) and optionally the running energies."""
+        3 x n_sites) and optionally the running energies. With energies=None the running
+        energies keep their old values: pass the new configurations' energies, or call
+        renormalize() after the upload (FP64 recompute), before relying on them."""
         cfg = np.ascontiguousarray(configs, np.float64).reshape(-1)
         if cfg.size != 3 * self.n_sites_total:
             raise ValueError("configs hold %d values, the batch %d" % (cfg.size, 3 * self.n_sites_total))
